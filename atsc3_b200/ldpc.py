@@ -1,0 +1,179 @@
+"""LDPC decoding on the GPU: plans, the flooding decoder and the
+``GpuMinSum`` drop-in.
+
+``GpuMinSum`` keeps the constructor and ``decode`` signature of
+``lab/m9_gpu.py:84-220`` (Felbs/atsc3) so the reference's callers
+(``lab/m9_fast.py:872-874``, ``lab/m44_ldm.py:2519-2520``) can use it
+unchanged.  Decoding runs in ``libatsc3_fec.so`` (one thread-block cluster per
+codeword, state in distributed shared memory); nothing here falls back to a
+CPU decoder.
+
+Two bit-exact semantics are offered (``semantics=``):
+
+* ``"torch"`` -- the reference GpuMinSum / numpy float64 decoders
+  (``lab/m9_gpu.py:168-211``, ``lab/m3_ldpc.py:560-630``): message update
+  first, ``its`` >= 1, variable sums accumulated onto the channel LLR.  The
+  default of ``GpuMinSum``, in float64 or float32.
+* ``"kernel"`` -- ``lab/ldpc_kernel.c`` and the numpy float32 fast path
+  (``lab/m3_ldpc.py:336-397``): syndrome before each update, ``its`` may be
+  0, variable sums from +0 then added to the channel LLR.  float32 only.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+
+from . import codes as C
+from . import native as N
+
+SEMANTICS = {"kernel": 0, "torch": 1}
+_DTYPES = {"float32": 0, "float64": 1}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Plan:
+    """Device tables of one code for one message dtype and cluster size."""
+
+    def __init__(self, cptr, cidx, vptr, vedge, n, dtype="float32",
+                 cluster=0):
+        self.n = int(n)
+        self.nc = len(cptr) - 1
+        self.nedges = int(len(cidx))
+        self.dtype = dtype
+        arrs = [np.ascontiguousarray(a, np.int32)
+                for a in (cptr, cidx, vptr, vedge)]
+        h = ctypes.c_void_p()
+        N.call("atsc3_ldpc_plan_create", *[a.ctypes.data for a in arrs],
+               self.n, self.nc, self.nedges, _DTYPES[dtype], int(cluster),
+               ctypes.byref(h))
+        self._h = h
+        info = np.zeros(10, np.int64)
+        N.call("atsc3_ldpc_plan_info", h, info.ctypes.data)
+        self.info = dict(zip(("n", "nc", "nedges", "cluster", "smem_bytes",
+                              "record_bytes", "dmax_c", "dmax_v",
+                              "table_bytes", "dtype"), info.tolist()))
+        self.cluster = self.info["cluster"]
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                N.lib().atsc3_ldpc_plan_destroy(h)
+            except Exception:       # interpreter shutdown
+                pass
+            self._h = None
+
+
+_PLANS = {}
+_PLANS_LOCK = threading.Lock()
+
+
+def plan_for(rate, n, dtype="float32", cluster=0):
+    """Cached Plan of an A/322 code."""
+    torch = _torch()
+    key = (rate, n, dtype, cluster, torch.cuda.current_device())
+    with _PLANS_LOCK:
+        p = _PLANS.get(key)
+        if p is None:
+            p = Plan(*C.csr(rate, n), n, dtype=dtype, cluster=cluster)
+            _PLANS[key] = p
+    return p
+
+
+def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
+                 want_bits=True, want_hard=False, threads=0, out=None,
+                 stream=None):
+    """Decode (nblk, n) device LLRs.  Returns a dict of device tensors:
+    bits (uint8, nblk x n) and/or hard (packed, nblk x ceil(n/32)*4 bytes),
+    conv (uint8), its (int32), bad (int32)."""
+    torch = _torch()
+    want_t = torch.float64 if plan.dtype == "float64" else torch.float32
+    if llr.dtype != want_t or llr.device.type != "cuda":
+        raise TypeError(f"llr must be a CUDA {want_t} tensor")
+    if llr.dim() != 2 or llr.shape[1] != plan.n or llr.stride(1) != 1:
+        raise ValueError("llr must be (nblk, n) with unit column stride")
+    nblk = llr.shape[0]
+    dev = llr.device
+    o = out if out is not None else {}
+    if want_bits and "bits" not in o:
+        o["bits"] = torch.empty((nblk, plan.n), dtype=torch.uint8, device=dev)
+    if want_hard and "hard" not in o:
+        o["hard"] = torch.empty((nblk, (plan.n + 31) // 32 * 4),
+                                dtype=torch.uint8, device=dev)
+    for k, dt in (("conv", torch.uint8), ("its", torch.int32),
+                  ("bad", torch.int32)):
+        if k not in o:
+            o[k] = torch.empty(nblk, dtype=dt, device=dev)
+    bits = o.get("bits") if want_bits else None
+    hard = o.get("hard") if want_hard else None
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    N.call("atsc3_ldpc_decode_flood", plan.handle, llr.data_ptr(),
+           llr.stride(0), nblk, int(iters), float(alpha),
+           SEMANTICS[semantics], N.ptr(bits),
+           bits.stride(0) if bits is not None else 0, N.ptr(hard),
+           hard.stride(0) if hard is not None else 0, o["conv"].data_ptr(),
+           o["its"].data_ptr(), o["bad"].data_ptr(), int(threads), st)
+    return o
+
+
+class GpuMinSum:
+    """Batched normalised min-sum for ONE (rate, Ninner) code -- drop-in for
+    ``lab/m9_gpu.py:84-220``.
+
+    ``checks`` is the per-check column list (``m3_ldpc.parity_check``).
+    ``decode(llr2d)`` takes (nblk, n) LLRs as numpy or a CUDA tensor and
+    returns numpy ``(bits uint8, converged bool, iters int32, bad int32)``.
+    """
+
+    BIG = 1e9
+
+    def __init__(self, checks, n, iters=50, alpha=0.75, device="cuda",
+                 dtype="float64", semantics="torch", cluster=0):
+        torch = _torch()
+        if dtype not in ("float64", "float32"):
+            raise ValueError("GpuMinSum on B200 decodes in float64 or float32 "
+                             "(bit-exact); bfloat16/float16 are not offered")
+        if semantics == "kernel" and dtype != "float32":
+            raise ValueError("kernel semantics are float32 only")
+        self.n, self.iters, self.alpha = int(n), iters, alpha
+        self.dev = torch.device(device)
+        self.dt = {"float64": torch.float64, "float32": torch.float32}[dtype]
+        self.dtype_name = dtype
+        self.semantics = semantics
+        with torch.cuda.device(self.dev):
+            self.plan = Plan(*C.csr_from_checks(checks, n), n, dtype=dtype,
+                             cluster=cluster)
+        self.nc = self.plan.nc
+        self.stats = dict(calls=0, iters=0, blocks=0)
+
+    def decode(self, llr2d, iters=None, alpha=None):
+        torch = _torch()
+        iters = iters or self.iters
+        alpha = self.alpha if alpha is None else alpha
+        if isinstance(llr2d, torch.Tensor):
+            llr = llr2d.to(self.dev, dtype=self.dt).contiguous()
+        else:
+            a = np.ascontiguousarray(np.asarray(llr2d, np.float64))
+            llr = torch.from_numpy(a).to(self.dev, dtype=self.dt)
+        if llr.dim() != 2 or llr.shape[1] != self.n:
+            raise ValueError(f"expected (nblk, {self.n}) LLRs")
+        nb = llr.shape[0]
+        with torch.cuda.device(self.dev):
+            o = decode_flood(self.plan, llr, iters=iters, alpha=alpha,
+                             semantics=self.semantics)
+        self.stats["calls"] += 1
+        self.stats["blocks"] += nb
+        its = o["its"].cpu().numpy()
+        self.stats["iters"] += int(its.max(initial=0))
+        return (o["bits"].cpu().numpy(), o["conv"].cpu().numpy().astype(bool),
+                its, o["bad"].cpu().numpy())

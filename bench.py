@@ -1,0 +1,431 @@
+#!/usr/bin/env python3
+"""Throughput of the B200 FEC back end on the frame-scale workload.
+
+Workload (one step = one frame): 1,216,939 complex64 cells per frame, 16-NUC
+with the 64800-bit rate-6/15 LDPC code, i.e. 75 whole FEC blocks of 16,200
+cells (the remaining 1,939 cells of the frame do not fill a block).  Each
+cell has a Rayleigh channel gain |CN(0,1)| that the equaliser removed, so the
+noise variance N0/h^2 is passed per cell.  Frame f is at Es/N0 =
+4.0 + 0.5*(f mod 9) dB (the 4..8 dB sweep), normalised min-sum alpha 0.75,
+at most 50 iterations, early stop on a zero syndrome, then BCH + descramble.
+Payload bits are seeded uniform random, encoded by the package's GPU
+transmitter; every step reads a different frame (0.93 GB of distinct frames
+for 64 steps, far above the 126 MB L2).
+
+metric = decoded info Mbit/s = 75 * 25728 payload bits per frame / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  `--impl reference` times the reference's own
+CPU path on the host cores instead (demap + de-interleave in numpy, the
+reference's compiled lab/ldpc_kernel.c, BCH), on a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+N_INNER, MOD, RATE = 64800, "16QAM", "6/15"
+CELLS_PER_FRAME = 1_216_939
+ESN0 = [4.0 + 0.5 * i for i in range(9)]
+ITERS, ALPHA = 50, 0.75
+METRIC = ("decoded info Mbit/s on 1 B200 at FER<=1e-4; mean iterations, "
+          "learned vs plain min-sum")
+PEAKS = os.path.join(HERE, "MEASURED_PEAKS.json")
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_frames(nframes, seed, device):
+    """Seeded frames: cells (F, 75, 16200) complex64, sigma2 same shape f32."""
+    import torch
+    from atsc3_b200 import codes as C
+    from atsc3_b200 import synth
+    nblk = CELLS_PER_FRAME // C.cells_per_block(N_INNER, MOD)
+    tx = synth.Transmitter(N_INNER, MOD, RATE, device=device, chunk=128)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    cells = torch.empty((nframes, nblk, tx.ncell), dtype=torch.complex64,
+                        device=device)
+    sig = torch.empty((nframes, nblk, tx.ncell), dtype=torch.float32,
+                      device=device)
+    for f in range(nframes):
+        pay = torch.randint(0, 2, (nblk, tx.kp), generator=g, device=device,
+                            dtype=torch.uint8)
+        x, _ = tx.encode(pay)
+        y, s2 = synth.channel(x, ESN0[f % len(ESN0)], "rayleigh", g)
+        cells[f] = y
+        sig[f] = s2
+    return cells, sig, nblk, tx.kp
+
+
+def cpu_reference_decode(cells, sig, threads):
+    """The reference's CPU path on host cores: float32 demap (numpy, the
+    lab/m44_ldm.py:2431-2494 arithmetic) with per-cell sigma2, de-interleave,
+    the reference's compiled lab/ldpc_kernel.c (thread sub-batches, as
+    lab/m44_ldm.py:2558-2576), BCH as a packed GF(2) product
+    (lab/m9_accel.py:212-236).  Returns (#blocks BCH-clean, its)."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    from atsc3_b200 import codes as C
+    pts = C.points_for(MOD, RATE)
+    nb = C.MOD_BITS[MOD]
+    lq = C.bicm_map(N_INNER, MOD, RATE)
+    tabs = C.csr(RATE, N_INNER)
+    K = C.kldpc(RATE, N_INNER)
+    nblk = cells.shape[0]
+    with ThreadPoolExecutor(threads) as ex:
+        q = np.concatenate(list(ex.map(
+            lambda b: oracle.demap(cells[b:b + 1], pts, nb, sig[b:b + 1]),
+            range(nblk))))
+    lam = oracle.deinterleave(q, lq, N_INNER)
+    bits, conv, its, bad = oracle.flood_ref(lam, tabs, N_INNER, iters=ITERS,
+                                            alpha=ALPHA, threads=threads)
+    syn = oracle.bch_syndrome_fast(bits[:, :K], N_INNER)
+    return sum(1 for s in syn if s == 0), its
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference CPU path, rank 0 only."""
+    if rank != 0:
+        return None
+    import torch
+    from atsc3_b200 import codes as C
+    threads = os.cpu_count() or 1
+    kp = C.kpayload(RATE, N_INNER)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    nsteps = args.steps + args.warmup
+    per = min(75, max(8, threads))
+    cells, sig, nblk, _ = make_frames(nsteps, args.seed, dev)
+    cells = cells[:, :per].cpu().numpy()
+    sig = sig[:, :per].cpu().numpy()
+    times, its_all = [], []
+    for s in range(nsteps):
+        t0 = time.perf_counter()
+        _, its = cpu_reference_decode(cells[s], sig[s], threads)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+            its_all.append(its)
+    tot = sum(times)
+    value = args.steps * per * kp / tot / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value,
+            "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": config(per),
+            "cpu_baseline": {"value": value, "unit": "Mbit/s",
+                             "cores": threads, "kind": "reference",
+                             "sample": f"{per} of the 75 blocks of each step's "
+                                       f"frame; demap numpy f32, "
+                                       f"lab/ldpc_kernel.c compiled -O3 "
+                                       f"-ffp-contract=off over {threads} "
+                                       f"threads, packed BCH"},
+            "e2e": {"value": value, "unit": "Mbit/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "mean_iters": float(np.mean(np.concatenate(its_all)))}
+    return line
+
+
+def config(blocks):
+    return {"workload": "frame-scale plain decode: 64800-bit LDPC rate 6/15, "
+                        "16-NUC, 1,216,939 cells/frame -> 75 FEC blocks, "
+                        "Rayleigh |CN(0,1)| gain with per-cell sigma2, "
+                        "Es/N0 4..8 dB step 0.5 cycling per frame",
+            "code": "64800 6/15 (Type B)", "constellation": "NUC_16_6/15",
+            "blocks_per_step": blocks, "cells_per_frame": CELLS_PER_FRAME,
+            "esn0_db": ESN0, "alpha": ALPHA, "iters_max": ITERS,
+            "early_stop": "zero syndrome", "sigma2": "per cell",
+            "parallelism": "blocks sharded per GPU (no exchange)",
+            "l2": "inputs larger than L2: a distinct 14.6 MB frame per step, "
+                  "0.93 GB over 64 steps"}
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from atsc3_b200 import codes as C
+    from atsc3_b200.pipeline import FecPipeline
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    K, W = args.steps, args.warmup
+    nframes = K + W
+    cells, sig, nblk, kp = make_frames(nframes, args.seed + 1000 * rank, dev)
+    pipe = FecPipeline(N_INNER, MOD, RATE, iters=ITERS, alpha=ALPHA,
+                       cluster=args.cluster, threads=args.threads, device=dev)
+    outs = []
+    for f in range(nframes):
+        outs.append({"conv": torch.empty(nblk, dtype=torch.uint8, device=dev),
+                     "its": torch.empty(nblk, dtype=torch.int32, device=dev),
+                     "bad": torch.empty(nblk, dtype=torch.int32, device=dev),
+                     "ok": torch.empty(nblk, dtype=torch.uint8, device=dev),
+                     "syn": torch.empty((nblk, 6), dtype=torch.int32, device=dev),
+                     "payload": torch.empty((nblk, kp // 8), dtype=torch.uint8,
+                                            device=dev)})
+    for f in range(W):
+        pipe.decode(cells[f], sig[f], out=outs[f])
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream(dev)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+          for _ in range(K)]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk = Clocks(local_rank) if rank == 0 else None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clk:
+        clk.start()
+    e0.record(st)
+    for s in range(K):
+        f = W + s
+        E = ev[s]
+        E[0].record(st)
+        ws = pipe._buffers(nblk)
+        from atsc3_b200 import demap as DM, ldpc as LDPC, bch as BCH
+        DM.demap(cells[f], MOD, RATE, sigma2=sig[f], n=N_INNER, out=ws["lam"])
+        E[1].record(st)
+        o = dict(ws)
+        o.update(outs[f])
+        LDPC.decode_flood(pipe.plan, ws["lam"], iters=ITERS, alpha=ALPHA,
+                          want_bits=False, want_hard=True,
+                          threads=args.threads, out=o)
+        E[2].record(st)
+        BCH.bch_check(ws["hard"], pipe.kldpc, N_INNER, kp, out=o)
+        E[3].record(st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop() if clk else None
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    stage = np.array([[E[0].elapsed_time(E[1]), E[1].elapsed_time(E[2]),
+                       E[2].elapsed_time(E[3])] for E in ev])
+    # results of the timed frames
+    conv = torch.stack([outs[W + s]["conv"] for s in range(K)]).cpu().numpy()
+    its = torch.stack([outs[W + s]["its"] for s in range(K)]).cpu().numpy()
+    ok = torch.stack([outs[W + s]["ok"] for s in range(K)]).cpu().numpy()
+    total_bits = world * K * nblk * kp
+    value = total_bits / (ms / 1e3) / 1e6
+    # ---- e2e: host buffers through the public API -------------------------
+    e2e = run_e2e(pipe, cells, sig, W, K, nblk, kp, dev, world)
+    # ---- roofline of the dominant kernel (the LDPC decoder) --------------
+    ldpc_ms = float(stage[:, 1].mean())
+    b_ldpc = nblk * (4 * N_INNER + N_INNER // 8 + 9)
+    hbm, peak_kind = peaks()
+    achieved = b_ldpc / (ldpc_ms / 1e3) / 1e9
+    fer = {}
+    for s in range(K):
+        e = ESN0[(W + s) % len(ESN0)]
+        d = fer.setdefault(f"{e:.1f}", [0, 0])
+        d[0] += int((ok[s] == 0).sum())
+        d[1] += nblk
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mbit/s",
+                "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K,
+                "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config(nblk),
+                "roofline": {"bound": "hbm", "achieved": achieved,
+                             "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": None,
+                             "kernel": "ldpc_flood_kernel<float,16,false>",
+                             "peak_kind": peak_kind,
+                             "bytes_per_launch": b_ldpc,
+                             "ms_per_launch": ldpc_ms},
+                "stage_ms": {"demap": float(stage[:, 0].mean()),
+                             "ldpc": ldpc_ms,
+                             "bch": float(stage[:, 2].mean())},
+                "gpu_launches": 3 * K,
+                "clocks": clocks, "e2e": e2e,
+                "mean_iters": float(its.mean()),
+                "converged_frac": float(conv.mean()),
+                "fer_bch_by_esn0": {k: v[0] / v[1] for k, v in sorted(fer.items())},
+                "plan": pipe.plan.info}
+    return line
+
+
+def run_e2e(pipe, cells, sig, W, K, nblk, kp, dev, world):
+    """Same metric through FecPipeline with pinned host buffers: H2D of the
+    step's cells + sigma2, decode, D2H of payload bytes and flags."""
+    import torch
+    nh = min(8, K)
+    hc = [cells[W + s].cpu().pin_memory() for s in range(nh)]
+    hs = [sig[W + s].cpu().pin_memory() for s in range(nh)]
+    hp = torch.empty((K, nblk, kp // 8), dtype=torch.uint8).pin_memory()
+    hf = torch.empty((K, 4, nblk), dtype=torch.int32).pin_memory()
+    dc = torch.empty_like(cells[0])
+    ds = torch.empty_like(sig[0])
+    st = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    flags = torch.empty((4, nblk), dtype=torch.int32, device=dev)
+    for s in range(2):   # warm the pinned path
+        dc.copy_(hc[s % nh], non_blocking=True)
+        ds.copy_(hs[s % nh], non_blocking=True)
+        pipe.decode(dc, ds)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for s in range(K):
+        dc.copy_(hc[s % nh], non_blocking=True)
+        ds.copy_(hs[s % nh], non_blocking=True)
+        ws = pipe.decode(dc, ds)
+        flags[0].copy_(ws["conv"])
+        flags[1].copy_(ws["its"])
+        flags[2].copy_(ws["bad"])
+        flags[3].copy_(ws["ok"])
+        hp[s].copy_(ws["payload"], non_blocking=True)
+        hf[s].copy_(flags, non_blocking=True)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    h2d = nblk * pipe.ncell * (8 + 4)
+    d2h = nblk * (kp // 8) + 4 * nblk * 4
+    return {"value": world * K * nblk * kp / (ms / 1e3) / 1e6, "unit": "Mbit/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": ms / K}
+
+
+def cpu_baseline(args, nblk_per_esn0=6):
+    """Reference CPU path on a bounded sample: nblk_per_esn0 blocks at each
+    of the 9 Es/N0 points (same mix as the GPU steps)."""
+    import torch
+    from atsc3_b200 import codes as C
+    threads = os.cpu_count() or 1
+    kp = C.kpayload(RATE, N_INNER)
+    cells, sig, nblk, _ = make_frames(len(ESN0), args.seed + 7,
+                                      "cuda" if torch.cuda.is_available() else "cpu")
+    c = cells[:, :nblk_per_esn0].reshape(-1, cells.shape[-1]).cpu().numpy()
+    s = sig[:, :nblk_per_esn0].reshape(-1, sig.shape[-1]).cpu().numpy()
+    t0 = time.perf_counter()
+    nok, its = cpu_reference_decode(c, s, threads)
+    dt = time.perf_counter() - t0
+    return {"value": c.shape[0] * kp / dt / 1e6, "unit": "Mbit/s",
+            "cores": threads, "kind": "reference",
+            "sample": f"{c.shape[0]} blocks ({nblk_per_esn0} per Es/N0 point "
+                      f"4..8 dB), demap numpy f32 + lab/ldpc_kernel.c "
+                      f"(-O3 -ffp-contract=off) over {threads} threads + "
+                      f"packed BCH; {dt:.1f} s wall, mean its "
+                      f"{float(np.mean(its)):.1f}"}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cluster", type=int, default=0)
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        a.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        line = run_reference(a, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    line = run_gpu(a, rank, world, local_rank)
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(a)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,171 @@
+/* atsc3_fec.h -- C ABI of the B200 (sm_100a) ATSC 3.0 FEC back end.
+ *
+ * One shared library, libatsc3_fec.so, exports everything below.  Plain C
+ * types only: pointers, sizes, and a cudaStream_t passed as void*.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in for the Felbs/atsc3 compiled min-sum kernel
+ *     (lab/ldpc_kernel.c:52-146, bound by ctypes in lab/m3_ldpc.py:425-456).
+ *     Same symbol names, same argument order and meaning, HOST pointers.
+ *
+ *  2. Device-pointer entry points used by the Python host layer
+ *     (atsc3_b200/) for the batched GPU path.  They replace the torch-eager
+ *     GPU code of lab/m9_gpu.py (GpuMinSum.decode :138-220, GpuBicm.demap
+ *     :301-316), the numpy demappers lab/m16_demap_fast.py:80-119 and
+ *     lab/m44_ldm.py:2431-2494, and the BCH helpers lab/m9_accel.py:197-236.
+ *     All pointers are device pointers unless stated; every launch goes to
+ *     the given stream and nothing synchronises unless stated.
+ *
+ * Return codes: 0 ok; -1 a check degree above ATSC3_MAX_ROW_DEG (the
+ * reference kernel's only error, lab/ldpc_kernel.c:78-80); -2 CUDA error;
+ * -3 invalid argument; -4 configuration the kernels do not support (e.g.
+ * shared memory needed above the device limit).  atsc3_last_error() returns
+ * a message for the last failure on the calling thread.
+ */
+#ifndef ATSC3_FEC_H
+#define ATSC3_FEC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATSC3_MAX_ROW_DEG 128
+
+/* ---- 1. reference drop-in ------------------------------------------------ */
+
+/* Returns 1.  Replaces ldpc_kernel_abi (lab/ldpc_kernel.c:52). */
+int32_t ldpc_kernel_abi(void);
+
+/* Replaces ldpc_minsum_f32 (lab/ldpc_kernel.c:65-146): flooding normalised
+ * min-sum in float32, syndrome checked before each update, first-minimum tie
+ * rule, variable sums in vedge order.  Bit-identical outputs (bits, conv,
+ * its, bad).  All pointers are HOST pointers, C-contiguous.  The decode runs
+ * on the GPU on a per-thread stream and the call returns when the outputs
+ * are written.  `work` is accepted for ABI compatibility and not touched.
+ * Device copies of the CSR tables are cached by content.  Thread-safe.
+ * Returns 0, -1 (degree > 128, nothing written), -2 (CUDA error), -3. */
+int32_t ldpc_minsum_f32(const float *llr, int32_t nblk, int32_t n,
+                        int32_t nc, int32_t nedges,
+                        const int32_t *cptr, const int32_t *cidx,
+                        const int32_t *vptr, const int32_t *vedge,
+                        int32_t iters, float alpha,
+                        uint8_t *bits, uint8_t *conv, int32_t *its,
+                        int32_t *bad, float *work);
+
+/* ---- 2. device-pointer entry points --------------------------------------- */
+
+const char *atsc3_last_error(void);
+
+/* Library / device facts: info[0] = SM count, [1] = max dynamic shared
+ * memory per block (bytes), [2] = compute capability major*10+minor,
+ * [3] = library version. */
+int32_t atsc3_device_info(int32_t *info);
+
+typedef struct atsc3_ldpc_plan atsc3_ldpc_plan;
+
+/* Build the device tables of one LDPC code for the flooding decoder.
+ * cptr/cidx/vptr/vedge: HOST CSR tables (lab/m3_ldpc.py:459-482 layout).
+ * dtype: 0 = float32 messages, 1 = float64 messages.
+ * cluster: thread-block cluster size (1, 2, 4, 8, 16), 0 = smallest that
+ * fits the per-codeword state in distributed shared memory.
+ * Replaces GpuMinSum.__init__ (lab/m9_gpu.py:95-135). */
+int32_t atsc3_ldpc_plan_create(const int32_t *cptr, const int32_t *cidx,
+                               const int32_t *vptr, const int32_t *vedge,
+                               int32_t n, int32_t nc, int32_t nedges,
+                               int32_t dtype, int32_t cluster,
+                               atsc3_ldpc_plan **out);
+void atsc3_ldpc_plan_destroy(atsc3_ldpc_plan *plan);
+
+/* info[0]=n [1]=nc [2]=nedges [3]=cluster [4]=shared bytes per CTA
+ * [5]=record bytes [6]=max row degree [7]=max column degree
+ * [8]=table bytes on device [9]=dtype */
+int32_t atsc3_ldpc_plan_info(const atsc3_ldpc_plan *plan, int64_t *info);
+
+/* Host-only table build used by the CPU tests: fills the check-phase and
+ * variable-phase sliced-ELL tables for a given cluster size without touching
+ * a GPU.  Call with null outputs to get the sizes in sizes[0..3] (entries of
+ * cent, cslice, vent, vslice); sizes[4] = checks per CTA, sizes[5] = log2 of
+ * variables per CTA. */
+int32_t atsc3_ldpc_tables_host(const int32_t *cptr, const int32_t *cidx,
+                               const int32_t *vptr, const int32_t *vedge,
+                               int32_t n, int32_t nc, int32_t nedges,
+                               int32_t cluster, int64_t *sizes,
+                               uint16_t *cent, int32_t *cslice,
+                               uint32_t *vent, int32_t *vslice);
+
+/* Flooding normalised min-sum over nblk codewords, one thread-block cluster
+ * per codeword, all iterations in one launch, per-codeword early stop.
+ * llr: device (nblk, ld_llr) float32 or float64 (the plan's dtype).
+ * semantics 0: lab/ldpc_kernel.c (syndrome before each update, its may be 0,
+ *   variable sum from +0 then added to the channel LLR);
+ * semantics 1: lab/m9_gpu.py:168-211 / lab/m3_ldpc.py:560-630 float64 path
+ *   (update first, its >= 1, variable sum accumulated onto the channel LLR).
+ * bits (nullable): (nblk, ld_bits) uint8 hard decisions, 1 = negative LLR.
+ * hard (nullable): (nblk, ld_hard) packed hard decisions, n/8 bytes, MSB
+ *   first in each byte (numpy packbits order).
+ * conv/its/bad: per codeword, as lab/ldpc_kernel.c:62.
+ * threads: CTA size (0 = 1024). */
+int32_t atsc3_ldpc_decode_flood(const atsc3_ldpc_plan *plan, const void *llr,
+                                int64_t ld_llr, int32_t nblk, int32_t iters,
+                                double alpha, int32_t semantics,
+                                uint8_t *bits, int64_t ld_bits,
+                                uint8_t *hard, int64_t ld_hard,
+                                uint8_t *conv, int32_t *its, int32_t *bad,
+                                int32_t threads, void *stream);
+
+/* NUC max-log soft demapper with the bit de-interleaver in its epilogue.
+ * cells: (nblk, ld_cells) complex64 as interleaved float pairs.
+ * pts: 3*M floats: Re p, Im p, |p|^2 (float32, |p|^2 rounded once from
+ *   float64), M = 2^nbits, label order (y0 = MSB).
+ * The point metric is |p|^2 - 2(Re z Re p + Im z Im p) in float32 in the
+ * operation order of lab/m44_ldm.py:2431-2451, per-bit minima, then
+ * (min_{b=1} - min_{b=0}) / sigma2 with IEEE division.
+ * sigma_mode 0: one sigma2 for all cells (sigma2_scalar);
+ *            1: one per cell, sigma2 = device (nblk, ld_sigma) float32
+ *               (the lab/m9_fast.py:1096-1115 convention);
+ *            2: one per block row, sigma2 = device (nblk,) float32;
+ *            3: raw minima difference, no division.
+ * lam_of_q (nullable, device int32 (ncell*nbits)): write the LLR of q_j to
+ *   out[lam_of_q[j]] (codeword order); null writes q order.
+ * out: (nblk, ld_out) float32. */
+int32_t atsc3_demap(const float *cells, int64_t ld_cells, int32_t nblk,
+                    int32_t ncell, const float *pts, int32_t nbits,
+                    int32_t sigma_mode, const float *sigma2, int64_t ld_sigma,
+                    float sigma2_scalar, const int32_t *lam_of_q, float *out,
+                    int64_t ld_out, void *stream);
+
+/* Per-row noise estimate of lab/m44_ldm.py:2480 / lab/m16_demap_fast.py:104:
+ * sigma2[b] = max(mean_cells(|z|^2 + min_p metric), 1e-9), accumulated in
+ * float64 (tolerance parity, not bit parity, with the numpy float32 mean). */
+int32_t atsc3_demap_row_sigma2(const float *cells, int64_t ld_cells,
+                               int32_t nblk, int32_t ncell, const float *pts,
+                               int32_t nbits, float *sigma2, void *stream);
+
+/* BCH zero-syndrome check (A/322 6.1.2.1) plus descramble of the payload.
+ * hard: (nblk, ld_hard) packed hard decisions (as atsc3_ldpc_decode_flood
+ *   writes them); the first kldpc bits are the BCH codeword.
+ * rtab: device (kldpc, 6) uint32, row pos = x^(kldpc-1-pos) mod g(x).
+ * syn: (nblk, 6) uint32 remainder words (word w = coefficients 32w..).
+ * ok: (nblk,) uint8, 1 when the syndrome is zero.
+ * scr (nullable): kpayload/8 scrambling bytes; payload (nullable):
+ *   (nblk, ld_payload) bytes = hard[:kpayload/8] XOR scr (descrambled
+ *   Baseband Packet, lab/m9_fast.py:942-949). */
+int32_t atsc3_bch_check(const uint8_t *hard, int64_t ld_hard, int32_t nblk,
+                        int32_t kldpc, const uint32_t *rtab, uint32_t *syn,
+                        uint8_t *ok, const uint8_t *scr, int32_t kpayload,
+                        uint8_t *payload, int64_t ld_payload, void *stream);
+
+/* Same syndrome from one byte per bit (lab/m9_accel.py:212-236 input). */
+int32_t atsc3_bch_syndrome_bits(const uint8_t *bits, int64_t ld_bits,
+                                int32_t nblk, int32_t kldpc,
+                                const uint32_t *rtab, uint32_t *syn,
+                                void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATSC3_FEC_H */

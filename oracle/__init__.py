@@ -1,0 +1,386 @@
+"""The parity oracle -- TEST INFRASTRUCTURE ONLY.
+
+A CPU restatement of the Felbs/atsc3 FEC back end, used as the checker by
+``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py``.  The product (``atsc3_b200``) never imports it and has no CPU
+fallback.
+
+Pinning: every function here is checked by ``tests/test_oracle.py`` against
+golden vectors produced by the reference itself (``tests/golden/``, made by
+``tests/golden/make_golden.py``), and the C decoder is additionally checked
+against the reference's own ``lab/ldpc_kernel.c`` compiled into
+``oracle/_ref/`` by ``oracle/build.py`` wherever that file is present.
+
+Contents (reference file:line each restates):
+* ``transmit`` / ``ldpc_encode`` / ``bch_encode`` / ``map_cells`` --
+  lab/m6_bicm.py:367-373 (``PlpChain.encode``), lab/m3_ldpc.py:119-159
+  (A/322 6.1.3 encoder), lab/m6_bicm.py:283-290, :228-236.
+* ``demap`` -- lab/m44_ldm.py:2431-2494 (float32 point metric and per-bit
+  minima), with a supplied scalar or per-cell sigma2 (lab/m9_fast.py:
+  1096-1115) or the per-row estimate.
+* ``bch_syndrome`` -- lab/m6_bicm.py:269-280 (polynomial remainder).
+* ``flood`` -- ``ldpc_oracle.c`` (lab/ldpc_kernel.c semantics and the
+  float64 / torch semantics); ``flood_ref`` -- the reference kernel itself.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from atsc3_b200 import codes as C          # noqa: E402  (tables + H, data only)
+
+_LIBS = {}
+
+
+def _load(path, name):
+    if name not in _LIBS:
+        if not os.path.exists(path):
+            from . import build as _b
+            _b.build()
+        _LIBS[name] = ctypes.CDLL(path)
+    return _LIBS[name]
+
+
+def oracle_lib():
+    from . import build as _b
+    L = _load(_b.ORACLE_SO, "oracle")
+    vp, i32 = ctypes.c_void_p, ctypes.c_int32
+    L.oracle_flood_f32.restype = i32
+    L.oracle_flood_f32.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp, i32,
+                                   ctypes.c_float, i32, vp, vp, vp, vp]
+    L.oracle_flood_f64.restype = i32
+    L.oracle_flood_f64.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp, i32,
+                                   ctypes.c_double, i32, vp, vp, vp, vp]
+    if hasattr(L, "oracle_layered_f32"):
+        L.oracle_layered_f32.restype = i32
+    return L
+
+
+def ref_lib():
+    """The reference's own compiled kernel, or None where it was not built."""
+    from . import build as _b
+    if not os.path.exists(_b.REF_SO):
+        try:
+            _b.build()
+        except Exception:
+            return None
+        if not os.path.exists(_b.REF_SO):
+            return None
+    L = _load(_b.REF_SO, "ref")
+    vp, i32 = ctypes.c_void_p, ctypes.c_int32
+    L.ldpc_minsum_f32.restype = i32
+    L.ldpc_minsum_f32.argtypes = [vp, i32, i32, i32, i32, vp, vp, vp, vp, i32,
+                                  ctypes.c_float, vp, vp, vp, vp, vp]
+    return L
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+def flood(llr, tables, n, iters=50, alpha=0.75, semantics=0, dtype=np.float32):
+    """Oracle flooding decode: (bits, conv bool, its, bad)."""
+    cptr, cidx, vptr, vedge = [np.ascontiguousarray(t, np.int32) for t in tables]
+    llr = np.ascontiguousarray(llr, dtype)
+    nblk = llr.shape[0]
+    bits = np.zeros((nblk, n), np.uint8)
+    conv = np.zeros(nblk, np.uint8)
+    its = np.zeros(nblk, np.int32)
+    bad = np.zeros(nblk, np.int32)
+    L = oracle_lib()
+    fn = L.oracle_flood_f32 if dtype == np.float32 else L.oracle_flood_f64
+    rc = fn(_p(llr), nblk, n, len(cptr) - 1, _p(cptr), _p(cidx), _p(vptr),
+            _p(vedge), int(iters), float(alpha), int(semantics), _p(bits),
+            _p(conv), _p(its), _p(bad))
+    if rc != 0:
+        raise RuntimeError(f"oracle decode returned {rc}")
+    return bits, conv.astype(bool), its, bad
+
+
+def flood_ref(llr, tables, n, iters=50, alpha=0.75, threads=1):
+    """The reference kernel (lab/ldpc_kernel.c) itself, sub-batched over
+    `threads` host threads the way lab/m44_ldm.py:2558-2576 drives it."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference kernel not built here")
+    cptr, cidx, vptr, vedge = [np.ascontiguousarray(t, np.int32) for t in tables]
+    llr = np.ascontiguousarray(llr, np.float32)
+    nblk = llr.shape[0]
+    ne = len(cidx)
+    bits = np.zeros((nblk, n), np.uint8)
+    conv = np.zeros(nblk, np.uint8)
+    its = np.zeros(nblk, np.int32)
+    bad = np.zeros(nblk, np.int32)
+
+    def one(lo, hi):
+        work = np.empty(n + ne, np.float32)
+        rc = L.ldpc_minsum_f32(
+            llr[lo:].ctypes.data, hi - lo, n, len(cptr) - 1, ne, _p(cptr),
+            _p(cidx), _p(vptr), _p(vedge), int(iters), float(alpha),
+            bits[lo:].ctypes.data, conv[lo:].ctypes.data,
+            its[lo:].ctypes.data, bad[lo:].ctypes.data, _p(work))
+        if rc != 0:
+            raise RuntimeError(f"reference kernel returned {rc}")
+
+    threads = max(1, min(threads, nblk))
+    if threads == 1:
+        one(0, nblk)
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        step = (nblk + threads - 1) // threads
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda i: one(i * step, min(nblk, (i + 1) * step)),
+                        range(threads)))
+    return bits, conv.astype(bool), its, bad
+
+
+# ---------------------------------------------------------------------------
+# transmitter (synthetic inputs)
+# ---------------------------------------------------------------------------
+
+def _addr(x, mm, M1, M2, Q1, Q2):
+    # A/322 6.1.3.1 step ii, lab/m3_ldpc.py:63-66
+    x = np.asarray(x, np.int64)
+    mm = np.asarray(mm, np.int64)
+    return np.where(x < M1, (x + mm * Q1) % max(M1, 1),
+                    M1 + (x - M1 + mm * Q2) % M2)
+
+
+def _pi_of(M1, M2, Q1, Q2, K):
+    # accumulator -> codeword index (lab/m3_ldpc.py:69-82, "standard")
+    a = np.arange(M1 + M2, dtype=np.int64)
+    s1, t1 = np.divmod(a, max(Q1, 1))
+    s2, t2 = np.divmod(a - M1, Q2)
+    return np.where(a < M1, K + 360 * t1 + s1, K + M1 + 360 * t2 + s2)
+
+
+def _accumulate(bits, rowptr, addr, row0, M1, M2, Q1, Q2, M):
+    """XOR of the table addresses hit by the set bits (lab/m3_ldpc.py:
+    129-135), vectorised over all bits of all blocks: (nblk, nbits) ->
+    (nblk, M)."""
+    nb = bits.shape[1]
+    bit = np.arange(nb)
+    row = row0 + bit // 360
+    cnt = (rowptr[row + 1] - rowptr[row]).astype(np.int64)
+    rep = np.repeat(bit, cnt)
+    first = np.repeat(rowptr[row].astype(np.int64), cnt)
+    within = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    acc = _addr(addr[first + within], rep % 360, M1, M2, Q1, Q2)
+    out = np.zeros((bits.shape[0], M), np.uint8)
+    for b in range(bits.shape[0]):
+        sel = bits[b, rep].astype(bool)
+        out[b] = (np.bincount(acc[sel], minlength=M) & 1).astype(np.uint8)
+    return out
+
+
+def ldpc_encode(s, rate, n):
+    """(nblk, K) info bits -> (nblk, n) codewords, A/322 6.1.3.1 / 6.1.3.2."""
+    s = np.atleast_2d(np.asarray(s, np.uint8))
+    typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+    rowptr, addr = C.address_rows(rate, n)
+    M = M1 + M2
+    pi = _pi_of(M1, M2, Q1, Q2, K)
+    lam = np.zeros((s.shape[0], n), np.uint8)
+    lam[:, :K] = s
+    p = _accumulate(s, rowptr, addr, 0, M1, M2, Q1, Q2, M)
+    if typ == "A":
+        p[:, :M1] = np.bitwise_xor.accumulate(p[:, :M1], axis=1)
+        lam[:, pi[:M1]] = p[:, :M1]
+        fb = _accumulate(lam[:, K:K + M1], rowptr, addr, K // 360, M1, M2,
+                         Q1, Q2, M)
+        p ^= fb
+        lam[:, pi[M1:]] = p[:, M1:]
+    else:
+        p = np.bitwise_xor.accumulate(p, axis=1)
+        lam[:, pi] = p
+    return lam
+
+
+def bch_encode(info, n):
+    """(nblk, K_ldpc - Mouter) -> (nblk, K_ldpc) systematic BCH codewords
+    (lab/m6_bicm.py:283-290)."""
+    info = np.atleast_2d(np.asarray(info, np.uint8))
+    g = C.bch_generator(n)
+    deg = C.MOUTER[n]
+    out = np.zeros((info.shape[0], info.shape[1] + deg), np.uint8)
+    out[:, :info.shape[1]] = info
+    for b in range(info.shape[0]):
+        v = int.from_bytes(np.packbits(info[b]).tobytes(), "big") >> (
+            (-info.shape[1]) % 8)
+        r = _poly_mod(v << deg, g, deg)
+        out[b, info.shape[1]:] = [(r >> (deg - 1 - i)) & 1 for i in range(deg)]
+    return out
+
+
+def _poly_mod(v, g, gd):
+    # lab/m6_bicm.py:269-273
+    while v and v.bit_length() - 1 >= gd:
+        v ^= g << ((v.bit_length() - 1) - gd)
+    return v
+
+
+def bch_syndrome(bits, n):
+    """Python-int syndrome of each row (0 = clean), lab/m6_bicm.py:276-280."""
+    bits = np.atleast_2d(np.asarray(bits, np.uint8))
+    g = C.bch_generator(n)
+    deg = C.MOUTER[n]
+    out = []
+    for row in bits:
+        v = int.from_bytes(np.packbits(row).tobytes(), "big") >> ((-len(row)) % 8)
+        out.append(_poly_mod(v, g, deg))
+    return out
+
+
+def map_cells(q, pts, nb):
+    """(nblk, ncell*nb) bits in q order -> complex cells (lab/m6_bicm.py:228)."""
+    q = np.asarray(q, np.uint8)
+    b = q.reshape(q.shape[0], -1, nb)
+    k = np.zeros(b.shape[:2], np.int64)
+    for i in range(nb):
+        k |= b[:, :, i].astype(np.int64) << (nb - 1 - i)
+    return np.asarray(pts)[k]
+
+
+def transmit(payload, n, mod, rate, pts=None):
+    """PlpChain.encode for a batch: payload bits -> complex128 cells."""
+    payload = np.atleast_2d(np.asarray(payload, np.uint8))
+    kp = payload.shape[1]
+    scr = payload ^ C.scrambler_sequence(kp)[None, :]
+    nouter = bch_encode(scr, n)
+    cw = ldpc_encode(nouter, rate, n)
+    q = cw[:, C.bicm_map(n, mod, rate)]
+    pts = C.alphabet(mod, rate) if pts is None else pts
+    return map_cells(q, pts, C.MOD_BITS[mod]), cw
+
+
+# ---------------------------------------------------------------------------
+# demapper
+# ---------------------------------------------------------------------------
+
+def point_metric(zr, zi, pr, pi, p2):
+    # lab/m44_ldm.py:2447-2451, float32, same operation order
+    q = zr[:, None] * pr[None, :]
+    q += zi[:, None] * pi[None, :]
+    q *= np.float32(-2.0)
+    q += p2[None, :]
+    return q
+
+
+def demap(cells2d, pts, nb, sigma2=None):
+    """(nblk, ncell) complex -> (nblk, ncell*nb) float32 LLRs in q order.
+
+    sigma2 None: per-row estimate (lab/m44_ldm.py:2480); a scalar; or a
+    (nblk, ncell) per-cell array (divide after the minima, lab/m9_fast.py:
+    1114)."""
+    cells2d = np.atleast_2d(cells2d)
+    nblk, ncell = cells2d.shape
+    pr, pi, p2 = C.point_tables_f32(pts)
+    zr = np.asarray(cells2d.real, np.float32)
+    zi = np.asarray(cells2d.imag, np.float32)
+    q = point_metric(zr.ravel(), zi.ravel(), pr, pi, p2).reshape(nblk, ncell, -1)
+    if sigma2 is None:
+        z2 = zr * zr + zi * zi
+        s2 = np.maximum((z2 + q.min(2)).mean(1), 1e-9)[:, None]
+    elif np.ndim(sigma2) == 0:
+        s2 = np.float32(sigma2)
+    else:
+        s2 = np.asarray(sigma2, np.float32).reshape(nblk, ncell)
+    qr = q.reshape(nblk, ncell, *([2] * nb))
+    sub = tuple(range(2, 2 + nb - 1))
+    out = np.empty((nblk, ncell, nb), np.float32)
+    head = (slice(None), slice(None))
+    for i in range(nb):
+        a = qr[head + (slice(None),) * i + (1,)].min(axis=sub)
+        b = qr[head + (slice(None),) * i + (0,)].min(axis=sub)
+        out[:, :, i] = (a - b) / s2
+    return out.reshape(nblk, ncell * nb)
+
+
+def deinterleave(q2d, lam_of_q, n):
+    lam = np.empty((q2d.shape[0], n), np.float32)
+    lam[:, lam_of_q] = q2d
+    return lam
+
+
+def awgn(cells, esn0_db, rng):
+    """complex64 cells + complex Gaussian noise of variance N0 = 10^(-Es/N0/10)
+    (unit-power alphabet): the draw order of lab/m6_bicm.py:436-438."""
+    n0 = 10 ** (-esn0_db / 10.0)
+    nz = (rng.standard_normal(cells.shape)
+          + 1j * rng.standard_normal(cells.shape)) / np.sqrt(2)
+    return (cells + nz * np.sqrt(n0)).astype(np.complex64), n0
+
+
+def synth_case(tx, nblk, kpay, ncell, esn0_db, channel, seed):
+    """The seeded synthetic-case procedure shared by the golden generator
+    (with the reference transmitter) and the tests (with ``transmit``):
+
+    payload bits (one rng.integers draw for the batch) -> tx -> complex64
+    cells through AWGN (scalar sigma2 = N0) or a per-cell Rayleigh gain
+    h = |CN(0,1)| equalised away, y = (h x + n)/h, sigma2_cell = N0/h^2.
+    Returns (payload, cells complex64 (nblk, ncell), sigma2)."""
+    rng = np.random.default_rng(seed)
+    pay = rng.integers(0, 2, (nblk, kpay), dtype=np.uint8)
+    x = np.asarray(tx(pay), np.complex128).reshape(nblk, ncell)
+    n0 = 10 ** (-esn0_db / 10.0)
+    if channel == "awgn":
+        nz = (rng.standard_normal((nblk, ncell))
+              + 1j * rng.standard_normal((nblk, ncell))) / np.sqrt(2)
+        y = (x + nz * np.sqrt(n0)).astype(np.complex64)
+        return pay, y, np.float32(n0)
+    if channel == "rayleigh":
+        h = np.abs(rng.standard_normal((nblk, ncell))
+                   + 1j * rng.standard_normal((nblk, ncell))) / np.sqrt(2)
+        nz = (rng.standard_normal((nblk, ncell))
+              + 1j * rng.standard_normal((nblk, ncell))) / np.sqrt(2)
+        y = ((h * x + nz * np.sqrt(n0)) / h).astype(np.complex64)
+        return pay, y, (n0 / h ** 2).astype(np.float32)
+    raise ValueError(channel)
+
+
+_BCH_MASKS = {}
+
+
+def _bch_masks(k, n):
+    """Packed (deg, k/64) uint64 masks: bit i of row j set iff x^(k-1-i)
+    mod g has x^j -- the table of lab/m9_accel.py:169-194."""
+    key = (k, n)
+    if key not in _BCH_MASKS:
+        R = C.bch_remainder_table(k, n)                      # (k, 6) u32
+        deg = C.MOUTER[n]
+        cols = np.unpackbits(R.view(np.uint8), axis=1,
+                             bitorder="little")[:, :deg]     # (k, deg)
+        pad = (-k) % 64
+        if pad:
+            cols = np.concatenate([cols, np.zeros((pad, deg), np.uint8)])
+        masks = np.ascontiguousarray(np.packbits(cols.T, axis=1)).view(np.uint64)
+        _BCH_MASKS[key] = (masks, pad)
+    return _BCH_MASKS[key]
+
+
+def bch_syndrome_fast(bits2d, n):
+    """Batch syndromes as a packed GF(2) matrix product (the evaluation of
+    lab/m9_accel.py:212-236); returns a list of Python ints."""
+    a = np.atleast_2d(np.asarray(bits2d, np.uint8))
+    nblk, k = a.shape
+    masks, pad = _bch_masks(k, n)
+    if pad:
+        a = np.concatenate([a, np.zeros((nblk, pad), np.uint8)], axis=1)
+    v = np.ascontiguousarray(np.packbits(a, axis=1)).view(np.uint64)
+    par = (np.bitwise_count(v[:, None, :] & masks[None, :, :]).sum(2)
+           & 1).astype(np.uint8)                              # (nblk, deg)
+    out = []
+    for row in par:
+        x = 0
+        for j in range(len(row) - 1, -1, -1):
+            x = (x << 1) | int(row[j])
+        out.append(x)
+    return out

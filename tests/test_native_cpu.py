@@ -1,0 +1,117 @@
+"""libatsc3_fec.so on the CPU: it loads, exports every symbol the header
+declares, and its host-side table build encodes the CSR tables exactly.
+No CUDA call is made."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from atsc3_b200 import codes as C
+from atsc3_b200 import native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "atsc3_fec.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b([a-z_0-9]+)\s*\(", txt)) - {"if"})
+
+
+def test_library_exports_every_declared_symbol():
+    L = N.lib()
+    syms = header_symbols()
+    assert "ldpc_minsum_f32" in syms and "ldpc_kernel_abi" in syms
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) <= set(N.SIGNATURES)
+    assert L.ldpc_kernel_abi() == 1
+
+
+def host_tables(rate, n, cluster):
+    tabs = [np.ascontiguousarray(t, np.int32) for t in C.csr(rate, n)]
+    nc = len(tabs[0]) - 1
+    ne = len(tabs[1])
+    sizes = np.zeros(6, np.int64)
+    args = [t.ctypes.data for t in tabs] + [n, nc, ne, cluster]
+    N.call("atsc3_ldpc_tables_host", *args, sizes.ctypes.data, None, None,
+           None, None)
+    cent = np.zeros(sizes[0], np.uint16)
+    cs = np.zeros(sizes[1], np.int32)
+    vent = np.zeros(sizes[2], np.uint32)
+    vs = np.zeros(sizes[3], np.int32)
+    N.call("atsc3_ldpc_tables_host", *args, sizes.ctypes.data,
+           cent.ctypes.data, cs.ctypes.data, vent.ctypes.data, vs.ctypes.data)
+    return tabs, cent, cs, vent, vs, int(sizes[4]), int(sizes[5])
+
+
+@pytest.mark.parametrize("rate,n,cluster", [("11/15", 16200, 1),
+                                            ("6/15", 64800, 4),
+                                            ("7/15", 64800, 8),
+                                            ("2/15", 64800, 16)])
+def test_host_tables_encode_csr(rate, n, cluster):
+    (cptr, cidx, vptr, vedge), cent, cs, vent, vs, ncp, nvlog2 = \
+        host_tables(rate, n, cluster)
+    nc = len(cptr) - 1
+    assert ncp % 32 == 0 and ncp * cluster >= nc
+    assert (1 << nvlog2) * cluster >= n
+    deg = np.diff(cptr)
+    for s in range(len(cs) - 1):
+        dm = cs[s + 1] - cs[s]
+        blk = cent[cs[s] * 32:(cs[s] + dm) * 32].reshape(dm, 32)
+        for l in range(32):
+            c = 32 * s + l
+            col = blk[:, l]
+            if c >= nc:
+                assert (col == 0xFFFF).all()
+                continue
+            assert np.array_equal(col[:deg[c]], cidx[cptr[c]:cptr[c + 1]])
+            assert (col[deg[c]:] == 0xFFFF).all()
+    vdeg = np.diff(vptr)
+    for s in range(len(vs) - 1):
+        dm = vs[s + 1] - vs[s]
+        blk = vent[vs[s] * 32:(vs[s] + dm) * 32].reshape(dm, 32)
+        for l in range(32):
+            i = 32 * s + l
+            col = blk[:, l]
+            if i >= n:
+                assert (col == 0xFFFFFFFF).all()
+                continue
+            e = col[:vdeg[i]]
+            chk = (e >> 16 & 15).astype(np.int64) * ncp + (e & 0xFFFF)
+            pos = (e >> 20).astype(np.int64)
+            assert np.array_equal(cptr[chk] + pos, vedge[vptr[i]:vptr[i + 1]])
+            assert (col[vdeg[i]:] == 0xFFFFFFFF).all()
+
+
+def test_host_tables_reject_bad_input():
+    tabs = [np.ascontiguousarray(t, np.int32).copy()
+            for t in C.csr("11/15", 16200)]
+    nc, ne = len(tabs[0]) - 1, len(tabs[1])
+    sizes = np.zeros(6, np.int64)
+
+    def rc(t, cluster=1):
+        return N.lib().atsc3_ldpc_tables_host(
+            *[a.ctypes.data for a in t], 16200, nc, ne, cluster,
+            sizes.ctypes.data, None, None, None, None)
+
+    assert rc(tabs) == 0
+    assert rc(tabs, cluster=3) == -3
+    bad = [a.copy() for a in tabs]
+    bad[1][5] = 16200                       # cidx out of range
+    assert rc(bad) == -3
+    bad = [a.copy() for a in tabs]
+    j = bad[2][1]                           # first edge of variable 1
+    bad[3][[0, j]] = bad[3][[j, 0]]         # vedge not variable-major
+    assert rc(bad) == -3
+    # a check of degree 129 is the reference kernel's -1
+    cptr = np.array([0, 129], np.int32)
+    cidx = np.arange(129, dtype=np.int32)
+    vptr = np.arange(130, dtype=np.int32)
+    vedge = np.arange(129, dtype=np.int32)
+    assert N.lib().atsc3_ldpc_tables_host(
+        cptr.ctypes.data, cidx.ctypes.data, vptr.ctypes.data,
+        vedge.ctypes.data, 129, 1, 129, 1, sizes.ctypes.data, None, None,
+        None, None) == -1
