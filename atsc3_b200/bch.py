@@ -27,8 +27,7 @@ def device_rtab(k, ninner, device):
     key = (k, ninner, str(device))
     t = _RT.get(key)
     if t is None:
-        t = torch.from_numpy(np.ascontiguousarray(
-            C.bch_remainder_table(k, ninner))).to(device)
+        t = torch.from_numpy(np.array(C.bch_remainder_table(k, ninner))).to(device)
         _RT[key] = t
     return t
 
@@ -38,7 +37,7 @@ def device_scrambler_bytes(kpay, device):
     key = ("scr", kpay, str(device))
     t = _RT.get(key)
     if t is None:
-        t = torch.from_numpy(np.packbits(C.scrambler_sequence(kpay))).to(device)
+        t = torch.from_numpy(np.packbits(np.array(C.scrambler_sequence(kpay)))).to(device)
         _RT[key] = t
     return t
 
@@ -81,9 +80,7 @@ def bch_syndrome_batch(bits2d, ninner=16200):
     """Drop-in for ``m9_accel.bch_syndrome_batch``: (nblk, n) {0,1} -> list
     of Python-int syndromes of the n-bit messages."""
     torch = _torch()
-    a = np.ascontiguousarray(np.asarray(bits2d, np.uint8))
-    if a.ndim == 1:
-        a = a[None]
+    a = np.array(bits2d, np.uint8, ndmin=2)      # fresh C-contiguous copy
     nblk, n = a.shape
     if nblk == 0:
         return []

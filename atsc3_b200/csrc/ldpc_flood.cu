@@ -526,13 +526,24 @@ struct OccHash {
 static std::mutex g_occ_mu;
 static std::unordered_map<OccKey, int, OccHash> g_occ;
 
-static int32_t prepare_fn(FloodFn fn, int smem, int cl) {
+// The kernel attributes are set once per (function, device) to the device
+// limits, so plans of different shared-memory sizes can share a function.
+static std::mutex g_attr_mu;
+static std::unordered_map<uint64_t, int> g_attr_done;
+
+static int32_t prepare_fn(FloodFn fn, int dev) {
+  const uint64_t key = (uint64_t)(uintptr_t)fn ^ ((uint64_t)dev << 56);
+  {
+    std::lock_guard<std::mutex> g(g_attr_mu);
+    if (g_attr_done.count(key)) return 0;
+  }
   ATSC3_CUDA(cudaFuncSetAttribute((const void *)fn,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  smem));
-  if (cl > 8)
-    ATSC3_CUDA(cudaFuncSetAttribute(
-        (const void *)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+                                  max_dyn_smem(dev)));
+  ATSC3_CUDA(cudaFuncSetAttribute(
+      (const void *)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  std::lock_guard<std::mutex> g(g_attr_mu);
+  g_attr_done[key] = 1;
   return 0;
 }
 
@@ -547,7 +558,7 @@ static int32_t max_clusters(FloodFn fn, int cl, int smem, int threads, int dev,
       return 0;
     }
   }
-  int32_t rc = prepare_fn(fn, smem, cl);
+  int32_t rc = prepare_fn(fn, dev);
   if (rc) return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cl, 1, 1);
@@ -588,8 +599,8 @@ int32_t flood_launch(const atsc3_ldpc_plan *p, const void *llr, int64_t ld_llr,
   ATSC3_ARG(hard == nullptr || (ld_hard >= (p->n + 7) / 8 && ld_hard % 4 == 0 &&
                                 ((uintptr_t)hard & 3) == 0),
             "hard needs ld_hard >= ceil(n/8), a multiple of 4, 4-byte aligned");
-  ATSC3_ARG(conv && its && bad, "null status output");
   if (nblk == 0) return 0;
+  ATSC3_ARG(conv && its && bad, "null status output");
   ATSC3_ARG(llr != nullptr, "null llr");
   if (threads <= 0) threads = 1024;
   ATSC3_ARG(threads % 32 == 0 && threads >= 64 && threads <= 1024,
@@ -607,6 +618,8 @@ int32_t flood_launch(const atsc3_ldpc_plan *p, const void *llr, int64_t ld_llr,
     set_error("unsupported: cluster configuration cannot be resident");
     return -4;
   }
+  rc = prepare_fn(fn, p->device);
+  if (rc) return rc;
   if (max_clusters_cap > 0) ncl = std::min(ncl, max_clusters_cap);
   ncl = std::min(ncl, nblk);
   FloodArgs a;
@@ -885,6 +898,23 @@ int32_t atsc3_ldpc_plan_info(const atsc3_ldpc_plan *p, int64_t *info) {
   info[7] = p->dmax_v;
   info[8] = p->table_bytes;
   info[9] = p->dtype;
+  return 0;
+}
+
+int32_t atsc3_ldpc_flood_config(const atsc3_ldpc_plan *plan, int32_t threads,
+                                int32_t semantics, int32_t *out) {
+  ATSC3_ARG(plan && out, "null argument");
+  if (threads <= 0) threads = 1024;
+  atsc3::FloodFn fn = atsc3::flood_fn(plan->dtype, plan->rec_bytes, semantics);
+  ATSC3_ARG(fn != nullptr, "no kernel for this dtype/semantics");
+  int ncl = 0;
+  int32_t rc = atsc3::max_clusters(fn, plan->cluster, plan->smem_bytes, threads,
+                                   plan->device, &ncl);
+  if (rc) return rc;
+  out[0] = ncl;
+  out[1] = plan->cluster;
+  out[2] = plan->smem_bytes;
+  out[3] = threads;
   return 0;
 }
 

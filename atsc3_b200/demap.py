@@ -50,8 +50,7 @@ def device_lam_of_q(n, mod, rate, device):
     key = ("lq", n, mod, rate, str(device))
     t = _DEV.get(key)
     if t is None:
-        t = torch.from_numpy(np.ascontiguousarray(
-            C.bicm_map(n, mod, rate), np.int32)).to(device)
+        t = torch.from_numpy(np.array(C.bicm_map(n, mod, rate), np.int32)).to(device)
         _DEV[key] = t
     return t
 

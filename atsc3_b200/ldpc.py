@@ -38,7 +38,10 @@ def _torch():
 
 
 class Plan:
-    """Device tables of one code for one message dtype and cluster size."""
+    """Device tables of one code for one message dtype and cluster size
+    (the CSR decoder of csrc/ldpc_flood.cu, any code)."""
+
+    kind = "csr"
 
     def __init__(self, cptr, cidx, vptr, vedge, n, dtype="float32",
                  cluster=0):
@@ -74,18 +77,68 @@ class Plan:
             self._h = None
 
 
+class QcPlan:
+    """Quasi-cyclic plan of an A/322 Type B code (float32 messages): the
+    decoder of csrc/ldpc_qc.cu, driven by circulant descriptors built from
+    the Annex A address rows."""
+
+    kind = "qc"
+
+    def __init__(self, rate, n, cluster=0):
+        typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+        if typ != "B":
+            raise ValueError("the quasi-cyclic decoder serves Type B codes")
+        rowptr, addr = C.address_rows(rate, n)
+        rowptr = np.ascontiguousarray(rowptr, np.int32)
+        addr = np.ascontiguousarray(addr, np.int32)
+        h = ctypes.c_void_p()
+        N.call("atsc3_ldpc_qc_plan_create", n, K, Q2, rowptr.ctypes.data,
+               addr.ctypes.data, int(cluster), ctypes.byref(h))
+        self._h = h
+        self.n, self.nc, self.dtype = n, n - K, "float32"
+        info = np.zeros(10, np.int64)
+        N.call("atsc3_ldpc_qc_plan_info", h, info.ctypes.data)
+        self.info = dict(zip(("n", "K", "Q", "cluster", "smem_bytes",
+                              "di_max", "dc_max", "table_bytes",
+                              "rows_per_cta", "nvlog2"), info.tolist()))
+        self.info["kind"] = "qc"
+        self.cluster = self.info["cluster"]
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                N.lib().atsc3_ldpc_qc_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
 _PLANS = {}
 _PLANS_LOCK = threading.Lock()
 
 
-def plan_for(rate, n, dtype="float32", cluster=0):
-    """Cached Plan of an A/322 code."""
+def plan_for(rate, n, dtype="float32", cluster=0, kind="auto"):
+    """Cached plan of an A/322 code.  kind "auto" picks the quasi-cyclic
+    decoder for the Type B codes it accepts (float32), else the CSR one."""
     torch = _torch()
-    key = (rate, n, dtype, cluster, torch.cuda.current_device())
+    key = (rate, n, dtype, cluster, kind, torch.cuda.current_device())
     with _PLANS_LOCK:
         p = _PLANS.get(key)
         if p is None:
-            p = Plan(*C.csr(rate, n), n, dtype=dtype, cluster=cluster)
+            if kind in ("auto", "qc") and dtype == "float32" and \
+                    C.ldpc_params(rate, n)[0] == "B":
+                try:
+                    p = QcPlan(rate, n, cluster=cluster)
+                except N.FecError as e:
+                    if kind == "qc" or e.rc != -4:
+                        raise
+            if p is None:
+                p = Plan(*C.csr(rate, n), n, dtype=dtype, cluster=cluster)
             _PLANS[key] = p
     return p
 
@@ -117,6 +170,15 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     bits = o.get("bits") if want_bits else None
     hard = o.get("hard") if want_hard else None
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    if getattr(plan, "kind", "csr") == "qc":
+        N.call("atsc3_ldpc_qc_decode", plan.handle, llr.data_ptr(),
+               llr.stride(0), nblk, int(iters), float(alpha),
+               SEMANTICS[semantics], N.ptr(bits),
+               bits.stride(0) if bits is not None else 0, N.ptr(hard),
+               hard.stride(0) if hard is not None else 0,
+               o["conv"].data_ptr(), o["its"].data_ptr(), o["bad"].data_ptr(),
+               int(threads), st)
+        return o
     N.call("atsc3_ldpc_decode_flood", plan.handle, llr.data_ptr(),
            llr.stride(0), nblk, int(iters), float(alpha),
            SEMANTICS[semantics], N.ptr(bits),

@@ -40,6 +40,18 @@ SIGNATURES = {
                                         c_f64, c_i32, c_vp, c_i64, c_vp,
                                         c_i64, c_vp, c_vp, c_vp, c_i32,
                                         c_vp]),
+    "atsc3_ldpc_flood_config": (c_i32, [c_vp, c_i32, c_i32, c_vp]),
+    "atsc3_ldpc_qc_plan_create": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp,
+                                          c_i32, c_vp]),
+    "atsc3_ldpc_qc_plan_destroy": (None, [c_vp]),
+    "atsc3_ldpc_qc_plan_info": (c_i32, [c_vp, c_vp]),
+    "atsc3_ldpc_qc_tables_host": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp,
+                                          c_i32, c_vp, c_vp, c_vp, c_vp,
+                                          c_vp, c_vp, c_vp]),
+    "atsc3_ldpc_qc_config": (c_i32, [c_vp, c_i32, c_i32, c_vp]),
+    "atsc3_ldpc_qc_decode": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32, c_f32,
+                                     c_i32, c_vp, c_i64, c_vp, c_i64, c_vp,
+                                     c_vp, c_vp, c_i32, c_vp]),
     "atsc3_demap": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32, c_i32,
                             c_vp, c_i64, c_f32, c_vp, c_vp, c_i64, c_vp]),
     "atsc3_demap_row_sigma2": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,

@@ -116,6 +116,53 @@ int32_t atsc3_ldpc_decode_flood(const atsc3_ldpc_plan *plan, const void *llr,
                                 uint8_t *conv, int32_t *its, int32_t *bad,
                                 int32_t threads, void *stream);
 
+/* Launch facts of the flooding decoder for this plan: out[0] = clusters that
+ * can be resident at once, [1] = CTAs per cluster, [2] = shared bytes per
+ * CTA, [3] = threads per CTA. */
+int32_t atsc3_ldpc_flood_config(const atsc3_ldpc_plan *plan, int32_t threads,
+                                int32_t semantics, int32_t *out);
+
+/* ---- quasi-cyclic decoder for the A/322 Type B codes ----------------------
+ * Same decoding semantics and outputs as atsc3_ldpc_decode_flood (float32),
+ * built from the Annex A address rows instead of CSR tables: the 360x360
+ * circulant structure replaces per-edge tables (see csrc/ldpc_qc.cu).
+ * Accepts Type B codes (Nldpc-Kldpc = 360*Qldpc) with at most one circulant
+ * per block; returns -4 otherwise.  Replaces GpuMinSum.__init__/decode for
+ * those codes. */
+typedef struct atsc3_ldpc_qc_plan atsc3_ldpc_qc_plan;
+
+int32_t atsc3_ldpc_qc_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
+                                  const int32_t *rowptr, const int32_t *addr,
+                                  int32_t cluster, atsc3_ldpc_qc_plan **out);
+void atsc3_ldpc_qc_plan_destroy(atsc3_ldpc_qc_plan *plan);
+
+/* info[0]=n [1]=K [2]=Q [3]=cluster [4]=shared bytes per CTA [5]=max
+ * information circulants per block row [6]=max per block column [7]=table
+ * bytes [8]=block rows per CTA [9]=log2 bits per CTA */
+int32_t atsc3_ldpc_qc_plan_info(const atsc3_ldpc_qc_plan *plan, int64_t *info);
+
+/* Host-only descriptor build for the CPU tests (no CUDA call).  meta (41
+ * ints): [0] row descriptors [1] column descriptors [2] log2 bits per CTA
+ * [3] checks per CTA [4] block rows per CTA [5] [6] max degrees [7] shared
+ * bytes [8..24] row split [25..41] variable-phase work split.  Array outputs
+ * may be null. */
+int32_t atsc3_ldpc_qc_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
+                                  const int32_t *rowptr, const int32_t *addr,
+                                  int32_t cluster, int32_t *meta,
+                                  int32_t *rdesc, int32_t *rptr,
+                                  int32_t *cdesc, int32_t *cptr, uint8_t *s0,
+                                  int32_t *rowinfo);
+
+int32_t atsc3_ldpc_qc_config(const atsc3_ldpc_qc_plan *plan, int32_t threads,
+                             int32_t semantics, int32_t *out);
+
+int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *plan, const float *llr,
+                             int64_t ld_llr, int32_t nblk, int32_t iters,
+                             float alpha, int32_t semantics, uint8_t *bits,
+                             int64_t ld_bits, uint8_t *hard, int64_t ld_hard,
+                             uint8_t *conv, int32_t *its, int32_t *bad,
+                             int32_t threads, void *stream);
+
 /* NUC max-log soft demapper with the bit de-interleaver in its epilogue.
  * cells: (nblk, ld_cells) complex64 as interleaved float pairs.
  * pts: 3*M floats: Re p, Im p, |p|^2 (float32, |p|^2 rounded once from

@@ -176,10 +176,13 @@ def test_known_answer_all_erasure(torch):
     assert int(o["bits"].sum()) == 0
 
 
-@pytest.mark.parametrize("n", [16200, 64800])
-def test_all_codes_random_llr_vs_oracle(n, torch):
+@pytest.mark.parametrize("n,kind", [(16200, "auto"), (64800, "auto"),
+                                    (64800, "csr")])
+def test_all_codes_random_llr_vs_oracle(n, kind, torch):
     """Every A/322 rate (Type A and B), random LLRs near the waterfall,
-    few iterations: the GPU decoder equals the oracle field by field."""
+    few iterations: the GPU decoder equals the oracle field by field.  kind
+    "auto" runs the quasi-cyclic decoder on the 64800 Type B codes, "csr"
+    forces the CSR decoder on all of them."""
     from atsc3_b200 import ldpc as LDPC
     rng = np.random.default_rng(n)
     for rate in C.RATES:
@@ -187,7 +190,7 @@ def test_all_codes_random_llr_vs_oracle(n, torch):
         llr = (rng.standard_normal((3, n)) * 2.5 + 1.5).astype(np.float32)
         llr[2] = np.abs(llr[2])                    # one clean block: its == 0
         want = oracle.flood(llr, tabs, n, iters=6, alpha=0.8)
-        plan = LDPC.plan_for(rate, n)
+        plan = LDPC.plan_for(rate, n, kind=kind)
         o = LDPC.decode_flood(plan, torch.from_numpy(llr).cuda(), iters=6,
                               alpha=0.8)
         assert np.array_equal(o["bits"].cpu().numpy(), want[0]), rate
@@ -291,3 +294,34 @@ def test_demap_llr_fast_dropin(torch):
     c2, _, _, cells2, s22, q2, _ = oracle_case("c64_256qam_10_15")
     got = demap_llr_fast(cells2[1], c2["mod"], c2["rate"], sigma2=float(s22))
     assert np.array_equal(got.astype(np.float32), q2[1])
+
+
+@pytest.mark.parametrize("cluster", [4, 8, 16])
+@pytest.mark.parametrize("rate", ["6/15", "8/15", "9/15", "10/15", "11/15",
+                                  "12/15", "13/15"])
+def test_qc_decoder_vs_oracle(rate, cluster, torch):
+    """Quasi-cyclic decoder, every 64800 Type B rate, several cluster sizes,
+    both semantics, against the oracle (30 iterations, mixed convergence)."""
+    from atsc3_b200 import native as N
+    from atsc3_b200.ldpc import QcPlan, decode_flood
+    n = 64800
+    try:
+        plan = QcPlan(rate, n, cluster=cluster)
+    except N.FecError as e:
+        assert e.rc == -4
+        pytest.skip(str(e))
+    rng = np.random.default_rng(cluster * 100 + len(rate))
+    tabs = C.csr(rate, n)
+    llr = (rng.standard_normal((6, n)) * 2.2 + 1.6).astype(np.float32)
+    x = torch.from_numpy(llr).cuda()
+    for sem, code in (("kernel", 0), ("torch", 1)):
+        want = oracle.flood(llr, tabs, n, iters=30, alpha=0.75, semantics=code)
+        o = decode_flood(plan, x, iters=30, alpha=0.75, semantics=sem,
+                         want_hard=True)
+        bits = o["bits"].cpu().numpy()
+        assert np.array_equal(bits, want[0]), (rate, sem)
+        assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
+        assert o["its"].cpu().numpy().tolist() == want[2].tolist(), (rate, sem)
+        assert o["bad"].cpu().numpy().tolist() == want[3].tolist(), (rate, sem)
+        assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
+                              np.packbits(bits, axis=1))
