@@ -71,10 +71,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 // shared::cta address in this CTA -> shared::cluster address of the same
 // offset in CTA `rank` of the cluster.
+// mapa only translates an address (no memory access), so it is not
+// volatile: the compiler may schedule and predicate it freely.
 __device__ __forceinline__ uint32_t dsmem_map(uint32_t local, uint32_t rank) {
   uint32_t r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
-               : "=r"(r) : "r"(local), "r"(rank));
+  asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
   return r;
 }
 

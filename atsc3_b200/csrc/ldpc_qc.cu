@@ -47,31 +47,40 @@ constexpr int QCHUNK = 12;                 // ceil(360 / 32) warps per row/colum
 constexpr int QMAXCL = 16;
 
 struct QcPlan {
-  int n = 0, K = 0, Q = 0, nbi = 0;
-  int cluster = 1, nvlog2 = 0, rows_per_cta = 0, ncp = 0, smem = 0;
-  int di_max = 0, dc_max = 0, device = 0;
+  int n = 0, K = 0, Q = 0, nbi = 0, nb = 0;
+  int cluster = 1, cpc = 0, rows_per_cta = 0, ncp = 0, smem = 0;
+  int dr_max = 0, dc_max = 0, device = 0;
   int64_t table_bytes = 0;
   int rb[QMAXCL + 1] = {0};     // block rows of CTA c: [rb[c], rb[c+1])
   int wb[QMAXCL + 1] = {0};     // variable-phase work items of CTA c
-  int2 *d_rdesc = nullptr;      // per row circulant: {360*g - u, u}
+  int4 *d_rdesc = nullptr;      // per row edge slot
   int32_t *d_rptr = nullptr;    // (Q+1)
-  int4 *d_cdesc = nullptr;      // per column circulant: {rank | pos<<8, rowoff, u, 0}
-  int32_t *d_cptr = nullptr;    // (nbi+1)
-  uint8_t *d_s0 = nullptr;      // (nbi*360) rotation start
-  int32_t *d_rowinfo = nullptr; // per row: rank | (d_r << 8), rowoff  (2*Q)
+  int4 *d_cdesc = nullptr;      // per column edge slot
+  int32_t *d_cptr = nullptr;    // (nb+1)
+  uint8_t *d_s0 = nullptr;      // (nb*360) rotation start
 };
 
+// One edge slot of a block row or block column, shared by its 360 checks
+// (bits):  x = owner CTA rank | WRAP flag << 8 | position << 16,
+//          y = byte offset of the 360-entry block in the owner's shared
+//              memory (posterior column for a row slot, record row for a
+//              column slot), z = circulant shift u, w = unused.
+// Row slot, check (r, k): target posterior index (k - u) mod 360.
+// Column slot, bit mm:    target record index (u + mm) mod 360.
+// WRAP marks the dual-diagonal wrap edge, absent for check (0, 0) and for
+// the last codeword bit.
+constexpr int QWRAP = 1 << 8;
+
 struct QcTables {
-  std::vector<int2> rdesc;
+  std::vector<int4> rdesc;
   std::vector<int32_t> rptr;
   std::vector<int4> cdesc;
   std::vector<int32_t> cptr;
   std::vector<uint8_t> s0;
-  std::vector<int32_t> rowinfo;
 };
 
-// Host: derive the block-row / block-column descriptors from the Annex A
-// address rows.  Returns 0, -3 or -4 (not a dup-free Type B code).
+// Host: derive the descriptors from the Annex A address rows.  Returns 0,
+// -3 or -4 (not a dup-free Type B code).
 int qc_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
              int cluster, QcPlan *p, QcTables *t) {
   if (n % QZ || K % QZ || Q <= 0 || (n - K) != Q * QZ) {
@@ -86,105 +95,104 @@ int qc_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     set_error("unsupported: codeword length above 65535");
     return -4;
   }
-  const int nbi = K / QZ;
-  struct Circ { int g, r, u; };
-  std::vector<std::vector<Circ>> rows(Q), cols(nbi);
-  for (int g = 0; g < nbi; ++g) {
+  const int nbi = K / QZ, nb = n / QZ;
+  struct Slot { int col, row, u, pos, wrap; };
+  std::vector<std::vector<Slot>> rows(Q), cols(nb);
+  for (int g = 0; g < nbi; ++g)
     for (int e = rowptr[g]; e < rowptr[g + 1]; ++e) {
       int x = addr[e];
       if (x < 0 || x >= n - K) {
         set_error("invalid argument: address outside the parity range");
         return -3;
       }
-      Circ c{g, x % Q, x / Q};
-      rows[c.r].push_back(c);
-      cols[g].push_back(c);
+      rows[x % Q].push_back(Slot{g, x % Q, x / Q, 0, 0});
     }
-  }
-  int di = 0;
+  int drm = 0;
   for (int r = 0; r < Q; ++r) {
     auto &R = rows[r];
-    std::sort(R.begin(), R.end(), [](const Circ &a, const Circ &b) {
-      return a.g < b.g;
+    std::sort(R.begin(), R.end(), [](const Slot &a, const Slot &b) {
+      return a.col < b.col;
     });
     for (size_t i = 1; i < R.size(); ++i)
-      if (R[i].g == R[i - 1].g) {
+      if (R[i].col == R[i - 1].col) {
         set_error("unsupported: two circulants share a block (use the CSR "
                   "decoder)");
         return -4;
       }
-    di = std::max(di, (int)R.size());
+    // dual diagonal: bits K+360(r-1)+k and K+360r+k (r >= 1); K+k and
+    // K+360(Q-1)+k-1 (r = 0, absent for k = 0)
+    if (r >= 1) {
+      R.push_back(Slot{nbi + r - 1, r, 0, 0, 0});
+      R.push_back(Slot{nbi + r, r, 0, 0, 0});
+    } else {
+      R.push_back(Slot{nbi, 0, 0, 0, 0});
+      R.push_back(Slot{nbi + Q - 1, 0, 1, 0, QWRAP});
+    }
+    for (int i = 0; i < (int)R.size(); ++i) {
+      R[i].pos = i;
+      cols[R[i].col].push_back(R[i]);
+    }
+    drm = std::max(drm, (int)R.size());
   }
-  if (di + 2 > 64) {
-    set_error("unsupported: block-row degree above 62");
+  if (drm > 64) {
+    set_error("unsupported: block-row degree above 64");
     return -4;
   }
-  // partition block rows over the cluster (contiguous, balanced by count)
-  p->n = n; p->K = K; p->Q = Q; p->nbi = nbi; p->cluster = cluster;
-  p->di_max = di;
-  p->dc_max = 0;
-  int per = (Q + cluster - 1) / cluster;
+  p->n = n; p->K = K; p->Q = Q; p->nbi = nbi; p->nb = nb;
+  p->cluster = cluster;
+  p->dr_max = drm;
+  // record rows and posterior columns, both split evenly over the cluster
+  const int per = (Q + cluster - 1) / cluster;
+  const int cpc = (nb + cluster - 1) / cluster;
   for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
   p->rows_per_cta = per;
   p->ncp = per * QZ;
-  std::vector<int> rrank(Q), rowoff(Q);
-  for (int r = 0; r < Q; ++r) {
-    rrank[r] = r / per;
-    rowoff[r] = (r - p->rb[rrank[r]]) * QZ;
-  }
-  int nvper = (n + cluster - 1) / cluster, nvl = 5;
-  while ((1 << nvl) < nvper) ++nvl;
-  p->nvlog2 = nvl;
-  // row descriptors
+  p->cpc = cpc;
+  const int tot_bytes = cpc * QZ * 4;
+  auto col_rank = [&](int b) { return b / cpc; };
+  auto col_base = [&](int b) { return (b % cpc) * QZ * 4; };
+  auto row_rank = [&](int r) { return r / per; };
+  auto row_base = [&](int r) { return tot_bytes + (r % per) * QZ * 16; };
   t->rptr.assign(Q + 1, 0);
   t->rdesc.clear();
   for (int r = 0; r < Q; ++r) {
-    for (auto &c : rows[r]) t->rdesc.push_back(make_int2(QZ * c.g - c.u, c.u));
+    for (auto &sl : rows[r])
+      t->rdesc.push_back(make_int4(col_rank(sl.col) | sl.wrap | (sl.pos << 16),
+                                   col_base(sl.col), sl.u, 0));
     t->rptr[r + 1] = (int)t->rdesc.size();
   }
-  t->rowinfo.assign(2 * Q, 0);
-  for (int r = 0; r < Q; ++r) {
-    t->rowinfo[2 * r] = rrank[r] | ((int)rows[r].size() << 8);
-    t->rowinfo[2 * r + 1] = rowoff[r];
-  }
-  // column descriptors, sorted by (u, r): the summation order before rotation
-  t->cptr.assign(nbi + 1, 0);
+  // column slots sorted by (u, row): ascending check order before rotation
+  t->cptr.assign(nb + 1, 0);
   t->cdesc.clear();
-  t->s0.assign((size_t)nbi * QZ, 0);
-  for (int g = 0; g < nbi; ++g) {
-    auto &Cc = cols[g];
-    std::sort(Cc.begin(), Cc.end(), [](const Circ &a, const Circ &b) {
-      return a.u != b.u ? a.u < b.u : a.r < b.r;
+  t->s0.assign((size_t)nb * QZ, 0);
+  int dcm = 0;
+  for (int b = 0; b < nb; ++b) {
+    auto &Cc = cols[b];
+    std::sort(Cc.begin(), Cc.end(), [](const Slot &a, const Slot &c) {
+      return a.u != c.u ? a.u < c.u : a.row < c.row;
     });
-    p->dc_max = std::max(p->dc_max, (int)Cc.size());
-    for (auto &c : Cc) {
-      int pos = 0;
-      for (auto &o : rows[c.r]) {
-        if (o.g == g) break;
-        ++pos;
-      }
-      t->cdesc.push_back(make_int4(rrank[c.r] | (pos << 8), rowoff[c.r], c.u, 0));
-    }
-    t->cptr[g + 1] = (int)t->cdesc.size();
+    dcm = std::max(dcm, (int)Cc.size());
+    for (auto &sl : Cc)
+      t->cdesc.push_back(make_int4(row_rank(sl.row) | sl.wrap | (sl.pos << 16),
+                                   row_base(sl.row), sl.u, 0));
+    t->cptr[b + 1] = (int)t->cdesc.size();
     for (int mm = 0; mm < QZ; ++mm) {
       int s = 0;
-      for (auto &c : Cc) s += (c.u + mm < QZ) ? 1 : 0;
-      t->s0[(size_t)g * QZ + mm] = (uint8_t)s;
+      for (auto &sl : Cc) s += (sl.u + mm < QZ) ? 1 : 0;
+      t->s0[(size_t)b * QZ + mm] = (uint8_t)s;
     }
   }
-  // variable-phase work items: (block column b, chunk q), w = b*12 + q,
-  // split into CL runs of equal edge count
-  const int ncols = nbi + Q;
-  std::vector<int64_t> wcost((size_t)ncols * QCHUNK);
+  p->dc_max = dcm;
+  // variable-phase work items (column b, chunk q), w = b*12 + q, split into
+  // CL runs of equal edge count
+  std::vector<int64_t> wcost((size_t)nb * QCHUNK);
   int64_t total = 0;
-  for (int b = 0; b < ncols; ++b) {
-    int deg = b < nbi ? (int)cols[b].size() : 2;
+  for (int b = 0; b < nb; ++b)
     for (int q = 0; q < QCHUNK; ++q) {
       int lanes = std::min(32, QZ - 32 * q);
-      wcost[(size_t)b * QCHUNK + q] = (int64_t)lanes * deg + 8;
+      wcost[(size_t)b * QCHUNK + q] = (int64_t)lanes * (int64_t)cols[b].size() + 16;
       total += wcost[(size_t)b * QCHUNK + q];
     }
-  }
   int64_t acc = 0;
   int c = 1;
   p->wb[0] = 0;
@@ -193,25 +201,24 @@ int qc_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     while (c < cluster && acc * cluster >= total * c) p->wb[c++] = w + 1;
   }
   while (c <= cluster) p->wb[c++] = (int)wcost.size();
-  p->smem = (1 << nvl) * 4 + p->ncp * 16 + 256;
+  p->smem = tot_bytes + p->ncp * 16 + 256;
   return 0;
 }
 
 struct QcArgs {
   const float *llr;
   int64_t ld_llr;
-  int nblk, n, K, Q, iters;
+  int nblk, n, iters;
   float alpha;
-  int nvlog2, ncp;
+  int cpc, ncp;
+  uint32_t cpc_inv;              // ceil(2^32 / cpc): bc / cpc for bc < 2^16
   int rb[QMAXCL + 1];
   int wb[QMAXCL + 1];
-  const int2 *rdesc;
+  const int4 *rdesc;
   const int32_t *rptr;
   const int4 *cdesc;
   const int32_t *cptr;
   const uint8_t *s0;
-  const int32_t *rowinfo;
-  int nbi;
   uint8_t *bits;
   int64_t ld_bits;
   uint8_t *hard;
@@ -221,36 +228,42 @@ struct QcArgs {
   int32_t *bad;
 };
 
-__device__ __forceinline__ float qc_msg(uint4 r, int pos) {
-  const float A = __uint_as_float(r.x), B = __uint_as_float(r.y);
-  float m = (pos == (int)(r.w & 0xFFu)) ? B : A;
-  const uint32_t s = pos < 32 ? (r.z >> pos) : (r.w >> (pos - 24));
-  return (s & 1u) ? -m : m;
+// edge message from a record {A, B, S, F | S1 << 8} for edge position pos
+__device__ __forceinline__ float qc_msg(uint4 r, uint32_t pos) {
+  const float m = (pos == (r.w & 0xFFu)) ? __uint_as_float(r.y)
+                                         : __uint_as_float(r.x);
+  const uint32_t s = pos < 32u ? (r.z >> pos) : (r.w >> (pos - 24u));
+  return __uint_as_float(__float_as_uint(m) ^ (s << 31));
 }
 
-// DI: unroll bound of information circulants per block row (>= di_max).
-template <bool TORCH, int DI>
-__global__ void __launch_bounds__(1024, 1) ldpc_qc_kernel(const QcArgs a) {
+// NCH: chunks of 8 edge slots per block row (compile-time, so every edge
+// position is a constant); MASK: sign-mask type.  DSMEM loads are issued
+// unconditionally -- an absent slot reads a harmless local address and is
+// masked out arithmetically -- so the loads of a chunk are straight-line
+// code the hardware can overlap.
+template <bool TORCH, int NCH, typename MASK, int NT>
+__global__ void __launch_bounds__(NT, 1) ldpc_qc_kernel(const QcArgs a) {
+  // variable-phase record loads in flight per thread (register budget)
+  constexpr int VB = NT >= 1024 ? 4 : (NT >= 768 ? 6 : 8);
   extern __shared__ __align__(16) unsigned char smem[];
   const int rank = (int)cluster_ctarank();
   const int CL = (int)cluster_nctarank();
-  const int nvp = 1 << a.nvlog2;
-  const uint32_t vmask = (uint32_t)nvp - 1u;
+  const int tot_bytes = a.cpc * QZ * 4;
   float *tot = reinterpret_cast<float *>(smem);
-  uint4 *rec = reinterpret_cast<uint4 *>(smem + (size_t)nvp * 4);
-  int *part = reinterpret_cast<int *>(smem + (size_t)nvp * 4 + (size_t)a.ncp * 16);
+  uint4 *rec = reinterpret_cast<uint4 *>(smem + tot_bytes);
+  int *part = reinterpret_cast<int *>(smem + tot_bytes + (size_t)a.ncp * 16);
   int *sbad = part + 32;
-  const uint32_t tot_sa = smem_u32(tot);
-  const uint32_t rec_sa = smem_u32(rec);
+  const uint32_t sm_sa = smem_u32(smem);
   const uint32_t part_sa = smem_u32(part);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
   const int r0 = a.rb[rank], r1 = a.rb[rank + 1];
   const int ncitems = (r1 - r0) * QCHUNK;
   const int w0 = a.wb[rank], w1 = a.wb[rank + 1];
-  const int vbase = rank * nvp;
-  const int vend = min(a.n, vbase + nvp);
-  const int K = a.K, Q = a.Q;
+  const int vbase = rank * a.cpc * QZ;
+  const int vend = min(a.n, vbase + a.cpc * QZ);
+  constexpr int MB = (int)sizeof(MASK) * 8;
+  const uint32_t dummy = sm_sa;                      // own, always mapped
 
   if (tid == 0) *sbad = 0;
 
@@ -265,57 +278,72 @@ __global__ void __launch_bounds__(1024, 1) ldpc_qc_kernel(const QcArgs a) {
       // ---------------- check phase ----------------------------------------
       int mybad = 0;
       for (int w = warp; w < ncitems; w += nwarps) {
-        const int r = r0 + w / QCHUNK;
-        const int k = (w % QCHUNK) * 32 + lane;
-        if (k < QZ) {
-          const int rp = __ldg(a.rptr + r);
-          const int d = __ldg(a.rptr + r + 1) - rp;
-          const int li = (r - r0) * QZ + k;
-          const uint4 ro = rec[li];
-          const float Ao = __uint_as_float(ro.x), Bo = __uint_as_float(ro.y);
-          const int Fo = (int)(ro.w & 0xFFu);
-          float t[DI + 2];
+        const int rl = w / QCHUNK;
+        const int r = r0 + rl;
+        const int k0 = (w - rl * QCHUNK) * 32 + lane;
+        const bool kv = k0 < QZ;
+        const int k = kv ? k0 : QZ - 1;
+        const int rp = __ldg(a.rptr + r);
+        const int deg = __ldg(a.rptr + r + 1) - rp;
+        const int4 *ds = a.rdesc + rp;
+        const int li = rl * QZ + k;
+        const uint4 ro = rec[li];
+        const float Ao = __uint_as_float(ro.x), Bo = __uint_as_float(ro.y);
+        const uint32_t Fo = ro.w & 0xFFu;
+        MASK So = (MASK)ro.z;
+        if constexpr (MB > 32) So |= (MASK)(ro.w >> 8) << 32;
+        float min1 = __int_as_float(0x7f800000), min2 = min1;
+        uint32_t first = 0;
+        MASK sv = 0, st = 0, live = 0;
 #pragma unroll
-          for (int i = 0; i < DI; ++i) {
-            if (i < d) {
-              const int2 ds = __ldg(a.rdesc + rp + i);
-              const uint32_t v = (uint32_t)(ds.x + k + (k < ds.y ? QZ : 0));
-              t[i] = dsmem_ld_f32(dsmem_map(tot_sa + (v & vmask) * 4u, v >> a.nvlog2));
+        for (int c = 0; c < NCH; ++c) {
+          float t[8];
+          uint32_t ad[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int j = c * 8 + u;
+            const int4 d = __ldg(ds + min(j, deg - 1));
+            const bool on = j < deg && !((d.x & QWRAP) && k == 0);
+            int o = k - d.z;
+            o += o < 0 ? QZ : 0;
+            ad[u] = on ? dsmem_map(sm_sa + (uint32_t)(d.y + 4 * o), (uint32_t)(d.x & 0xFF))
+                       : dummy;
+            if (on) live |= (MASK)1 << j;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) t[u] = dsmem_ld_f32(ad[u]);
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int j = c * 8 + u;
+            const MASK bit = (MASK)1 << j;
+            if (live & bit) {
+              if (t[u] < 0.f) st |= bit;
+              float mo = ((uint32_t)j == Fo) ? Bo : Ao;
+              if (So & bit) mo = -mo;
+              const float v = __fsub_rn(t[u], mo);
+              if (v < 0.f) sv |= bit;
+              const float mag = fabsf(v);
+              if (mag < min1) { min2 = min1; min1 = mag; first = (uint32_t)j; }
+              else if (mag < min2) { min2 = mag; }
             }
           }
-          const uint32_t pa = (uint32_t)(r >= 1 ? K + QZ * (r - 1) + k : K + k);
-          const bool hasb = r >= 1 || k >= 1;
-          const uint32_t pb = (uint32_t)(r >= 1 ? K + QZ * r + k : K + QZ * (Q - 1) + k - 1);
-          const float ta = dsmem_ld_f32(dsmem_map(tot_sa + (pa & vmask) * 4u, pa >> a.nvlog2));
-          float tb = 0.f;
-          if (hasb) tb = dsmem_ld_f32(dsmem_map(tot_sa + (pb & vmask) * 4u, pb >> a.nvlog2));
-          float min1 = __int_as_float(0x7f800000), min2 = min1;
-          int first = 0;
-          uint32_t syn = 0;
-          uint64_t sg = 0;
-          auto edge = [&](float tv, int j) {
-            syn ^= tv < 0.f ? 1u : 0u;
-            float mo = (j == Fo) ? Bo : Ao;
-            const uint32_t so = j < 32 ? (ro.z >> j) : (ro.w >> (j - 24));
-            if (so & 1u) mo = -mo;
-            const float v = __fsub_rn(tv, mo);
-            if (v < 0.f) sg |= 1ull << j;
-            const float mag = fabsf(v);
-            if (mag < min1) { min2 = min1; min1 = mag; first = j; }
-            else if (mag < min2) { min2 = mag; }
-          };
-#pragma unroll
-          for (int i = 0; i < DI; ++i)
-            if (i < d) edge(t[i], i);
-          edge(ta, d);
-          if (hasb) edge(tb, d + 1);
-          const int deg = d + (hasb ? 2 : 1);
-          if (__popcll(sg) & 1) sg ^= (deg >= 64 ? ~0ull : ((1ull << deg) - 1ull));
+        }
+        int par, syn;
+        if constexpr (MB > 32) {
+          par = __popcll((unsigned long long)sv) & 1;
+          syn = __popcll((unsigned long long)st) & 1;
+        } else {
+          par = __popc((uint32_t)sv) & 1;
+          syn = __popc((uint32_t)st) & 1;
+        }
+        if (par) sv ^= live;
+        if (kv) {
+          uint32_t hi = 0;
+          if constexpr (MB > 32) hi = (uint32_t)((unsigned long long)sv >> 32) << 8;
           rec[li] = make_uint4(__float_as_uint(__fmul_rn(min1, a.alpha)),
                                __float_as_uint(__fmul_rn(min2, a.alpha)),
-                               (uint32_t)sg,
-                               (uint32_t)first | ((uint32_t)(sg >> 32) << 8));
-          mybad += (int)syn;
+                               (uint32_t)sv, first | hi);
+          mybad += syn;
         }
       }
       mybad = __reduce_add_sync(0xffffffffu, mybad);
@@ -337,22 +365,14 @@ __global__ void __launch_bounds__(1024, 1) ldpc_qc_kernel(const QcArgs a) {
             bo[i] = tot[i - vbase] < 0.f ? 1 : 0;
         }
         if (a.hard) {
+          // whole bytes: 360-bit columns are 45-byte aligned
           uint8_t *ho = a.hard + (size_t)b * a.ld_hard;
-          for (int wq = vbase; wq < vend; wq += 32 * nwarps) {
-            const int i = wq + (warp << 5) + lane;
-            const bool ng = i < vend && tot[i - vbase] < 0.f;
-            const uint32_t m = __ballot_sync(0xffffffffu, ng);
-            const int base = wq + (warp << 5);
-            if (lane == 0 && base < vend) {
-              const uint32_t word = __byte_perm(__brev(m), 0u, 0x0123u);
-              if (base + 32 <= vend) {
-                *reinterpret_cast<uint32_t *>(ho + (base >> 3)) = word;
-              } else {
-                const int nbyte = (vend - base + 7) >> 3;
-                for (int q = 0; q < nbyte; ++q)
-                  ho[(base >> 3) + q] = (uint8_t)(word >> (8 * q));
-              }
-            }
+          for (int by = (vbase >> 3) + tid; by < (vend >> 3); by += blockDim.x) {
+            uint32_t v = 0;
+            const float *tp = tot + (by * 8 - vbase);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v |= (tp[q] < 0.f ? 1u : 0u) << (7 - q);
+            ho[by] = (uint8_t)v;
           }
         }
         if (rank == 0 && tid == 0) {
@@ -365,69 +385,68 @@ __global__ void __launch_bounds__(1024, 1) ldpc_qc_kernel(const QcArgs a) {
       // ---------------- variable phase -------------------------------------
       for (int w = w0 + warp; w < w1; w += nwarps) {
         const int bc = w / QCHUNK;
-        const int mm = (w % QCHUNK) * 32 + lane;
-        if (mm < QZ) {
-          const int lamidx = bc * QZ + mm;
-          const float li = lam[lamidx];
-          float acc = TORCH ? li : 0.f;
-          if (bc < a.nbi) {
-            const int cs = __ldg(a.cptr + bc);
-            const int d = __ldg(a.cptr + bc + 1) - cs;
-            const int s0 = __ldg(a.s0 + (size_t)bc * QZ + mm);
-            for (int t0 = 0; t0 < d; t0 += 4) {
-              uint4 rr[4];
-              int pos[4];
+        const int mm0 = (w - bc * QCHUNK) * 32 + lane;
+        const bool mv = mm0 < QZ;
+        const int mm = mv ? mm0 : QZ - 1;
+        const int lamidx = bc * QZ + mm;
+        const float li = lam[lamidx];
+        float acc = TORCH ? li : 0.f;
+        const int cs = __ldg(a.cptr + bc);
+        const int d = __ldg(a.cptr + bc + 1) - cs;
+        const int s0 = __ldg(a.s0 + lamidx);
+        const int4 *ds = a.cdesc + cs;
+        if (d == 2) {
+          // dual-diagonal parity column (warp-uniform): two slots, no padding
+          uint32_t ad[2], pos[2];
+          bool on[2];
 #pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                pos[u] = -1;
-                if (t0 + u < d) {
-                  int i = s0 + t0 + u;
-                  if (i >= d) i -= d;
-                  const int4 ds = __ldg(a.cdesc + cs + i);
-                  int kk = ds.z + mm;
-                  if (kk >= QZ) kk -= QZ;
-                  pos[u] = ds.x >> 8;
-                  rr[u] = dsmem_ld_v4(dsmem_map(
-                      rec_sa + (uint32_t)(ds.y + kk) * 16u, (uint32_t)(ds.x & 0xFF)));
-                }
-              }
-#pragma unroll
-              for (int u = 0; u < 4; ++u)
-                if (pos[u] >= 0) acc = __fadd_rn(acc, qc_msg(rr[u], pos[u]));
-            }
-          } else {
-            const int tt = bc - a.nbi;           // parity block column
-            const int2 ri = __ldg(reinterpret_cast<const int2 *>(a.rowinfo) + tt);
-            const int dt = ri.x >> 8;
-            const int p1 = tt >= 1 ? dt + 1 : dt;
-            const uint4 m1 = dsmem_ld_v4(dsmem_map(
-                rec_sa + (uint32_t)(ri.y + mm) * 16u, (uint32_t)(ri.x & 0xFF)));
-            int rank2 = -1, off2 = 0, p2 = 0;
-            if (tt + 1 < Q) {
-              const int2 r2 = __ldg(reinterpret_cast<const int2 *>(a.rowinfo) + tt + 1);
-              rank2 = r2.x & 0xFF;
-              off2 = r2.y + mm;
-              p2 = r2.x >> 8;
-            } else if (mm + 1 < QZ) {
-              const int2 r2 = __ldg(reinterpret_cast<const int2 *>(a.rowinfo));
-              rank2 = r2.x & 0xFF;
-              off2 = r2.y + mm + 1;
-              p2 = (r2.x >> 8) + 1;
-            }
-            uint4 m2 = make_uint4(0u, 0u, 0u, 0u);
-            if (rank2 >= 0)
-              m2 = dsmem_ld_v4(dsmem_map(rec_sa + (uint32_t)off2 * 16u, (uint32_t)rank2));
-            acc = __fadd_rn(acc, qc_msg(m1, p1));
-            if (rank2 >= 0) acc = __fadd_rn(acc, qc_msg(m2, p2));
+          for (int u = 0; u < 2; ++u) {
+            int i = s0 + u;
+            i -= i >= 2 ? 2 : 0;
+            const int4 e = __ldg(ds + i);
+            on[u] = !((e.x & QWRAP) && mm == QZ - 1);
+            int o = e.z + mm;
+            o -= o >= QZ ? QZ : 0;
+            pos[u] = (uint32_t)e.x >> 16;
+            ad[u] = on[u] ? dsmem_map(sm_sa + (uint32_t)(e.y + 16 * o),
+                                      (uint32_t)(e.x & 0xFF))
+                          : dummy;
           }
+          const uint4 q0 = dsmem_ld_v4(ad[0]);
+          const uint4 q1 = dsmem_ld_v4(ad[1]);
+          if (on[0]) acc = __fadd_rn(acc, qc_msg(q0, pos[0]));
+          if (on[1]) acc = __fadd_rn(acc, qc_msg(q1, pos[1]));
+        } else
+        for (int t0 = 0; t0 < d; t0 += VB) {
+          uint32_t ad[VB], pos[VB];
+          bool on[VB];
+#pragma unroll
+          for (int u = 0; u < VB; ++u) {
+            int i = s0 + t0 + u;
+            i -= i >= d ? d : 0;
+            i = min(i, d - 1);
+            const int4 e = __ldg(ds + i);
+            on[u] = t0 + u < d && !((e.x & QWRAP) && mm == QZ - 1);
+            int o = e.z + mm;
+            o -= o >= QZ ? QZ : 0;
+            pos[u] = (uint32_t)e.x >> 16;
+            ad[u] = on[u] ? dsmem_map(sm_sa + (uint32_t)(e.y + 16 * o),
+                                      (uint32_t)(e.x & 0xFF))
+                          : dummy;
+          }
+          uint4 rr[VB];
+#pragma unroll
+          for (int u = 0; u < VB; ++u) rr[u] = dsmem_ld_v4(ad[u]);
+#pragma unroll
+          for (int u = 0; u < VB; ++u)
+            if (on[u]) acc = __fadd_rn(acc, qc_msg(rr[u], pos[u]));
+        }
+        if (mv) {
           const float nv = TORCH ? acc : __fadd_rn(li, acc);
-          const uint32_t owner = (uint32_t)lamidx >> a.nvlog2;
-          if ((int)owner == rank) {
-            tot[lamidx - vbase] = nv;
-          } else {
-            dsmem_st_u32(dsmem_map(tot_sa + ((uint32_t)lamidx & vmask) * 4u, owner),
-                         __float_as_uint(nv));
-          }
+          const int owner = (int)__umulhi((uint32_t)bc, a.cpc_inv);   // bc / cpc
+          const uint32_t off = (uint32_t)((bc - owner * a.cpc) * QZ + mm) * 4u;
+          if (owner == rank) tot[off >> 2] = nv;
+          else dsmem_st_u32(dsmem_map(sm_sa + off, (uint32_t)owner), __float_as_uint(nv));
         }
       }
       __syncthreads();
@@ -440,10 +459,25 @@ __global__ void __launch_bounds__(1024, 1) ldpc_qc_kernel(const QcArgs a) {
 
 typedef void (*QcFn)(const QcArgs);
 
-static QcFn qc_fn(int semantics, int di) {
-  if (di <= 8) return semantics ? ldpc_qc_kernel<true, 8> : ldpc_qc_kernel<false, 8>;
-  if (di <= 16) return semantics ? ldpc_qc_kernel<true, 16> : ldpc_qc_kernel<false, 16>;
-  if (di <= 32) return semantics ? ldpc_qc_kernel<true, 32> : ldpc_qc_kernel<false, 32>;
+#define ATSC3_QC_FN(NCH, MASK)                                              \
+  (nt == 1024 ? (semantics ? ldpc_qc_kernel<true, NCH, MASK, 1024>           \
+                           : ldpc_qc_kernel<false, NCH, MASK, 1024>)         \
+   : nt == 768 ? (semantics ? ldpc_qc_kernel<true, NCH, MASK, 768>           \
+                            : ldpc_qc_kernel<false, NCH, MASK, 768>)         \
+               : (semantics ? ldpc_qc_kernel<true, NCH, MASK, 512>           \
+                            : ldpc_qc_kernel<false, NCH, MASK, 512>))
+
+// The CTA size picks the build: > 768 threads -> 1024-thread build (64
+// registers, 4 record loads in flight per thread), > 512 -> 768 (85, 6),
+// else 512 (128, 8).
+static QcFn qc_fn(int semantics, int dr, int threads) {
+  const int nt = threads > 768 ? 1024 : (threads > 512 ? 768 : 512);
+  if (dr <= 8) return ATSC3_QC_FN(1, uint32_t);
+  if (dr <= 16) return ATSC3_QC_FN(2, uint32_t);
+  if (dr <= 24) return ATSC3_QC_FN(3, uint32_t);
+  if (dr <= 32) return ATSC3_QC_FN(4, uint32_t);
+  if (dr <= 40) return ATSC3_QC_FN(5, unsigned long long);
+  if (dr <= 56) return ATSC3_QC_FN(7, unsigned long long);
   return nullptr;
 }
 
@@ -549,12 +583,11 @@ int32_t atsc3_ldpc_qc_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
     h->p.table_bytes += (int64_t)bytes;
     return bytes ? cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
   };
-  cudaError_t e = up((void **)&h->p.d_rdesc, t.rdesc.data(), t.rdesc.size() * 8);
+  cudaError_t e = up((void **)&h->p.d_rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_rptr, t.rptr.data(), t.rptr.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_cdesc, t.cdesc.data(), t.cdesc.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_cptr, t.cptr.data(), t.cptr.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
-  if (e == cudaSuccess) e = up((void **)&h->p.d_rowinfo, t.rowinfo.data(), t.rowinfo.size() * 4);
   if (e != cudaSuccess) {
     atsc3_ldpc_qc_plan_destroy(h);
     return cuda_fail(e, "qc plan upload");
@@ -570,7 +603,6 @@ void atsc3_ldpc_qc_plan_destroy(atsc3_ldpc_qc_plan *h) {
   cudaFree(h->p.d_cdesc);
   cudaFree(h->p.d_cptr);
   cudaFree(h->p.d_s0);
-  cudaFree(h->p.d_rowinfo);
   delete h;
 }
 
@@ -581,11 +613,11 @@ int32_t atsc3_ldpc_qc_plan_info(const atsc3_ldpc_qc_plan *h, int64_t *info) {
   info[2] = h->p.Q;
   info[3] = h->p.cluster;
   info[4] = h->p.smem;
-  info[5] = h->p.di_max;
+  info[5] = h->p.dr_max;
   info[6] = h->p.dc_max;
   info[7] = h->p.table_bytes;
   info[8] = h->p.rows_per_cta;
-  info[9] = h->p.nvlog2;
+  info[9] = h->p.cpc;
   return 0;
 }
 
@@ -593,34 +625,30 @@ int32_t atsc3_ldpc_qc_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
                                   const int32_t *rowptr, const int32_t *addr,
                                   int32_t cluster, int32_t *meta,
                                   int32_t *rdesc, int32_t *rptr,
-                                  int32_t *cdesc, int32_t *cptr, uint8_t *s0,
-                                  int32_t *rowinfo) {
+                                  int32_t *cdesc, int32_t *cptr, uint8_t *s0) {
   using namespace atsc3;
   ATSC3_ARG(meta && rowptr && addr, "null argument");
   QcPlan p;
   QcTables t;
   int rc = qc_build(n, kldpc, qldpc, rowptr, addr, cluster, &p, &t);
   if (rc) return rc;
-  // meta: [0] rdesc entries [1] cdesc entries [2] nvlog2 [3] ncp
-  //       [4] rows/CTA [5] di_max [6] dc_max [7] smem [8..8+CL] rb [25..] wb
   meta[0] = (int32_t)t.rdesc.size();
   meta[1] = (int32_t)t.cdesc.size();
-  meta[2] = p.nvlog2;
+  meta[2] = p.cpc;
   meta[3] = p.ncp;
   meta[4] = p.rows_per_cta;
-  meta[5] = p.di_max;
+  meta[5] = p.dr_max;
   meta[6] = p.dc_max;
   meta[7] = p.smem;
   for (int c = 0; c <= QMAXCL; ++c) {
     meta[8 + c] = p.rb[c];
     meta[25 + c] = p.wb[c];
   }
-  if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 8);
+  if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
   if (cptr) std::memcpy(cptr, t.cptr.data(), t.cptr.size() * 4);
   if (s0) std::memcpy(s0, t.s0.data(), t.s0.size());
-  if (rowinfo) std::memcpy(rowinfo, t.rowinfo.data(), t.rowinfo.size() * 4);
   return 0;
 }
 
@@ -629,7 +657,7 @@ int32_t atsc3_ldpc_qc_config(const atsc3_ldpc_qc_plan *h, int32_t threads,
   using namespace atsc3;
   ATSC3_ARG(h && out, "null argument");
   if (threads <= 0) threads = 1024;
-  QcFn fn = qc_fn(semantics, h->p.di_max);
+  QcFn fn = qc_fn(semantics, h->p.dr_max, threads);
   ATSC3_ARG(fn != nullptr, "no kernel for this degree");
   int ncl = 0;
   int32_t rc = qc_max_clusters(fn, h->p.cluster, h->p.smem, threads, h->p.device, &ncl);
@@ -664,7 +692,7 @@ int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *h, const float *llr,
   if (threads <= 0) threads = 1024;
   ATSC3_ARG(threads % 32 == 0 && threads >= 64 && threads <= 1024,
             "threads must be a multiple of 32 in [64, 1024]");
-  QcFn fn = qc_fn(semantics, p.di_max);
+  QcFn fn = qc_fn(semantics, p.dr_max, threads);
   if (!fn) {
     set_error("unsupported: block-row degree too high");
     return -4;
@@ -685,11 +713,10 @@ int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *h, const float *llr,
   a.ld_llr = ld_llr;
   a.nblk = nblk;
   a.n = p.n;
-  a.K = p.K;
-  a.Q = p.Q;
   a.iters = iters;
   a.alpha = alpha;
-  a.nvlog2 = p.nvlog2;
+  a.cpc = p.cpc;
+  a.cpc_inv = (uint32_t)((0x100000000ull + (uint64_t)p.cpc - 1) / (uint64_t)p.cpc);
   a.ncp = p.ncp;
   for (int c = 0; c <= QMAXCL; ++c) {
     a.rb[c] = p.rb[c];
@@ -700,8 +727,6 @@ int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *h, const float *llr,
   a.cdesc = p.d_cdesc;
   a.cptr = p.d_cptr;
   a.s0 = p.d_s0;
-  a.rowinfo = p.d_rowinfo;
-  a.nbi = p.nbi;
   a.bits = bits;
   a.ld_bits = ld_bits;
   a.hard = hard;

@@ -99,8 +99,8 @@ class QcPlan:
         info = np.zeros(10, np.int64)
         N.call("atsc3_ldpc_qc_plan_info", h, info.ctypes.data)
         self.info = dict(zip(("n", "K", "Q", "cluster", "smem_bytes",
-                              "di_max", "dc_max", "table_bytes",
-                              "rows_per_cta", "nvlog2"), info.tolist()))
+                              "dr_max", "dc_max", "table_bytes",
+                              "rows_per_cta", "cols_per_cta"), info.tolist()))
         self.info["kind"] = "qc"
         self.cluster = self.info["cluster"]
 

@@ -47,7 +47,7 @@ SIGNATURES = {
     "atsc3_ldpc_qc_plan_info": (c_i32, [c_vp, c_vp]),
     "atsc3_ldpc_qc_tables_host": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp,
                                           c_i32, c_vp, c_vp, c_vp, c_vp,
-                                          c_vp, c_vp, c_vp]),
+                                          c_vp, c_vp]),
     "atsc3_ldpc_qc_config": (c_i32, [c_vp, c_i32, c_i32, c_vp]),
     "atsc3_ldpc_qc_decode": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32, c_f32,
                                      c_i32, c_vp, c_i64, c_vp, c_i64, c_vp,

@@ -137,21 +137,21 @@ int32_t atsc3_ldpc_qc_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
 void atsc3_ldpc_qc_plan_destroy(atsc3_ldpc_qc_plan *plan);
 
 /* info[0]=n [1]=K [2]=Q [3]=cluster [4]=shared bytes per CTA [5]=max
- * information circulants per block row [6]=max per block column [7]=table
- * bytes [8]=block rows per CTA [9]=log2 bits per CTA */
+ * block-row degree [6]=max block-column degree [7]=table bytes [8]=block
+ * rows per CTA [9]=360-bit columns per CTA */
 int32_t atsc3_ldpc_qc_plan_info(const atsc3_ldpc_qc_plan *plan, int64_t *info);
 
-/* Host-only descriptor build for the CPU tests (no CUDA call).  meta (41
- * ints): [0] row descriptors [1] column descriptors [2] log2 bits per CTA
- * [3] checks per CTA [4] block rows per CTA [5] [6] max degrees [7] shared
- * bytes [8..24] row split [25..41] variable-phase work split.  Array outputs
- * may be null. */
+/* Host-only descriptor build for the CPU tests (no CUDA call).  meta (42
+ * ints): [0] row slots [1] column slots [2] 360-bit columns per CTA [3]
+ * checks per CTA [4] block rows per CTA [5] max row degree [6] max column
+ * degree [7] shared bytes [8..24] row split [25..41] variable-phase work
+ * split.  rdesc/cdesc are int4 slots (rank | wrap<<8 | position<<16, byte
+ * base, shift, 0).  Array outputs may be null. */
 int32_t atsc3_ldpc_qc_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
                                   const int32_t *rowptr, const int32_t *addr,
                                   int32_t cluster, int32_t *meta,
                                   int32_t *rdesc, int32_t *rptr,
-                                  int32_t *cdesc, int32_t *cptr, uint8_t *s0,
-                                  int32_t *rowinfo);
+                                  int32_t *cdesc, int32_t *cptr, uint8_t *s0);
 
 int32_t atsc3_ldpc_qc_config(const atsc3_ldpc_qc_plan *plan, int32_t threads,
                              int32_t semantics, int32_t *out);

@@ -115,3 +115,24 @@ def test_host_tables_reject_bad_input():
         cptr.ctypes.data, cidx.ctypes.data, vptr.ctypes.data,
         vedge.ctypes.data, 129, 1, 129, 1, sizes.ctypes.data, None, None,
         None, None) == -1
+
+
+def test_install_rebinds_and_restores():
+    """atsc3_b200.install mirrors lab/m9_accel.py:392-433 (swap module
+    attributes, restore on uninstall) for the four replaced entry points."""
+    import types
+    from atsc3_b200 import install as I
+    m9_gpu = types.SimpleNamespace(GpuMinSum="ref")
+    m16 = types.SimpleNamespace(demap_llr_fast="ref")
+    m9a = types.SimpleNamespace(bch_syndrome_batch="ref", bch_syndrome="ref")
+    m3 = types.SimpleNamespace(_kernel_lib="ref")
+    assert I.install(m9_gpu, m16, m9a, m3) == 5
+    from atsc3_b200 import bch, demap, ldpc
+    assert m9_gpu.GpuMinSum is ldpc.GpuMinSum
+    assert m16.demap_llr_fast is demap.demap_llr_fast
+    assert m9a.bch_syndrome_batch is bch.bch_syndrome_batch
+    lib = m3._kernel_lib()
+    assert lib.ldpc_kernel_abi() == 1
+    I.uninstall()
+    assert m9_gpu.GpuMinSum == "ref" and m3._kernel_lib == "ref"
+    assert m9a.bch_syndrome == "ref" and m16.demap_llr_fast == "ref"
