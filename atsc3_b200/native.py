@@ -60,6 +60,12 @@ SIGNATURES = {
                                 c_vp, c_i32, c_vp, c_i64, c_vp]),
     "atsc3_bch_syndrome_bits": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,
                                         c_vp, c_vp]),
+    "atsc3_fec_decode_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_i64, c_i32,
+                                         c_i32, c_vp, c_i32, c_i32, c_vp,
+                                         c_i64, c_f32, c_vp, c_i32, c_f32,
+                                         c_vp, c_i32, c_vp, c_i32, c_vp,
+                                         c_i64, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                         c_vp]),
 }
 
 

@@ -211,6 +211,30 @@ int32_t atsc3_bch_syndrome_bits(const uint8_t *bits, int64_t ld_bits,
                                 const uint32_t *rtab, uint32_t *syn,
                                 void *stream);
 
+/* ---- decode without device allocation -------------------------------------
+ * No counterpart in the reference (its decoders allocate through numpy and
+ * torch).  For callers that must not allocate device memory on their decode
+ * path -- a real-time loop with a fixed memory budget, or a host that only
+ * lends the GPU pre-reserved buffers: the demap -> LDPC -> BCH chain of
+ * atsc3_demap / atsc3_ldpc_qc_decode (plan_kind 1) or
+ * atsc3_ldpc_decode_flood (plan_kind 0) / atsc3_bch_check in one call, with
+ * its LLR and hard-decision intermediates in a fixed file-scope device
+ * scratch (about 4.3 MB on every GPU that loads the library) instead of
+ * caller buffers.  Limit: at most 16 codewords of at most 64800 bits per
+ * call (-3 otherwise).  The first call on a device looks up the scratch
+ * address: make it before any stream capture.  Calls that overlap on the GPU
+ * share the scratch and race.  Arguments mean what they mean for the three
+ * calls it chains (sigma_mode 0..2, lam_of_q required, float32 plans);
+ * calls no allocator itself (the plan is made at set-up). */
+int32_t atsc3_fec_decode_noalloc(
+    const void *plan, int32_t plan_kind, const float *cells, int64_t ld_cells,
+    int32_t nblk, int32_t ncell, const float *pts, int32_t nbits,
+    int32_t sigma_mode, const float *sigma2, int64_t ld_sigma,
+    float sigma2_scalar, const int32_t *lam_of_q, int32_t iters, float alpha,
+    const uint32_t *rtab, int32_t kldpc, const uint8_t *scr, int32_t kpayload,
+    uint8_t *payload, int64_t ld_payload, uint8_t *conv, int32_t *its,
+    int32_t *bad, uint32_t *syn, uint8_t *ok, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
