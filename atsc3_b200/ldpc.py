@@ -239,3 +239,89 @@ class GpuMinSum:
         self.stats["iters"] += int(its.max(initial=0))
         return (o["bits"].cpu().numpy(), o["conv"].cpu().numpy().astype(bool),
                 its, o["bad"].cpu().numpy())
+
+
+class LayeredPlan:
+    """Layered min-sum plan of an A/322 Type B code (csrc/ldpc_layered.cu).
+
+    Not bit-comparable with the flooding decoders (different schedule);
+    bit-exact with oracle.layered.  ``ctas`` = resident CTAs (codewords in
+    flight); the scratch workspace is allocated once per plan for them."""
+
+    kind = "layered"
+
+    def __init__(self, rate, n, ctas=0, device=None):
+        torch = _torch()
+        typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+        if typ != "B":
+            raise ValueError("the layered decoder serves Type B codes")
+        rowptr, addr = [np.ascontiguousarray(a, np.int32)
+                        for a in C.address_rows(rate, n)]
+        h = ctypes.c_void_p()
+        N.call("atsc3_ldpc_layered_plan_create", n, K, Q2, rowptr.ctypes.data,
+               addr.ctypes.data, ctypes.byref(h))
+        self._h = h
+        self.n, self.rate, self.dtype = n, rate, "float32"
+        self.device = torch.device(device or "cuda")
+        if not ctas:
+            sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+            ctas = 2 * sms
+        self.ctas = int(ctas)
+        nbytes = ctypes.c_int64()
+        N.call("atsc3_ldpc_layered_workspace", h, self.ctas, ctypes.byref(nbytes))
+        self.ws = torch.empty(nbytes.value, dtype=torch.uint8, device=self.device)
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                N.lib().atsc3_ldpc_layered_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def decode_layered(plan, llr, iters=50, alpha=0.75, want_bits=True,
+                   want_hard=False, out=None, stream=None):
+    """Layered decode of (nblk, n) float32 CUDA LLRs; same outputs as
+    decode_flood.  Raises if a staged copy timed out (bounded waits)."""
+    torch = _torch()
+    if llr.dtype != torch.float32 or llr.device.type != "cuda":
+        raise TypeError("llr must be a CUDA float32 tensor")
+    if llr.dim() != 2 or llr.shape[1] != plan.n or llr.stride(1) != 1:
+        raise ValueError("llr must be (nblk, n) with unit column stride")
+    nblk = llr.shape[0]
+    dev = llr.device
+    o = out if out is not None else {}
+    if want_bits and "bits" not in o:
+        o["bits"] = torch.empty((nblk, plan.n), dtype=torch.uint8, device=dev)
+    if want_hard and "hard" not in o:
+        o["hard"] = torch.empty((nblk, (plan.n + 31) // 32 * 4),
+                                dtype=torch.uint8, device=dev)
+    for k, dt in (("conv", torch.uint8), ("its", torch.int32),
+                  ("bad", torch.int32)):
+        if k not in o:
+            o[k] = torch.empty(nblk, dtype=dt, device=dev)
+    bits = o.get("bits") if want_bits else None
+    hard = o.get("hard") if want_hard else None
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    N.call("atsc3_ldpc_layered_decode", plan.handle, llr.data_ptr(),
+           llr.stride(0), nblk, int(iters), float(alpha), N.ptr(bits),
+           bits.stride(0) if bits is not None else 0, N.ptr(hard),
+           hard.stride(0) if hard is not None else 0, o["conv"].data_ptr(),
+           o["its"].data_ptr(), o["bad"].data_ptr(), plan.ws.data_ptr(),
+           plan.ctas, plan.err.data_ptr(), st)
+    return o
+
+
+def check_layered_error(plan):
+    """Raise if a layered launch recorded a copy timeout (syncs)."""
+    if int(plan.err.item()) != 0:
+        plan.err.zero_()
+        raise N.FecError("atsc3_ldpc_layered_decode", -2,
+                         "a staged copy did not complete (bounded wait)")

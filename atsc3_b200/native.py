@@ -52,6 +52,14 @@ SIGNATURES = {
     "atsc3_ldpc_qc_decode": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32, c_f32,
                                      c_i32, c_vp, c_i64, c_vp, c_i64, c_vp,
                                      c_vp, c_vp, c_i32, c_vp]),
+    "atsc3_ldpc_layered_plan_create": (c_i32, [c_i32, c_i32, c_i32, c_vp,
+                                               c_vp, c_vp]),
+    "atsc3_ldpc_layered_plan_destroy": (None, [c_vp]),
+    "atsc3_ldpc_layered_workspace": (c_i32, [c_vp, c_i32, c_vp]),
+    "atsc3_ldpc_layered_decode": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32,
+                                          c_f32, c_vp, c_i64, c_vp, c_i64,
+                                          c_vp, c_vp, c_vp, c_vp, c_i32, c_vp,
+                                          c_vp]),
     "atsc3_demap": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32, c_i32,
                             c_vp, c_i64, c_f32, c_vp, c_vp, c_i64, c_vp]),
     "atsc3_demap_row_sigma2": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,

@@ -163,6 +163,32 @@ int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *plan, const float *llr,
                              uint8_t *conv, int32_t *its, int32_t *bad,
                              int32_t threads, void *stream);
 
+/* ---- layered decoder for the A/322 Type B codes ----------------------------
+ * Layered normalised min-sum: the Q block rows are the layers, the posterior
+ * is updated in place after each layer, syndrome before the first and after
+ * every full iteration (csrc/ldpc_layered.cu; the bit-exact CPU statement is
+ * oracle_layered_f32).  No reference counterpart: the reference decodes
+ * flooding only.  One CTA per codeword; per-CTA scratch (posterior + check
+ * records) lives in the caller's workspace, sized by
+ * atsc3_ldpc_layered_workspace for `ctas` resident CTAs.  Bounded waits: a
+ * copy that never completes sets *err = 1 (device int32, caller-zeroed). */
+typedef struct atsc3_ldpc_layered_plan atsc3_ldpc_layered_plan;
+
+int32_t atsc3_ldpc_layered_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
+                                       const int32_t *rowptr,
+                                       const int32_t *addr,
+                                       atsc3_ldpc_layered_plan **out);
+void atsc3_ldpc_layered_plan_destroy(atsc3_ldpc_layered_plan *plan);
+int32_t atsc3_ldpc_layered_workspace(const atsc3_ldpc_layered_plan *plan,
+                                     int32_t ctas, int64_t *bytes);
+int32_t atsc3_ldpc_layered_decode(const atsc3_ldpc_layered_plan *plan,
+                                  const float *llr, int64_t ld_llr,
+                                  int32_t nblk, int32_t iters, float alpha,
+                                  uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+                                  int64_t ld_hard, uint8_t *conv, int32_t *its,
+                                  int32_t *bad, void *workspace, int32_t ctas,
+                                  int32_t *err, void *stream);
+
 /* NUC max-log soft demapper with the bit de-interleaver in its epilogue.
  * cells: (nblk, ld_cells) complex64 as interleaved float pairs.
  * pts: 3*M floats: Re p, Im p, |p|^2 (float32, |p|^2 rounded once from

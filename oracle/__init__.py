@@ -59,8 +59,9 @@ def oracle_lib():
     L.oracle_flood_f64.restype = i32
     L.oracle_flood_f64.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp, i32,
                                    ctypes.c_double, i32, vp, vp, vp, vp]
-    if hasattr(L, "oracle_layered_f32"):
-        L.oracle_layered_f32.restype = i32
+    L.oracle_layered_f32.restype = i32
+    L.oracle_layered_f32.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp, i32,
+                                     ctypes.c_float, vp, vp, vp, vp]
     return L
 
 
@@ -384,3 +385,51 @@ def bch_syndrome_fast(bits2d, n):
             x = (x << 1) | int(row[j])
         out.append(x)
     return out
+
+
+def qc_row_slots(rate, n):
+    """Block-row slot lists of a quasi-cyclic Type B code, built from the
+    Annex A address rows: (Q, rptr, col, u, wrap).  Row r, in position
+    order: its information circulants by block column (column g, shift
+    x // Q for entry x with x % Q == r), then the dual-diagonal parity slots
+    (columns K/360 + r - 1 and K/360 + r; row 0: K/360 and the wrap slot
+    K/360 + Q - 1 with shift 1)."""
+    typ, K, M1, M2, Q1, Q = C.ldpc_params(rate, n)
+    if typ != "B":
+        raise ValueError("layered oracle: Type B codes only")
+    rowptr, addr = C.address_rows(rate, n)
+    nbi = K // 360
+    rows = [[] for _ in range(Q)]
+    for g in range(nbi):
+        for x in addr[rowptr[g]:rowptr[g + 1]]:
+            rows[x % Q].append((g, x // Q, 0))
+    rp, col, u, wrap = [0], [], [], []
+    for r in range(Q):
+        sl = sorted(rows[r])
+        if len(set(g for g, _, _ in sl)) != len(sl):
+            raise ValueError("two circulants share a block: not layerable")
+        sl += [(nbi + r - 1, 0, 0), (nbi + r, 0, 0)] if r else \
+              [(nbi, 0, 0), (nbi + Q - 1, 1, 1)]
+        for g, uu, w in sl:
+            col.append(g)
+            u.append(uu)
+            wrap.append(w)
+        rp.append(len(col))
+    return (Q,) + tuple(np.asarray(a, np.int32) for a in (rp, col, u, wrap))
+
+
+def layered(llr, rate, n, iters=50, alpha=0.75):
+    """Oracle layered decode (the GPU layered schedule): (bits, conv, its, bad)."""
+    Q, rp, col, u, wrap = qc_row_slots(rate, n)
+    llr = np.ascontiguousarray(llr, np.float32)
+    nblk = llr.shape[0]
+    bits = np.zeros((nblk, n), np.uint8)
+    conv = np.zeros(nblk, np.uint8)
+    its = np.zeros(nblk, np.int32)
+    bad = np.zeros(nblk, np.int32)
+    rc = oracle_lib().oracle_layered_f32(
+        _p(llr), nblk, n, Q, _p(rp), _p(col), _p(u), _p(wrap), int(iters),
+        float(alpha), _p(bits), _p(conv), _p(its), _p(bad))
+    if rc != 0:
+        raise RuntimeError(f"oracle layered decode returned {rc}")
+    return bits, conv.astype(bool), its, bad
