@@ -219,6 +219,13 @@ struct QcArgs {
   const int4 *cdesc;
   const int32_t *cptr;
   const uint8_t *s0;
+  // optional learned weights: record minima become relu(min*w_a - w_b) with
+  // (w_a, w_b) = (walpha, wbeta)[min(it, wT-1)][dbucket[check degree]];
+  // null -> (alpha, 0), which is bit-identical to min*alpha
+  const float *walpha;
+  const float *wbeta;
+  const int8_t *dbucket;
+  int wT, wnb;
   uint8_t *bits;
   int64_t ld_bits;
   uint8_t *hard;
@@ -340,8 +347,20 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qc_kernel(const QcArgs a) {
         if (kv) {
           uint32_t hi = 0;
           if constexpr (MB > 32) hi = (uint32_t)((unsigned long long)sv >> 32) << 8;
-          rec[li] = make_uint4(__float_as_uint(__fmul_rn(min1, a.alpha)),
-                               __float_as_uint(__fmul_rn(min2, a.alpha)),
+          float wa = a.alpha, wb = 0.f;
+          if (a.walpha) {
+            int nl;
+            if constexpr (MB > 32) nl = __popcll((unsigned long long)live);
+            else nl = __popc((uint32_t)live);
+            const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+            wa = __ldg(a.walpha + wi);
+            wb = __ldg(a.wbeta + wi);
+          }
+          float A = __fsub_rn(__fmul_rn(min1, wa), wb);
+          float B = __fsub_rn(__fmul_rn(min2, wa), wb);
+          A = A > 0.f ? A : 0.f;
+          B = B > 0.f ? B : 0.f;
+          rec[li] = make_uint4(__float_as_uint(A), __float_as_uint(B),
                                (uint32_t)sv, first | hi);
           mybad += syn;
         }
@@ -669,12 +688,33 @@ int32_t atsc3_ldpc_qc_config(const atsc3_ldpc_qc_plan *h, int32_t threads,
   return 0;
 }
 
+int32_t atsc3_ldpc_qc_decode_weighted(
+    const atsc3_ldpc_qc_plan *h, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream);
+
 int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *h, const float *llr,
                              int64_t ld_llr, int32_t nblk, int32_t iters,
                              float alpha, int32_t semantics, uint8_t *bits,
                              int64_t ld_bits, uint8_t *hard, int64_t ld_hard,
                              uint8_t *conv, int32_t *its, int32_t *bad,
                              int32_t threads, void *stream) {
+  return atsc3_ldpc_qc_decode_weighted(h, llr, ld_llr, nblk, iters, alpha,
+                                       semantics, nullptr, nullptr, 0, 0,
+                                       nullptr, bits, ld_bits, hard, ld_hard,
+                                       conv, its, bad, threads, stream);
+}
+
+int32_t atsc3_ldpc_qc_decode_weighted(
+    const atsc3_ldpc_qc_plan *h, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream) {
   using namespace atsc3;
   ATSC3_ARG(h != nullptr, "null plan");
   const QcPlan &p = h->p;
@@ -727,6 +767,15 @@ int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *h, const float *llr,
   a.cdesc = p.d_cdesc;
   a.cptr = p.d_cptr;
   a.s0 = p.d_s0;
+  if (walpha) {
+    ATSC3_ARG(wbeta && dbucket && wT > 0 && wnb > 0,
+              "weights need wbeta, dbucket, wT > 0, wnb > 0");
+    a.walpha = walpha;
+    a.wbeta = wbeta;
+    a.dbucket = dbucket;
+    a.wT = wT;
+    a.wnb = wnb;
+  }
   a.bits = bits;
   a.ld_bits = ld_bits;
   a.hard = hard;

@@ -145,10 +145,11 @@ def plan_for(rate, n, dtype="float32", cluster=0, kind="auto"):
 
 def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
                  want_bits=True, want_hard=False, threads=0, out=None,
-                 stream=None):
+                 stream=None, weights=None):
     """Decode (nblk, n) device LLRs.  Returns a dict of device tensors:
     bits (uint8, nblk x n) and/or hard (packed, nblk x ceil(n/32)*4 bytes),
-    conv (uint8), its (int32), bad (int32)."""
+    conv (uint8), its (int32), bad (int32).  weights: optional learned
+    (walpha, wbeta, dbucket) device tensors (quasi-cyclic plans only)."""
     torch = _torch()
     want_t = torch.float64 if plan.dtype == "float64" else torch.float32
     if llr.dtype != want_t or llr.device.type != "cuda":
@@ -170,10 +171,18 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     bits = o.get("bits") if want_bits else None
     hard = o.get("hard") if want_hard else None
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    if weights is not None and getattr(plan, "kind", "csr") != "qc":
+        raise ValueError("learned weights run on the quasi-cyclic decoder")
     if getattr(plan, "kind", "csr") == "qc":
-        N.call("atsc3_ldpc_qc_decode", plan.handle, llr.data_ptr(),
+        wa = wb = db = None
+        wT = wnb = 0
+        if weights is not None:
+            wa, wb, db = weights
+            wT, wnb = wa.shape
+        N.call("atsc3_ldpc_qc_decode_weighted", plan.handle, llr.data_ptr(),
                llr.stride(0), nblk, int(iters), float(alpha),
-               SEMANTICS[semantics], N.ptr(bits),
+               SEMANTICS[semantics], N.ptr(wa), N.ptr(wb), wT, wnb, N.ptr(db),
+               N.ptr(bits),
                bits.stride(0) if bits is not None else 0, N.ptr(hard),
                hard.stride(0) if hard is not None else 0,
                o["conv"].data_ptr(), o["its"].data_ptr(), o["bad"].data_ptr(),

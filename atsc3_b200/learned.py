@@ -1,0 +1,278 @@
+"""Differentiable unrolled weighted min-sum and its learned weights.
+
+``WeightedMinSum`` (a ``torch.autograd.Function``) runs the forward and the
+hand-written backward kernels of ``csrc/wms.cu``: T flooding iterations with
+per-iteration, per-check-degree scale ``alpha[t, d]`` and offset
+``beta[t, d]`` (messages ``sgn * relu(alpha * mu - beta)``), checkpointing one
+16-byte record per check per iteration and recomputing messages in the
+backward.  ``reference_f64`` is the same forward in float64 torch ops whose
+autograd gradient (and finite differences) check the kernels.
+
+``train`` fits the weights on LLRs produced by this package's own demapper
+from seeded synthetic blocks (mean BCE of the output LLRs against the
+transmitted bits, LLR > 0 meaning bit 0); ``save_weights`` / ``load_weights``
+keep them with a manifest (code, iterations, degree buckets, seed, step) so
+training resumes by step.
+"""
+from __future__ import annotations
+
+import ctypes
+import functools
+import json
+import os
+
+import numpy as np
+
+from . import codes as C
+from . import native as N
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@functools.lru_cache(maxsize=None)
+def host_tables(rate, n):
+    """CSR tables + per variable-major edge (check, position) + per-check
+    degree bucket.  Buckets = the code's distinct check degrees, ascending."""
+    cptr, cidx, vptr, vedge = C.csr(rate, n)
+    deg = np.diff(cptr)
+    if deg.max() > 32:
+        raise ValueError("weighted min-sum serves check degrees <= 32")
+    chk = np.repeat(np.arange(len(deg), dtype=np.int32), deg)
+    pos = (np.arange(len(cidx)) - cptr[chk]).astype(np.int32)
+    buckets = np.unique(deg)
+    cb = np.searchsorted(buckets, deg).astype(np.int8)
+    return dict(cptr=cptr, cidx=cidx, vptr=vptr, vedge=vedge,
+                vchk=chk[vedge].astype(np.int32), vpos=pos[vedge],
+                cbucket=cb, buckets=buckets, n=n, nc=len(deg), ne=len(cidx))
+
+
+class WmsCode:
+    """Device copy of host_tables for one code."""
+
+    def __init__(self, rate, n, device="cuda"):
+        torch = _torch()
+        h = host_tables(rate, n)
+        self.rate, self.n = rate, n
+        self.nc, self.ne = h["nc"], h["ne"]
+        self.buckets = h["buckets"]
+        self.nbucket = len(self.buckets)
+        self.dev = torch.device(device)
+        self.t = {k: torch.from_numpy(np.array(h[k])).to(self.dev)
+                  for k in ("cptr", "cidx", "vptr", "vedge", "vchk", "vpos",
+                            "cbucket")}
+
+    def ptrs(self):
+        t = self.t
+        return [t[k].data_ptr() for k in ("cptr", "cidx", "vptr", "vedge",
+                                          "vchk", "vpos", "cbucket")]
+
+    def init_params(self, iters, alpha=0.75, beta=0.0):
+        torch = _torch()
+        a = torch.full((iters, self.nbucket), float(alpha), device=self.dev)
+        b = torch.full((iters, self.nbucket), float(beta), device=self.dev)
+        return a, b
+
+
+class WeightedMinSum:
+    """torch.autograd.Function wrapper: out = WeightedMinSum.apply(llr,
+    alpha, beta, code, bf16).  llr (nblk, n) float32 CUDA (not
+    differentiated: it is data); alpha, beta (T, nbucket) float32."""
+
+    @staticmethod
+    def _fn():
+        torch = _torch()
+
+        class _F(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, llr, alpha, beta, code, bf16):
+                iters = alpha.shape[0]
+                nblk = llr.shape[0]
+                llr = llr.contiguous()
+                a = alpha.detach().contiguous().float()
+                b = beta.detach().contiguous().float()
+                rec = torch.empty((iters, nblk, code.nc, 16), dtype=torch.uint8,
+                                  device=llr.device)
+                out = torch.empty_like(llr)
+                N.call("atsc3_wms_forward", *code.ptrs(), code.n, code.nc,
+                       code.ne, code.nbucket, nblk, iters, llr.data_ptr(),
+                       a.data_ptr(), b.data_ptr(), int(bool(bf16)),
+                       rec.data_ptr(), out.data_ptr(),
+                       torch.cuda.current_stream(llr.device).cuda_stream)
+                ctx.save_for_backward(llr, a, b, rec)
+                ctx.code = code
+                return out
+
+            @staticmethod
+            def backward(ctx, g):
+                llr, a, b, rec = ctx.saved_tensors
+                code = ctx.code
+                iters, nblk = a.shape[0], llr.shape[0]
+                gt = g.contiguous().float().clone()
+                ga = torch.zeros_like(a)
+                gb = torch.zeros_like(b)
+                work = torch.empty(nblk * code.n + 2 * nblk * code.ne,
+                                   dtype=torch.float32, device=llr.device)
+                N.call("atsc3_wms_backward", *code.ptrs(), code.n, code.nc,
+                       code.ne, code.nbucket, nblk, iters, llr.data_ptr(),
+                       a.data_ptr(), b.data_ptr(), rec.data_ptr(),
+                       gt.data_ptr(), ga.data_ptr(), gb.data_ptr(),
+                       work.data_ptr(),
+                       torch.cuda.current_stream(llr.device).cuda_stream)
+                return None, ga, gb, None, None
+
+        return _F
+
+    _F = None
+
+    @classmethod
+    def apply(cls, llr, alpha, beta, code, bf16=False):
+        if cls._F is None:
+            cls._F = cls._fn()
+        return cls._F.apply(llr, alpha, beta, code, bf16)
+
+
+def reference_f64(llr, alpha, beta, rate, n):
+    """The weighted min-sum forward in float64 torch ops (CPU), for autograd
+    and finite-difference checks.  Same rules as csrc/wms.cu: first-minimum
+    arg-min, sign(x) = -1 iff x < 0, relu(alpha*mu - beta)."""
+    torch = _torch()
+    h = host_tables(rate, n)
+    cptr, cidx = h["cptr"], h["cidx"]
+    deg = np.diff(cptr)
+    nc, dmax = len(deg), int(deg.max())
+    idx = np.full((nc, dmax), n, np.int64)
+    mask = np.zeros((nc, dmax), bool)
+    for c in range(nc):
+        idx[c, :deg[c]] = cidx[cptr[c]:cptr[c + 1]]
+        mask[c, :deg[c]] = True
+    idx_t = torch.from_numpy(idx)
+    mask_t = torch.from_numpy(mask)
+    cb = torch.from_numpy(h["cbucket"].astype(np.int64))
+    llr = llr.double()
+    nb = llr.shape[0]
+    iters = alpha.shape[0]
+    ar = torch.arange(dmax)
+    inf = torch.tensor(float("inf"), dtype=torch.float64)
+    m = torch.zeros((nb, nc, dmax), dtype=torch.float64)
+    tot = llr
+    for t in range(iters):
+        tp = torch.cat([tot, torch.zeros((nb, 1), dtype=torch.float64)], 1)
+        x = tp[:, idx_t] - m
+        sx = (x < 0) & mask_t
+        par = (sx.sum(-1) % 2).bool()
+        mag = torch.where(mask_t, x.abs(), inf)
+        mn = mag.detach()
+        min1v = mn.min(-1, keepdim=True).values
+        first = ((mn == min1v).long() * (dmax - ar)).argmax(-1, keepdim=True)
+        mn2 = mn.scatter(-1, first, float("inf"))
+        min2v = mn2.min(-1, keepdim=True).values
+        second = ((mn2 == min2v).long() * (dmax - ar)).argmax(-1, keepdim=True)
+        min1 = mag.gather(-1, first)
+        min2 = mag.gather(-1, second)
+        mu = torch.where(ar == first, min2, min1)
+        a = alpha[t][cb].double()[None, :, None] * mu - beta[t][cb].double()[None, :, None]
+        sgn = torch.where(par[..., None] ^ sx, -1.0, 1.0).double()
+        m = torch.where(mask_t, sgn * torch.relu(a), torch.zeros((), dtype=torch.float64))
+        s = torch.zeros((nb, n + 1), dtype=torch.float64)
+        s = s.index_add(1, idx_t.reshape(-1), m.reshape(nb, -1))
+        tot = llr + s[:, :n]
+    return tot
+
+
+def bce_loss(out_llr, bits):
+    """Mean BCE of output LLRs against the true bits (LLR > 0 = bit 0)."""
+    torch = _torch()
+    return torch.nn.functional.binary_cross_entropy_with_logits(
+        -out_llr, bits.to(out_llr.dtype))
+
+
+# ---------------------------------------------------------------------------
+# training on the package's own demapper output
+# ---------------------------------------------------------------------------
+
+def make_batch(tx, gen, nblk, esn0_lo, esn0_hi, channel="awgn", device="cuda"):
+    """Seeded blocks -> (llr (nblk, n) float32 codeword order, codewords)."""
+    torch = _torch()
+    from . import demap as DM
+    from . import synth
+    pay = torch.randint(0, 2, (nblk, tx.kp), generator=gen, device=device,
+                        dtype=torch.uint8)
+    x, cw = tx.encode(pay)
+    esn0 = torch.rand(nblk, generator=gen, device=device) * (esn0_hi - esn0_lo) + esn0_lo
+    ys, ss = [], []
+    for i in range(nblk):
+        y, s2 = synth.channel(x[i:i + 1], float(esn0[i]), channel, gen)
+        ys.append(y)
+        ss.append(s2 if channel == "rayleigh" else
+                  torch.full((1, x.shape[1]), float(s2), device=device))
+    y = torch.cat(ys)
+    s2 = torch.cat(ss)
+    lam = DM.demap(y, tx.mod, tx.rate, sigma2=s2, n=tx.n)
+    return lam, cw
+
+
+def save_weights(path, alpha, beta, manifest):
+    torch = _torch()
+    torch.save({"alpha": alpha.detach().cpu(), "beta": beta.detach().cpu(),
+                "manifest": manifest}, path)
+
+
+def load_weights(path, device="cuda"):
+    torch = _torch()
+    d = torch.load(path, map_location="cpu")
+    return d["alpha"].to(device), d["beta"].to(device), d["manifest"]
+
+
+def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
+          channel="awgn", seed=1, bf16=False, log_every=50, resume=None,
+          device="cuda"):
+    """Adam on (alpha, beta) of the unrolled decoder; returns (alpha, beta,
+    history).  Fresh seeded blocks every step."""
+    torch = _torch()
+    from . import synth
+    code = WmsCode(rate, n, device)
+    tx = synth.Transmitter(n, mod, rate, device=device)
+    alpha, beta = code.init_params(iters)
+    start = 0
+    if resume is not None:
+        a0, b0, man = load_weights(resume, device)
+        alpha.copy_(a0)
+        beta.copy_(b0)
+        start = int(man.get("step", 0))
+    alpha.requires_grad_(True)
+    beta.requires_grad_(True)
+    opt = torch.optim.Adam([alpha, beta], lr=lr)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed + start)
+    hist = []
+    for step in range(start, start + steps):
+        lam, cw = make_batch(tx, gen, nblk, esn0[0], esn0[1], channel, device)
+        out = WeightedMinSum.apply(lam, alpha, beta, code, bf16)
+        loss = bce_loss(out, cw)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            beta.clamp_(min=0.0)
+        if step % log_every == 0 or step == start + steps - 1:
+            hist.append((step, float(loss)))
+    manifest = {"rate": rate, "n": n, "mod": mod, "iters": iters,
+                "buckets": [int(x) for x in code.buckets], "seed": seed,
+                "step": start + steps, "esn0": list(esn0), "channel": channel,
+                "bf16": bool(bf16)}
+    return alpha.detach(), beta.detach(), hist, manifest
+
+
+def inference_weights(alpha, beta, buckets, device="cuda"):
+    """(walpha, wbeta, dbucket) device tensors for the quasi-cyclic decoder:
+    dbucket[degree] = bucket index of that check degree."""
+    torch = _torch()
+    db = np.zeros(64, np.int8)
+    for i, d in enumerate(buckets):
+        db[int(d)] = i
+    return (alpha.detach().float().contiguous().to(device),
+            beta.detach().float().contiguous().to(device),
+            torch.from_numpy(db).to(device))

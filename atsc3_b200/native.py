@@ -60,6 +60,15 @@ SIGNATURES = {
                                           c_f32, c_vp, c_i64, c_vp, c_i64,
                                           c_vp, c_vp, c_vp, c_vp, c_i32, c_vp,
                                           c_vp]),
+    "atsc3_wms_forward": (c_i32, [c_vp] * 7 + [c_i32] * 6 + [c_vp, c_vp, c_vp,
+                                                             c_i32, c_vp, c_vp,
+                                                             c_vp]),
+    "atsc3_wms_backward": (c_i32, [c_vp] * 7 + [c_i32] * 6 + [c_vp] * 9),
+    "atsc3_ldpc_qc_decode_weighted": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32,
+                                              c_f32, c_i32, c_vp, c_vp, c_i32,
+                                              c_i32, c_vp, c_vp, c_i64, c_vp,
+                                              c_i64, c_vp, c_vp, c_vp, c_i32,
+                                              c_vp]),
     "atsc3_demap": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32, c_i32,
                             c_vp, c_i64, c_f32, c_vp, c_vp, c_i64, c_vp]),
     "atsc3_demap_row_sigma2": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,

@@ -163,6 +163,19 @@ int32_t atsc3_ldpc_qc_decode(const atsc3_ldpc_qc_plan *plan, const float *llr,
                              uint8_t *conv, int32_t *its, int32_t *bad,
                              int32_t threads, void *stream);
 
+/* As atsc3_ldpc_qc_decode with learned weights: each check's record minima
+ * become relu(min*wa - wb), (wa, wb) = (walpha, wbeta)[min(it, wT-1)][
+ * dbucket[check degree]] for the update of iteration it (0-based);
+ * walpha/wbeta (wT, wnb) float32 and dbucket (64) int8 are device arrays.
+ * With walpha == NULL it is atsc3_ldpc_qc_decode. */
+int32_t atsc3_ldpc_qc_decode_weighted(
+    const atsc3_ldpc_qc_plan *plan, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream);
+
 /* ---- layered decoder for the A/322 Type B codes ----------------------------
  * Layered normalised min-sum: the Q block rows are the layers, the posterior
  * is updated in place after each layer, syndrome before the first and after
@@ -188,6 +201,34 @@ int32_t atsc3_ldpc_layered_decode(const atsc3_ldpc_layered_plan *plan,
                                   int64_t ld_hard, uint8_t *conv, int32_t *its,
                                   int32_t *bad, void *workspace, int32_t ctas,
                                   int32_t *err, void *stream);
+
+/* ---- differentiable weighted min-sum ---------------------------------------
+ * Unrolled flooding min-sum with per-iteration, per-check-degree scale and
+ * offset: m = sgn * relu(alpha[t][d] * mu - beta[t][d]) (csrc/wms.cu).  No
+ * reference counterpart.  Tables: device CSR (cptr, cidx, vptr, vedge), the
+ * check and position of each variable-major edge (vchk, vpos), the degree
+ * bucket of each check (int8).  records: (iters, nblk, nc) 16-byte per-check
+ * checkpoints written by the forward and read by the backward.  Forward
+ * writes tot_out = the posterior after `iters` iterations (no early stop).
+ * Backward: gtot in = dL/dtot_out (overwritten), galpha/gbeta accumulate
+ * (caller zeroes), work = nblk*n + 2*nblk*ne floats. */
+int32_t atsc3_wms_forward(const int32_t *cptr, const int32_t *cidx,
+                          const int32_t *vptr, const int32_t *vedge,
+                          const int32_t *vchk, const int32_t *vpos,
+                          const int8_t *cbucket, int32_t n, int32_t nc,
+                          int32_t ne, int32_t nbucket, int32_t nblk,
+                          int32_t iters, const float *llr, const float *alpha,
+                          const float *beta, int32_t bf16, void *records,
+                          float *tot_out, void *stream);
+int32_t atsc3_wms_backward(const int32_t *cptr, const int32_t *cidx,
+                           const int32_t *vptr, const int32_t *vedge,
+                           const int32_t *vchk, const int32_t *vpos,
+                           const int8_t *cbucket, int32_t n, int32_t nc,
+                           int32_t ne, int32_t nbucket, int32_t nblk,
+                           int32_t iters, const float *llr, const float *alpha,
+                           const float *beta, const void *records, float *gtot,
+                           float *galpha, float *gbeta, float *work,
+                           void *stream);
 
 /* NUC max-log soft demapper with the bit de-interleaver in its epilogue.
  * cells: (nblk, ld_cells) complex64 as interleaved float pairs.

@@ -1,0 +1,133 @@
+"""The hand-written weighted min-sum kernels (forward + backward) against the
+float64 autograd reference on 4 blocks of the 64800-bit rate-8/15 code, the
+plain-normalised special case, and the BF16-message variant."""
+import numpy as np
+import pytest
+
+from atsc3_b200 import codes as C
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(seed=5, nb=4, n=64800, rate="8/15"):
+    import oracle
+    c_rng = np.random.default_rng(seed)
+    tx = lambda p: oracle.transmit(p, n, "64QAM", rate)[0]
+    pay, cells, s2 = oracle.synth_case(tx, nb, C.kpayload(rate, n),
+                                       C.cells_per_block(n, "64QAM"), 11.5,
+                                       "awgn", seed)
+    q = oracle.demap(cells, C.points_for("64QAM", rate), 6, s2)
+    lam = oracle.deinterleave(q, C.bicm_map(n, "64QAM", rate), n)
+    cw = oracle.transmit(pay, n, "64QAM", rate)[1]
+    return lam, cw
+
+
+def test_wms_forward_and_gradients_vs_float64_reference():
+    import torch
+    from atsc3_b200.learned import (WeightedMinSum, WmsCode, bce_loss,
+                                    reference_f64)
+    rate, n, T = "8/15", 64800, 12
+    lam, cw = _case()
+    code = WmsCode(rate, n)
+    rng = np.random.default_rng(7)
+    a0 = (0.7 + 0.2 * rng.random((T, code.nbucket))).astype(np.float32)
+    b0 = (0.1 * rng.random((T, code.nbucket))).astype(np.float32)
+    a = torch.tensor(a0, device="cuda", requires_grad=True)
+    b = torch.tensor(b0, device="cuda", requires_grad=True)
+    x = torch.from_numpy(lam).cuda()
+    bits = torch.from_numpy(cw).cuda()
+    out = WeightedMinSum.apply(x, a, b, code, False)
+    loss = bce_loss(out, bits)
+    loss.backward()
+    a64 = torch.tensor(a0, dtype=torch.float64, requires_grad=True)
+    b64 = torch.tensor(b0, dtype=torch.float64, requires_grad=True)
+    ref = reference_f64(torch.from_numpy(lam), a64, b64, rate, n)
+    lref = bce_loss(ref, torch.from_numpy(cw).double())
+    lref.backward()
+    o = out.detach().cpu().double().numpy()
+    r = ref.detach().numpy()
+    close = np.abs(o - r) <= 1e-3 * np.maximum(1.0, np.abs(r))
+    assert close.mean() > 0.999, close.mean()
+    assert abs(float(loss) - float(lref)) <= 1e-4 * abs(float(lref))
+    for g, gr in ((a.grad, a64.grad), (b.grad, b64.grad)):
+        g = g.cpu().double().numpy()
+        gr = gr.numpy()
+        rel = np.abs(g - gr).max() / max(np.abs(gr).max(), 1e-12)
+        assert rel < 1e-2, rel
+
+
+def test_wms_unweighted_equals_plain_minsum_hard_decisions():
+    """alpha = 0.75, beta = 0 for T iterations is the normalised min-sum
+    without early stop: same hard decisions as the float32 oracle when the
+    oracle runs the same number of updates (torch semantics)."""
+    import torch
+    import oracle
+    from atsc3_b200.learned import WeightedMinSum, WmsCode
+    rate, n, T = "8/15", 64800, 6
+    lam, cw = _case(seed=9)
+    code = WmsCode(rate, n)
+    a, b = code.init_params(T, 0.75, 0.0)
+    out = WeightedMinSum.apply(torch.from_numpy(lam).cuda(), a, b, code, False)
+    want = oracle.flood(lam, C.csr(rate, n), n, iters=T, alpha=0.75, semantics=1)
+    got = (out.cpu().numpy() < 0).astype(np.uint8)
+    for i in range(len(lam)):
+        if not want[1][i]:                # no early stop happened: same T
+            assert (got[i] != want[0][i]).mean() < 1e-3
+
+
+def test_wms_bf16_messages_close_to_fp32():
+    import torch
+    from atsc3_b200.learned import WeightedMinSum, WmsCode, bce_loss
+    rate, n, T = "8/15", 64800, 12
+    lam, cw = _case(seed=11)
+    code = WmsCode(rate, n)
+    a, b = code.init_params(T, 0.8, 0.05)
+    x = torch.from_numpy(lam).cuda()
+    bits = torch.from_numpy(cw).cuda()
+    l32 = float(bce_loss(WeightedMinSum.apply(x, a, b, code, False), bits))
+    l16 = float(bce_loss(WeightedMinSum.apply(x, a, b, code, True), bits))
+    assert abs(l16 - l32) <= 0.05 * abs(l32) + 1e-4
+
+
+def test_weighted_qc_decoder_matches_wms_forward():
+    """The inference decoder with learned weights (quasi-cyclic, torch
+    semantics) computes the same posterior as the differentiable forward for
+    blocks that run all T iterations: identical hard decisions."""
+    import torch
+    from atsc3_b200.ldpc import decode_flood, plan_for
+    from atsc3_b200.learned import WeightedMinSum, WmsCode, inference_weights
+    rate, n, T = "8/15", 64800, 12
+    lam, cw = _case(seed=13, nb=6)
+    lam[:3] *= 0.55                        # weaker blocks: no early stop
+    code = WmsCode(rate, n)
+    rng = np.random.default_rng(4)
+    a = torch.tensor(0.7 + 0.2 * rng.random((T, code.nbucket)), dtype=torch.float32, device="cuda")
+    b = torch.tensor(0.1 * rng.random((T, code.nbucket)), dtype=torch.float32, device="cuda")
+    x = torch.from_numpy(lam).cuda()
+    ref = (WeightedMinSum.apply(x, a, b, code, False) < 0).to(torch.uint8).cpu().numpy()
+    plan = plan_for(rate, n)
+    o = decode_flood(plan, x, iters=T, semantics="torch",
+                     weights=inference_weights(a, b, code.buckets))
+    its = o["its"].cpu().numpy()
+    bits = o["bits"].cpu().numpy()
+    ran_all = np.flatnonzero(~o["conv"].cpu().numpy().astype(bool))
+    assert len(ran_all) >= 1
+    for i in ran_all:
+        assert its[i] == T
+        assert np.array_equal(bits[i], ref[i])
+
+
+def test_weighted_qc_with_zero_offset_is_plain():
+    import torch
+    from atsc3_b200.ldpc import decode_flood, plan_for
+    from atsc3_b200.learned import WmsCode, inference_weights
+    rate, n = "8/15", 64800
+    lam, cw = _case(seed=15, nb=4)
+    code = WmsCode(rate, n)
+    a, b = code.init_params(5, 0.75, 0.0)
+    x = torch.from_numpy(lam).cuda()
+    plan = plan_for(rate, n)
+    p = decode_flood(plan, x, iters=50)
+    w = decode_flood(plan, x, iters=50, weights=inference_weights(a, b, code.buckets))
+    for k in ("bits", "conv", "its", "bad"):
+        assert torch.equal(p[k], w[k]), k
