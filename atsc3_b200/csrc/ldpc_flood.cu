@@ -437,6 +437,8 @@ __global__ void __launch_bounds__(1024, 1) ldpc_flood_kernel(const FloodArgs a) 
           a.its[b] = it;
           a.bad[b] = done ? 0 : badct;
         }
+        // outputs read posteriors the next codeword's prologue overwrites
+        __syncthreads();
         break;
       }
       // ---------------- variable phase ------------------------------------

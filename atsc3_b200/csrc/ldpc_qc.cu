@@ -399,6 +399,9 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qc_kernel(const QcArgs a) {
           a.its[b] = it;
           a.bad[b] = done ? 0 : badct;
         }
+        // the packing above reads posteriors other threads overwrite in the
+        // next codeword's prologue
+        __syncthreads();
         break;
       }
       // ---------------- variable phase -------------------------------------

@@ -1,0 +1,163 @@
+"""Learned vs plain normalised min-sum: thresholds, training, FER and
+iteration sweeps (all on the GPU, BCH as the arbiter).
+
+    python -m atsc3_b200.evaluate [--steps 2000] [--batch 256] [--blocks 100000]
+
+For each MODCOD (64800-bit rate 6/15 with 16-NUC, 8/15 with 64-NUC, 10/15
+with 256-NUC):
+1. threshold: the lowest Es/N0 (0.1 dB grid) at which the plain decoder
+   (alpha 0.75, at most 50 iterations, AWGN) reaches a block error rate of
+   1e-2 on 2000 seeded blocks -- the "3/3"-style search the reference uses
+   for its LDM thresholds, run with this decoder;
+2. training: per-iteration, per-check-degree scale/offset of the unrolled
+   12-iteration weighted min-sum (``learned.train``) on fresh seeded blocks
+   at Es/N0 uniform in [thr-0.5, thr+1.5], half AWGN, half Rayleigh gain;
+3. evaluation on held-out seeded blocks over an Es/N0 sweep: block errors
+   (BCH syndrome nonzero or information bits wrong), mean iterations and
+   decoded Mbit/s for the plain and the learned decoder, both the same
+   flooding schedule with early stop (iterations past 12 reuse the last
+   learned row).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import bch as BCH
+from . import codes as C
+from . import demap as DM
+from . import ldpc as LDPC
+from . import learned as LR
+from . import synth
+
+MODCODS = (("6/15", "16QAM"), ("8/15", "64QAM"), ("10/15", "256QAM"))
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def blocks(tx, gen, nblk, esn0, channel="awgn"):
+    """Seeded blocks at one Es/N0: (lam float32 codeword order, codewords)."""
+    torch = _torch()
+    pay = torch.randint(0, 2, (nblk, tx.kp), generator=gen, device=tx.dev,
+                        dtype=torch.uint8)
+    x, cw = tx.encode(pay)
+    y, s2 = synth.channel(x, esn0, channel, gen)
+    lam = DM.demap(y, tx.mod, tx.rate, sigma2=s2 if channel == "rayleigh" else float(s2),
+                   n=tx.n)
+    return lam, cw
+
+
+def decode_count(plan, lam, cw, kldpc, n, weights=None, iters=50, alpha=0.75):
+    """(block errors, sum of iterations, GPU ms) for one batch."""
+    torch = _torch()
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    e0.record()
+    o = LDPC.decode_flood(plan, lam, iters=iters, alpha=alpha, want_bits=True,
+                          want_hard=True, weights=weights)
+    e1.record()
+    chk = BCH.bch_check(o["hard"], kldpc, n, want_payload=False)
+    wrong = (o["bits"][:, :kldpc] != cw[:, :kldpc]).any(dim=1)
+    err = wrong | (chk["ok"] == 0)
+    torch.cuda.synchronize()
+    return int(err.sum()), int(o["its"].sum()), e0.elapsed_time(e1)
+
+
+def threshold(rate, mod, n=64800, target=1e-2, nblk=2000, seed=11, lo=-2.0,
+              hi=24.0):
+    torch = _torch()
+    tx = synth.Transmitter(n, mod, rate, device="cuda")
+    plan = LDPC.plan_for(rate, n)
+    K = C.kldpc(rate, n)
+
+    def fer(e):
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        errs = 0
+        for lo_ in range(0, nblk, 500):
+            lam, cw = blocks(tx, gen, min(500, nblk - lo_), e)
+            errs += decode_count(plan, lam, cw, K, n)[0]
+        return errs / nblk
+
+    # coarse-to-fine bisection on a 0.1 dB grid
+    while hi - lo > 0.1 + 1e-9:
+        mid = round((lo + hi) / 2 / 0.1) * 0.1
+        if mid <= lo or mid >= hi:
+            break
+        if fer(mid) <= target:
+            hi = mid
+        else:
+            lo = mid
+    return round(hi, 1)
+
+
+def sweep(rate, mod, weights, esn0s, nblk, n=64800, seed=99, chunk=2000):
+    torch = _torch()
+    tx = synth.Transmitter(n, mod, rate, device="cuda")
+    plan = LDPC.plan_for(rate, n)
+    K = C.kldpc(rate, n)
+    kp = C.kpayload(rate, n)
+    out = []
+    for e in esn0s:
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed + int(round(e * 10)))
+        acc = {"plain": [0, 0, 0.0], "learned": [0, 0, 0.0]}
+        for lo in range(0, nblk, chunk):
+            lam, cw = blocks(tx, gen, min(chunk, nblk - lo), e)
+            for name, w in (("plain", None), ("learned", weights)):
+                er, it, ms = decode_count(plan, lam, cw, K, n, weights=w)
+                acc[name][0] += er
+                acc[name][1] += it
+                acc[name][2] += ms
+        row = {"esn0_db": e, "blocks": nblk}
+        for name, (er, it, ms) in acc.items():
+            row[name] = {"fer": er / nblk, "block_errors": er,
+                         "mean_iters": it / nblk,
+                         "mbit_s": nblk * kp / (ms / 1e3) / 1e6}
+        out.append(row)
+    return out
+
+
+def run(steps=2000, batch=256, nblk=100000, points=6, out_dir=None, seed=1):
+    report = {}
+    out_dir = out_dir or os.path.join(HERE, "data")
+    for rate, mod in MODCODS:
+        t0 = time.time()
+        thr = threshold(rate, mod)
+        al, be, hist, man = LR.train(rate, 64800, mod, steps=steps, nblk=batch,
+                                     iters=12, esn0=(thr - 0.5, thr + 1.5),
+                                     channel="mixed", seed=seed,
+                                     log_every=max(1, steps // 10))
+        man["threshold_db"] = thr
+        path = os.path.join(out_dir, f"weights_{rate.replace('/', '_')}_{mod}.pt")
+        LR.save_weights(path, al, be, man)
+        code = LR.WmsCode(rate, 64800)
+        w = LR.inference_weights(al, be, code.buckets)
+        esn0s = [round(thr + 0.2 * i, 1) for i in range(points)]
+        rows = sweep(rate, mod, w, esn0s, nblk // points)
+        report[f"{rate} {mod}"] = {"threshold_db": thr, "train_loss": hist,
+                                   "weights": path, "sweep": rows,
+                                   "seconds": time.time() - t0}
+    return report
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--blocks", type=int, default=100000)
+    ap.add_argument("--points", type=int, default=6)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    print(json.dumps(run(a.steps, a.batch, a.blocks, a.points, a.out)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -194,22 +194,34 @@ def bce_loss(out_llr, bits):
 # ---------------------------------------------------------------------------
 
 def make_batch(tx, gen, nblk, esn0_lo, esn0_hi, channel="awgn", device="cuda"):
-    """Seeded blocks -> (llr (nblk, n) float32 codeword order, codewords)."""
+    """Seeded blocks -> (llr (nblk, n) float32 codeword order, codewords).
+
+    Es/N0 is drawn per block uniformly in [esn0_lo, esn0_hi]; channel
+    "awgn", "rayleigh" (per-cell |CN(0,1)| gain, equalised, per-cell sigma2)
+    or "mixed" (odd blocks Rayleigh).  LLRs come from this package's
+    demapper with the per-cell noise variance."""
     torch = _torch()
     from . import demap as DM
-    from . import synth
     pay = torch.randint(0, 2, (nblk, tx.kp), generator=gen, device=device,
                         dtype=torch.uint8)
     x, cw = tx.encode(pay)
-    esn0 = torch.rand(nblk, generator=gen, device=device) * (esn0_hi - esn0_lo) + esn0_lo
-    ys, ss = [], []
-    for i in range(nblk):
-        y, s2 = synth.channel(x[i:i + 1], float(esn0[i]), channel, gen)
-        ys.append(y)
-        ss.append(s2 if channel == "rayleigh" else
-                  torch.full((1, x.shape[1]), float(s2), device=device))
-    y = torch.cat(ys)
-    s2 = torch.cat(ss)
+    esn0 = torch.rand(nblk, 1, generator=gen, device=device) * (esn0_hi - esn0_lo) + esn0_lo
+    n0 = torch.pow(10.0, -esn0 / 10.0)
+
+    def cn():
+        re = torch.randn(x.shape, generator=gen, device=device)
+        im = torch.randn(x.shape, generator=gen, device=device)
+        return torch.complex(re, im) / np.sqrt(2.0)
+
+    if channel == "awgn":
+        h = torch.ones(x.shape, device=device)
+    else:
+        h = cn().abs()
+        if channel == "mixed":
+            odd = (torch.arange(nblk, device=device) % 2 == 1)[:, None]
+            h = torch.where(odd, h, torch.ones_like(h))
+    y = ((h * x + cn() * torch.sqrt(n0)) / h).to(torch.complex64)
+    s2 = (n0 / h ** 2).to(torch.float32)
     lam = DM.demap(y, tx.mod, tx.rate, sigma2=s2, n=tx.n)
     return lam, cw
 

@@ -325,3 +325,25 @@ def test_qc_decoder_vs_oracle(rate, cluster, torch):
         assert o["bad"].cpu().numpy().tolist() == want[3].tolist(), (rate, sem)
         assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
                               np.packbits(bits, axis=1))
+
+
+@pytest.mark.parametrize("kind", ["qc", "csr"])
+def test_many_codewords_per_cluster_outputs_consistent(kind, torch):
+    """More codewords than resident clusters: every cluster decodes several
+    codewords in turn; packed hard decisions, bits and status of every block
+    must match the oracle (a retire/prologue overlap would corrupt them)."""
+    from atsc3_b200 import ldpc as LDPC
+    rate, n = "10/15", 64800
+    rng = np.random.default_rng(31)
+    nb = 100
+    llr = (rng.standard_normal((nb, n)) * 1.5 + 2.5).astype(np.float32)
+    plan = LDPC.plan_for(rate, n, kind=kind)
+    o = LDPC.decode_flood(plan, torch.from_numpy(llr).cuda(), iters=8,
+                          want_hard=True)
+    bits = o["bits"].cpu().numpy()
+    assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
+                          np.packbits(bits, axis=1))
+    sel = [0, 33, 66, 99]
+    want = oracle.flood(llr[sel], C.csr(rate, n), n, iters=8)
+    assert np.array_equal(bits[sel], want[0])
+    assert o["its"].cpu().numpy()[sel].tolist() == want[2].tolist()
