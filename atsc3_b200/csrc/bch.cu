@@ -130,9 +130,69 @@ int32_t bch_bits_launch(const uint8_t *bits, int64_t ld_bits, int nblk,
   return 0;
 }
 
+// ---- uneven batches: per-block BCH length, tables and payload -------------
+struct BchBatchArgs {
+  const uint8_t *hard;
+  const int64_t *hard_off;
+  const int32_t *kldpc;
+  const uint32_t *rtab;
+  const int64_t *rtab_off;    // uint32 words
+  const uint8_t *scr;         // scrambling bytes (longest payload)
+  const int32_t *kpay;
+  uint8_t *payload;
+  const int64_t *pay_off;
+  uint32_t *syn;
+  uint8_t *ok;
+};
+
+__global__ void __launch_bounds__(256) bch_batch_kernel(const BchBatchArgs a) {
+  const int b = blockIdx.x;
+  const uint8_t *h = a.hard + a.hard_off[b];
+  const int kldpc = a.kldpc[b];
+  const uint32_t *rtab = a.rtab + a.rtab_off[b];
+  uint32_t acc[6] = {0, 0, 0, 0, 0, 0};
+  const int nword = kldpc >> 5;
+  const uint32_t *hw = reinterpret_cast<const uint32_t *>(h);
+  for (int w = threadIdx.x; w < nword; w += blockDim.x) {
+    uint32_t v = __ldg(hw + w);
+    while (v) {
+      const int t = __ffs(v) - 1;
+      v &= v - 1;
+      fold_row(acc, rtab, 32 * w + 8 * (t >> 3) + (7 - (t & 7)));
+    }
+  }
+  for (int pos = nword * 32 + threadIdx.x; pos < kldpc; pos += blockDim.x)
+    if ((h[pos >> 3] >> (7 - (pos & 7))) & 1) fold_row(acc, rtab, pos);
+  if (a.payload) {
+    uint8_t *po = a.payload + a.pay_off[b];
+    for (int j = threadIdx.x; j < (a.kpay[b] >> 3); j += blockDim.x)
+      po[j] = h[j] ^ __ldg(a.scr + j);
+  }
+  reduce_store(acc, a.syn + (size_t)b * 6, a.ok + b);
+}
+
 }  // namespace atsc3
 
 extern "C" {
+
+int32_t atsc3_bch_batch(const uint8_t *hard, const int64_t *hard_off,
+                        const int32_t *kldpc, const uint32_t *rtab,
+                        const int64_t *rtab_off, const uint8_t *scr,
+                        const int32_t *kpay, uint8_t *payload,
+                        const int64_t *pay_off, uint32_t *syn, uint8_t *ok,
+                        int32_t nblk, void *stream) {
+  using namespace atsc3;
+  ATSC3_ARG(nblk >= 0, "negative size");
+  if (nblk == 0) return 0;
+  ATSC3_ARG(hard && hard_off && kldpc && rtab && rtab_off && syn && ok, "null pointer");
+  ATSC3_ARG(!payload || (scr && kpay && pay_off), "payload needs scr, kpay, pay_off");
+  BchBatchArgs a{hard, hard_off, kldpc, rtab, rtab_off, scr, kpay, payload,
+                 pay_off, syn, ok};
+  bch_batch_kernel<<<nblk, 256, 0, (cudaStream_t)stream>>>(a);
+  ATSC3_CUDA(cudaGetLastError());
+  return 0;
+}
+
 
 int32_t atsc3_bch_check(const uint8_t *hard, int64_t ld_hard, int32_t nblk,
                         int32_t kldpc, const uint32_t *rtab, uint32_t *syn,

@@ -234,9 +234,91 @@ int32_t row_sigma_launch(const float *cells, int64_t ld_cells, int nblk,
   return 0;
 }
 
+// ---- uneven batches: every block its own constellation ---------------------
+// One CTA per chunk of up to 256 cells of one block (chunk_blk / chunk_start
+// built on the host); the CTA stages its block's alphabet (up to 4096
+// points) and dispatches on the block's bits per symbol.
+struct DemapBatchArgs {
+  const float2 *cells;
+  const int64_t *cell_off;
+  const int32_t *ncell;
+  const int32_t *nbits;
+  const float *pts;
+  const int64_t *pts_off;     // floats, 3*M per alphabet
+  const float *sigma2;        // one per block
+  const int32_t *lq;
+  const int64_t *lq_off;
+  float *llr;
+  const int64_t *llr_off;
+  const int32_t *chunk_blk;
+  const int32_t *chunk_start;
+};
+
+template <int NB>
+__device__ __forceinline__ void demap_cell_batch(const DemapBatchArgs &a, int b,
+                                                 int s, const float *sp) {
+  constexpr int M = 1 << NB;
+  const float2 z = a.cells[a.cell_off[b] + s];
+  float mn[NB][2];
+  cell_minima<NB>(z.x, z.y, sp, sp + M, sp + 2 * M, mn, nullptr);
+  const float s2 = a.sigma2[b];
+  const int32_t *lq = a.lq + a.lq_off[b];
+  float *o = a.llr + a.llr_off[b];
+#pragma unroll
+  for (int i = 0; i < NB; ++i)
+    o[__ldg(lq + s * NB + i)] = __fdiv_rn(__fsub_rn(mn[i][1], mn[i][0]), s2);
+}
+
+__global__ void __launch_bounds__(256) demap_batch_kernel(const DemapBatchArgs a) {
+  extern __shared__ float sp[];
+  const int b = a.chunk_blk[blockIdx.x];
+  const int s = a.chunk_start[blockIdx.x] + threadIdx.x;
+  const int nb = a.nbits[b];
+  const int M3 = 3 << nb;
+  const float *src = a.pts + a.pts_off[b];
+  for (int k = threadIdx.x; k < M3; k += blockDim.x) sp[k] = src[k];
+  __syncthreads();
+  if (s >= a.ncell[b]) return;
+  switch (nb) {
+    case 2: demap_cell_batch<2>(a, b, s, sp); break;
+    case 4: demap_cell_batch<4>(a, b, s, sp); break;
+    case 6: demap_cell_batch<6>(a, b, s, sp); break;
+    case 8: demap_cell_batch<8>(a, b, s, sp); break;
+    case 10: demap_cell_batch<10>(a, b, s, sp); break;
+    case 12: demap_cell_batch<12>(a, b, s, sp); break;
+  }
+}
+
 }  // namespace atsc3
 
 extern "C" {
+
+int32_t atsc3_demap_batch(const float *cells, const int64_t *cell_off,
+                          const int32_t *ncell, const int32_t *nbits,
+                          const float *pts, const int64_t *pts_off,
+                          const float *sigma2, const int32_t *lq,
+                          const int64_t *lq_off, float *llr,
+                          const int64_t *llr_off, const int32_t *chunk_blk,
+                          const int32_t *chunk_start, int32_t nchunks,
+                          int32_t max_nbits, void *stream) {
+  using namespace atsc3;
+  ATSC3_ARG(nchunks >= 0, "negative size");
+  if (nchunks == 0) return 0;
+  ATSC3_ARG(cells && cell_off && ncell && nbits && pts && pts_off && sigma2 &&
+                lq && lq_off && llr && llr_off && chunk_blk && chunk_start,
+            "null pointer");
+  ATSC3_ARG(max_nbits >= 2 && max_nbits <= 12, "max_nbits must be 2..12");
+  const int smem = 3 * (1 << max_nbits) * 4;
+  if (smem > 48 * 1024)
+    ATSC3_CUDA(cudaFuncSetAttribute((const void *)demap_batch_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  DemapBatchArgs a{(const float2 *)cells, cell_off, ncell, nbits, pts, pts_off,
+                   sigma2, lq, lq_off, llr, llr_off, chunk_blk, chunk_start};
+  demap_batch_kernel<<<nchunks, 256, smem, (cudaStream_t)stream>>>(a);
+  ATSC3_CUDA(cudaGetLastError());
+  return 0;
+}
+
 
 int32_t atsc3_demap(const float *cells, int64_t ld_cells, int32_t nblk,
                     int32_t ncell, const float *pts, int32_t nbits,

@@ -296,190 +296,213 @@ __device__ __forceinline__ uint64_t low_mask64(int d) {
   return d >= 64 ? ~0ull : ((1ull << d) - 1ull);
 }
 
+// Geometry and tables of one code, as the per-codeword decoder sees them.
+struct CwView {
+  int n, nc, ncp, nvlog2, nslc, nslv;
+  const uint16_t *cent;
+  const int32_t *cslice;
+  const uint32_t *vent;
+  const int32_t *vslice;
+};
+
+// Decode ONE codeword with the whole cluster (every CTA of the cluster calls
+// this with the same arguments).  sm: this CTA's shared memory for the
+// codeword (posteriors, records, partial counts).  Writes bits_row /
+// hard_row (nullable) and *conv, *its, *bad (rank 0).  Ends after a
+// __syncthreads, with no distributed-shared-memory access in flight.
 template <typename T, int RB, bool TORCH>
-__global__ void __launch_bounds__(1024, 1) ldpc_flood_kernel(const FloodArgs a) {
+__device__ __forceinline__ void flood_codeword(
+    const CwView &g, const T *lam, int iters, T alpha, unsigned char *sm,
+    int rank, int CL, uint8_t *bits_row, uint8_t *hard_row, uint8_t *conv,
+    int32_t *its, int32_t *bad) {
   using R = Rec<T, RB>;
   constexpr int NV = R::NV;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int rank = (int)cluster_ctarank();
-  const int CL = (int)cluster_nctarank();
-  const int nvp = 1 << a.nvlog2;
+  const int nvp = 1 << g.nvlog2;
   const uint32_t vmask = (uint32_t)nvp - 1u;
-  T *tot = reinterpret_cast<T *>(smem);
-  uint4 *rec = reinterpret_cast<uint4 *>(smem + (size_t)nvp * sizeof(T));
-  int *part = reinterpret_cast<int *>(smem + (size_t)nvp * sizeof(T) +
-                                      (size_t)a.ncp * RB);
+  T *tot = reinterpret_cast<T *>(sm);
+  uint4 *rec = reinterpret_cast<uint4 *>(sm + (size_t)nvp * sizeof(T));
+  int *part = reinterpret_cast<int *>(sm + (size_t)nvp * sizeof(T) +
+                                      (size_t)g.ncp * RB);
   int *sbad = part + 32;
   const uint32_t tot_sa = smem_u32(tot);
   const uint32_t rec_sa = smem_u32(rec);
   const uint32_t part_sa = smem_u32(part);
-  const T alpha = (T)a.alpha;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  const int cs0 = rank * (a.ncp >> 5);
-  const int cs1 = min(a.nslc, cs0 + (a.ncp >> 5));
+  const int cs0 = rank * (g.ncp >> 5);
+  const int cs1 = min(g.nslc, cs0 + (g.ncp >> 5));
   const int vs0 = rank * (nvp >> 5);
-  const int vs1 = min(a.nslv, vs0 + (nvp >> 5));
-  const int cbase = rank * a.ncp;
+  const int vs1 = min(g.nslv, vs0 + (nvp >> 5));
+  const int cbase = rank * g.ncp;
   const int vbase = rank * nvp;
-  const int vend = min(a.n, vbase + nvp);
+  const int vend = min(g.n, vbase + nvp);
 
+  for (int i = vbase + tid; i < vend; i += blockDim.x) tot[i - vbase] = lam[i];
+  for (int q = tid; q < g.ncp * NV; q += blockDim.x)
+    rec[q] = make_uint4(0u, 0u, 0u, 0u);
   if (tid == 0) *sbad = 0;
+  __syncthreads();
+  cluster_sync_all();
 
-  for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
-    const T *lam = reinterpret_cast<const T *>(a.llr) + (size_t)b * a.ld_llr;
-    for (int i = vbase + tid; i < vend; i += blockDim.x) tot[i - vbase] = lam[i];
-    for (int q = tid; q < a.ncp * NV; q += blockDim.x)
-      rec[q] = make_uint4(0u, 0u, 0u, 0u);
+  for (int it = 0;; ++it) {
+    // ---------------- check phase (syndrome + new records) ----------------
+    int mybad = 0;
+    for (int s = cs0 + warp; s < cs1; s += nwarps) {
+      const int c = (s << 5) + lane;
+      const int e0 = __ldg(g.cslice + s);
+      const int dm = __ldg(g.cslice + s + 1) - e0;
+      if (c < g.nc) {
+        const uint16_t *ent = g.cent + ((size_t)e0 << 5) + lane;
+        uint4 ro[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) ro[q] = rec[(c - cbase) * NV + q];
+        const T Ao = R::A(ro), Bo = R::B(ro);
+        const int Fo = R::F(ro);
+        T min1 = pos_inf<T>(), min2 = pos_inf<T>();
+        int first = 0, deg = 0;
+        uint32_t syn = 0;
+        uint64_t slo = 0, shi = 0;
+        for (int k0 = 0; k0 < dm; k0 += 8) {
+          uint32_t vi[8];
+          T t[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            vi[u] = (k0 + u < dm) ? (uint32_t)__ldg(ent + ((k0 + u) << 5))
+                                  : 0xFFFFu;
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            t[u] = vi[u] != 0xFFFFu
+                       ? dsmem_ld<T>(dsmem_map(
+                             tot_sa + (vi[u] & vmask) * (uint32_t)sizeof(T),
+                             vi[u] >> g.nvlog2))
+                       : T(0);
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (vi[u] == 0xFFFFu) continue;
+            const int j = k0 + u;
+            syn ^= (t[u] < T(0)) ? 1u : 0u;
+            T mo = (j == Fo) ? Bo : Ao;
+            if (R::sign(ro, j)) mo = -mo;
+            const T v = sub_rn(t[u], mo);
+            const uint64_t sg = (v < T(0)) ? 1ull : 0ull;
+            if (j < 64) slo |= sg << j; else shi |= sg << (j - 64);
+            const T mag = fabs(v);
+            if (mag < min1) { min2 = min1; min1 = mag; first = j; }
+            else if (mag < min2) { min2 = mag; }
+            deg = j + 1;
+          }
+        }
+        const int par = (__popcll(slo) + __popcll(shi)) & 1;
+        if (par) {
+          slo ^= low_mask64(deg);
+          shi ^= deg > 64 ? low_mask64(deg - 64) : 0ull;
+        }
+        uint4 rn[NV];
+        R::pack(rn, mul_rn(min1, alpha), mul_rn(min2, alpha), first, slo, shi);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) rec[(c - cbase) * NV + q] = rn[q];
+        mybad += (int)syn;
+      }
+    }
+    mybad = __reduce_add_sync(0xffffffffu, mybad);
+    if (lane == 0 && mybad) atomicAdd(sbad, mybad);
+    __syncthreads();
+    if (tid < CL)
+      dsmem_st_u32(dsmem_map(part_sa + (uint32_t)(((it & 1) * 16 + rank) * 4),
+                             (uint32_t)tid),
+                   (uint32_t)*sbad);
+    cluster_sync_all();
+    int badct = 0;
+    for (int r = 0; r < CL; ++r) badct += part[(it & 1) * 16 + r];
+    if (tid == 0) *sbad = 0;
+    const bool done = (badct == 0) && (!TORCH || it > 0);
+    if (done || it >= iters) {
+      // ---------------- retire: hard decisions and status ------------------
+      if (bits_row)
+        for (int i = vbase + tid; i < vend; i += blockDim.x)
+          bits_row[i] = tot[i - vbase] < T(0) ? 1 : 0;
+      if (hard_row) {
+        for (int w0 = vbase; w0 < vend; w0 += 32 * nwarps) {
+          const int i = w0 + (warp << 5) + lane;
+          const bool ng = i < vend && tot[i - vbase] < T(0);
+          const uint32_t m = __ballot_sync(0xffffffffu, ng);
+          const int base = w0 + (warp << 5);
+          if (lane == 0 && base < vend) {
+            const uint32_t word = __byte_perm(__brev(m), 0u, 0x0123u);
+            if (base + 32 <= vend) {
+              *reinterpret_cast<uint32_t *>(hard_row + (base >> 3)) = word;
+            } else {
+              const int nbyte = (vend - base + 7) >> 3;
+              for (int q = 0; q < nbyte; ++q)
+                hard_row[(base >> 3) + q] = (uint8_t)(word >> (8 * q));
+            }
+          }
+        }
+      }
+      if (rank == 0 && tid == 0) {
+        *conv = done ? 1 : 0;
+        *its = it;
+        *bad = done ? 0 : badct;
+      }
+      // outputs read posteriors the next codeword's prologue overwrites
+      __syncthreads();
+      return;
+    }
+    // ---------------- variable phase --------------------------------------
+    for (int s = vs0 + warp; s < vs1; s += nwarps) {
+      const int i = (s << 5) + lane;
+      const int e0 = __ldg(g.vslice + s);
+      const int dm = __ldg(g.vslice + s + 1) - e0;
+      if (i < g.n) {
+        const uint32_t *ent = g.vent + ((size_t)e0 << 5) + lane;
+        const T li = lam[i];
+        T acc = TORCH ? li : T(0);
+        for (int k0 = 0; k0 < dm; k0 += 4) {
+          uint32_t en[4];
+          uint4 rr[4][NV];
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            en[u] = (k0 + u < dm) ? __ldg(ent + ((k0 + u) << 5)) : 0xFFFFFFFFu;
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (en[u] == 0xFFFFFFFFu) continue;
+            const uint32_t ra = dsmem_map(
+                rec_sa + (en[u] & 0xFFFFu) * (uint32_t)RB, (en[u] >> 16) & 15u);
+            rr[u][0] = dsmem_ld_v4(ra);
+            if (NV > 1 && R::need_hi((int)(en[u] >> 20)))
+              rr[u][NV - 1] = dsmem_ld_v4(ra + 16u);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (en[u] == 0xFFFFFFFFu) continue;
+            const int j = (int)(en[u] >> 20);
+            T m = (j == R::F(rr[u])) ? R::B(rr[u]) : R::A(rr[u]);
+            if (R::sign(rr[u], j)) m = -m;
+            acc = add_rn(acc, m);
+          }
+        }
+        tot[i - vbase] = TORCH ? acc : add_rn(li, acc);
+      }
+    }
     __syncthreads();
     cluster_sync_all();
+  }
+}
 
-    for (int it = 0;; ++it) {
-      // ---------------- check phase (syndrome + new records) --------------
-      int mybad = 0;
-      for (int s = cs0 + warp; s < cs1; s += nwarps) {
-        const int c = (s << 5) + lane;
-        const int e0 = __ldg(a.cslice + s);
-        const int dm = __ldg(a.cslice + s + 1) - e0;
-        if (c < a.nc) {
-          const uint16_t *ent = a.cent + ((size_t)e0 << 5) + lane;
-          uint4 ro[NV];
-#pragma unroll
-          for (int q = 0; q < NV; ++q) ro[q] = rec[(c - cbase) * NV + q];
-          const T Ao = R::A(ro), Bo = R::B(ro);
-          const int Fo = R::F(ro);
-          T min1 = pos_inf<T>(), min2 = pos_inf<T>();
-          int first = 0, deg = 0;
-          uint32_t syn = 0;
-          uint64_t slo = 0, shi = 0;
-          for (int k0 = 0; k0 < dm; k0 += 8) {
-            uint32_t vi[8];
-            T t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-              vi[u] = (k0 + u < dm) ? (uint32_t)__ldg(ent + ((k0 + u) << 5))
-                                    : 0xFFFFu;
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-              t[u] = vi[u] != 0xFFFFu
-                         ? dsmem_ld<T>(dsmem_map(
-                               tot_sa + (vi[u] & vmask) * (uint32_t)sizeof(T),
-                               vi[u] >> a.nvlog2))
-                         : T(0);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              if (vi[u] == 0xFFFFu) continue;
-              const int j = k0 + u;
-              syn ^= (t[u] < T(0)) ? 1u : 0u;
-              T mo = (j == Fo) ? Bo : Ao;
-              if (R::sign(ro, j)) mo = -mo;
-              const T v = sub_rn(t[u], mo);
-              const uint64_t sg = (v < T(0)) ? 1ull : 0ull;
-              if (j < 64) slo |= sg << j; else shi |= sg << (j - 64);
-              const T mag = fabs(v);
-              if (mag < min1) { min2 = min1; min1 = mag; first = j; }
-              else if (mag < min2) { min2 = mag; }
-              deg = j + 1;
-            }
-          }
-          const int par = (__popcll(slo) + __popcll(shi)) & 1;
-          if (par) {
-            slo ^= low_mask64(deg);
-            shi ^= deg > 64 ? low_mask64(deg - 64) : 0ull;
-          }
-          uint4 rn[NV];
-          R::pack(rn, mul_rn(min1, alpha), mul_rn(min2, alpha), first, slo, shi);
-#pragma unroll
-          for (int q = 0; q < NV; ++q) rec[(c - cbase) * NV + q] = rn[q];
-          mybad += (int)syn;
-        }
-      }
-      mybad = __reduce_add_sync(0xffffffffu, mybad);
-      if (lane == 0 && mybad) atomicAdd(sbad, mybad);
-      __syncthreads();
-      if (tid < CL)
-        dsmem_st_u32(dsmem_map(part_sa + (uint32_t)(((it & 1) * 16 + rank) * 4),
-                               (uint32_t)tid),
-                     (uint32_t)*sbad);
-      cluster_sync_all();
-      int badct = 0;
-      for (int r = 0; r < CL; ++r) badct += part[(it & 1) * 16 + r];
-      if (tid == 0) *sbad = 0;
-      const bool done = (badct == 0) && (!TORCH || it > 0);
-      if (done || it >= a.iters) {
-        // ---------------- retire: hard decisions and status ----------------
-        if (a.bits) {
-          uint8_t *bo = a.bits + (size_t)b * a.ld_bits;
-          for (int i = vbase + tid; i < vend; i += blockDim.x)
-            bo[i] = tot[i - vbase] < T(0) ? 1 : 0;
-        }
-        if (a.hard) {
-          uint8_t *ho = a.hard + (size_t)b * a.ld_hard;
-          for (int w0 = vbase; w0 < vend; w0 += 32 * nwarps) {
-            const int i = w0 + (warp << 5) + lane;
-            const bool ng = i < vend && tot[i - vbase] < T(0);
-            const uint32_t m = __ballot_sync(0xffffffffu, ng);
-            const int base = w0 + (warp << 5);
-            if (lane == 0 && base < vend) {
-              const uint32_t word = __byte_perm(__brev(m), 0u, 0x0123u);
-              if (base + 32 <= vend) {
-                *reinterpret_cast<uint32_t *>(ho + (base >> 3)) = word;
-              } else {
-                const int nbyte = (vend - base + 7) >> 3;
-                for (int q = 0; q < nbyte; ++q)
-                  ho[(base >> 3) + q] = (uint8_t)(word >> (8 * q));
-              }
-            }
-          }
-        }
-        if (rank == 0 && tid == 0) {
-          a.conv[b] = done ? 1 : 0;
-          a.its[b] = it;
-          a.bad[b] = done ? 0 : badct;
-        }
-        // outputs read posteriors the next codeword's prologue overwrites
-        __syncthreads();
-        break;
-      }
-      // ---------------- variable phase ------------------------------------
-      for (int s = vs0 + warp; s < vs1; s += nwarps) {
-        const int i = (s << 5) + lane;
-        const int e0 = __ldg(a.vslice + s);
-        const int dm = __ldg(a.vslice + s + 1) - e0;
-        if (i < a.n) {
-          const uint32_t *ent = a.vent + ((size_t)e0 << 5) + lane;
-          const T li = lam[i];
-          T acc = TORCH ? li : T(0);
-          for (int k0 = 0; k0 < dm; k0 += 4) {
-            uint32_t en[4];
-            uint4 rr[4][NV];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-              en[u] = (k0 + u < dm) ? __ldg(ent + ((k0 + u) << 5)) : 0xFFFFFFFFu;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              if (en[u] == 0xFFFFFFFFu) continue;
-              const uint32_t ra = dsmem_map(
-                  rec_sa + (en[u] & 0xFFFFu) * (uint32_t)RB, (en[u] >> 16) & 15u);
-              rr[u][0] = dsmem_ld_v4(ra);
-              if (NV > 1 && R::need_hi((int)(en[u] >> 20)))
-                rr[u][NV - 1] = dsmem_ld_v4(ra + 16u);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              if (en[u] == 0xFFFFFFFFu) continue;
-              const int j = (int)(en[u] >> 20);
-              T m = (j == R::F(rr[u])) ? R::B(rr[u]) : R::A(rr[u]);
-              if (R::sign(rr[u], j)) m = -m;
-              acc = add_rn(acc, m);
-            }
-          }
-          tot[i - vbase] = TORCH ? acc : add_rn(li, acc);
-        }
-      }
-      __syncthreads();
-      cluster_sync_all();
-    }
+template <typename T, int RB, bool TORCH>
+__global__ void __launch_bounds__(1024, 1) ldpc_flood_kernel(const FloodArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int rank = (int)cluster_ctarank();
+  const int CL = (int)cluster_nctarank();
+  const CwView g{a.n, a.nc, a.ncp, a.nvlog2, a.nslc, a.nslv,
+                 a.cent, a.cslice, a.vent, a.vslice};
+  for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
+    const T *lam = reinterpret_cast<const T *>(a.llr) + (size_t)b * a.ld_llr;
+    flood_codeword<T, RB, TORCH>(
+        g, lam, a.iters, (T)a.alpha, smem, rank, CL,
+        a.bits ? a.bits + (size_t)b * a.ld_bits : nullptr,
+        a.hard ? a.hard + (size_t)b * a.ld_hard : nullptr, a.conv + b,
+        a.its + b, a.bad + b);
   }
   // no CTA may leave while a peer can still read its shared memory
   __syncthreads();
@@ -959,3 +982,165 @@ int32_t atsc3_ldpc_tables_host(const int32_t *cptr, const int32_t *cidx,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// uneven batches: one persistent launch over codewords of different codes
+// ===========================================================================
+
+namespace atsc3 {
+
+struct BatchPlanDev {
+  CwView g;
+  int rb;
+  int pad[3];
+};
+
+struct BatchArgs {
+  const BatchPlanDev *plans;
+  const int32_t *bplan;      // plan index of each block
+  const int32_t *order;      // queue position -> block (most work first)
+  const float *llr;
+  const int64_t *llr_off;    // floats
+  uint8_t *hard;
+  const int64_t *hard_off;   // bytes, 4-byte aligned
+  uint8_t *conv;
+  int32_t *its;
+  int32_t *bad;
+  int32_t *counter;          // zeroed before the launch
+  int nblk, iters;
+  float alpha;
+};
+
+// Clusters pull blocks from a device queue: rank 0 takes the next position
+// and writes the block index into every CTA's slot (shared word 0); the
+// codeword's state starts at shared byte 16.
+__global__ void __launch_bounds__(1024, 1) ldpc_batch_kernel(const BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int *slot = reinterpret_cast<int *>(smem);
+  const uint32_t slot_sa = smem_u32(slot);
+  const int rank = (int)cluster_ctarank();
+  const int CL = (int)cluster_nctarank();
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) {
+      const int q = atomicAdd(a.counter, 1);
+      const int b = q < a.nblk ? __ldg(a.order + q) : -1;
+      for (int r = 0; r < CL; ++r) dsmem_st_u32(dsmem_map(slot_sa, (uint32_t)r), (uint32_t)b);
+    }
+    cluster_sync_all();
+    const int b = *slot;
+    cluster_sync_all();            // everyone has read the slot
+    if (b < 0) break;
+    const BatchPlanDev P = a.plans[__ldg(a.bplan + b)];
+    const float *lam = a.llr + __ldg(a.llr_off + b);
+    uint8_t *hr = a.hard ? a.hard + __ldg(a.hard_off + b) : nullptr;
+    if (P.rb == 16)
+      flood_codeword<float, 16, false>(P.g, lam, a.iters, a.alpha, smem + 16,
+                                       rank, CL, nullptr, hr, a.conv + b,
+                                       a.its + b, a.bad + b);
+    else
+      flood_codeword<float, 32, false>(P.g, lam, a.iters, a.alpha, smem + 16,
+                                       rank, CL, nullptr, hr, a.conv + b,
+                                       a.its + b, a.bad + b);
+  }
+  __syncthreads();
+  cluster_sync_all();
+}
+
+}  // namespace atsc3
+
+extern "C" {
+
+int32_t atsc3_ldpc_batch_prepare(const atsc3_ldpc_plan *const *plans,
+                                 int32_t nplans, void *desc,
+                                 int32_t *cluster_out, int32_t *smem_out) {
+  using namespace atsc3;
+  ATSC3_ARG(plans && nplans > 0 && desc && cluster_out && smem_out, "bad argument");
+  std::vector<BatchPlanDev> h(nplans);
+  int cl = plans[0]->cluster, smem = 0;
+  for (int i = 0; i < nplans; ++i) {
+    const atsc3_ldpc_plan *p = plans[i];
+    ATSC3_ARG(p && p->dtype == 0, "batch plans must be float32 CSR plans");
+    ATSC3_ARG(p->cluster == cl, "batch plans must share one cluster size");
+    ATSC3_ARG(p->rec_bytes == 16 || p->rec_bytes == 32, "record size");
+    h[i].g = CwView{p->n, p->nc, p->ncp, p->nvlog2, p->nslc, p->nslv,
+                    p->d_cent, p->d_cslice, p->d_vent, p->d_vslice};
+    h[i].rb = p->rec_bytes;
+    smem = std::max(smem, p->smem_bytes);
+  }
+  ATSC3_CUDA(cudaMemcpy(desc, h.data(), h.size() * sizeof(BatchPlanDev),
+                        cudaMemcpyHostToDevice));
+  *cluster_out = cl;
+  *smem_out = smem + 16;
+  return 0;
+}
+
+int32_t atsc3_ldpc_batch_desc_bytes(int32_t nplans, int64_t *bytes) {
+  ATSC3_ARG(nplans > 0 && bytes, "bad argument");
+  *bytes = (int64_t)nplans * (int64_t)sizeof(atsc3::BatchPlanDev);
+  return 0;
+}
+
+int32_t atsc3_ldpc_batch_decode(const void *desc, int32_t cluster, int32_t smem,
+                                const int32_t *bplan, const int32_t *order,
+                                int32_t nblk, const float *llr,
+                                const int64_t *llr_off, uint8_t *hard,
+                                const int64_t *hard_off, uint8_t *conv,
+                                int32_t *its, int32_t *bad, int32_t iters,
+                                float alpha, int32_t *counter, int32_t threads,
+                                int32_t cap_clusters, void *stream) {
+  using namespace atsc3;
+  ATSC3_ARG(desc && bplan && order && llr && llr_off && conv && its && bad &&
+                counter,
+            "null pointer");
+  ATSC3_ARG(cluster >= 1 && cluster <= 16, "cluster");
+  ATSC3_ARG(iters >= 0 && nblk >= 0, "negative size");
+  if (nblk == 0) return 0;
+  if (threads <= 0) threads = 1024;
+  ATSC3_ARG(threads % 32 == 0 && threads >= 64 && threads <= 1024, "threads");
+  int dev = 0;
+  ATSC3_CUDA(cudaGetDevice(&dev));
+  FloodFn fn = reinterpret_cast<FloodFn>(ldpc_batch_kernel);
+  int32_t rc = prepare_fn(fn, dev);
+  if (rc) return rc;
+  int ncl = 0;
+  rc = max_clusters(fn, cluster, smem, threads, dev, &ncl);
+  if (rc) return rc;
+  if (ncl <= 0) {
+    set_error("unsupported: batch cluster configuration cannot be resident");
+    return -4;
+  }
+  if (cap_clusters > 0) ncl = std::min(ncl, cap_clusters);
+  ncl = std::min(ncl, nblk);
+  BatchArgs a;
+  a.plans = reinterpret_cast<const BatchPlanDev *>(desc);
+  a.bplan = bplan;
+  a.order = order;
+  a.llr = llr;
+  a.llr_off = llr_off;
+  a.hard = hard;
+  a.hard_off = hard_off;
+  a.conv = conv;
+  a.its = its;
+  a.bad = bad;
+  a.counter = counter;
+  a.nblk = nblk;
+  a.iters = iters;
+  a.alpha = alpha;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ncl * cluster, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = (cudaStream_t)stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ATSC3_CUDA(cudaLaunchKernelEx(&cfg, ldpc_batch_kernel, a));
+  return 0;
+}
+
+}  // extern "C"
+

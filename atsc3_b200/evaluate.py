@@ -71,7 +71,9 @@ def decode_count(plan, lam, cw, kldpc, n, weights=None, iters=50, alpha=0.75):
 
 
 def threshold(rate, mod, n=64800, target=1e-2, nblk=2000, seed=11, lo=-2.0,
-              hi=24.0):
+              hi=24.0, step=0.1):
+    """Lowest Es/N0 on a `step` grid in (lo, hi] where the plain decoder's
+    block error rate over `nblk` seeded blocks is <= target (bisection)."""
     torch = _torch()
     tx = synth.Transmitter(n, mod, rate, device="cuda")
     plan = LDPC.plan_for(rate, n)
@@ -86,16 +88,15 @@ def threshold(rate, mod, n=64800, target=1e-2, nblk=2000, seed=11, lo=-2.0,
             errs += decode_count(plan, lam, cw, K, n)[0]
         return errs / nblk
 
-    # coarse-to-fine bisection on a 0.1 dB grid
-    while hi - lo > 0.1 + 1e-9:
-        mid = round((lo + hi) / 2 / 0.1) * 0.1
+    while hi - lo > step + 1e-9:
+        mid = round((lo + hi) / 2 / step) * step
         if mid <= lo or mid >= hi:
             break
         if fer(mid) <= target:
             hi = mid
         else:
             lo = mid
-    return round(hi, 1)
+    return round(hi, 2)
 
 
 def sweep(rate, mod, weights, esn0s, nblk, n=64800, seed=99, chunk=2000):

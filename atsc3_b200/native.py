@@ -69,6 +69,14 @@ SIGNATURES = {
                                               c_i32, c_vp, c_vp, c_i64, c_vp,
                                               c_i64, c_vp, c_vp, c_vp, c_i32,
                                               c_vp]),
+    "atsc3_demap_batch": (c_i32, [c_vp] * 13 + [c_i32, c_i32, c_vp]),
+    "atsc3_ldpc_batch_desc_bytes": (c_i32, [c_i32, c_vp]),
+    "atsc3_ldpc_batch_prepare": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp]),
+    "atsc3_ldpc_batch_decode": (c_i32, [c_vp, c_i32, c_i32, c_vp, c_vp, c_i32,
+                                        c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                        c_vp, c_i32, c_f32, c_vp, c_i32,
+                                        c_i32, c_vp]),
+    "atsc3_bch_batch": (c_i32, [c_vp] * 11 + [c_i32, c_vp]),
     "atsc3_demap": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32, c_i32,
                             c_vp, c_i64, c_f32, c_vp, c_vp, c_i64, c_vp]),
     "atsc3_demap_row_sigma2": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,

@@ -278,6 +278,50 @@ int32_t atsc3_bch_syndrome_bits(const uint8_t *bits, int64_t ld_bits,
                                 const uint32_t *rtab, uint32_t *syn,
                                 void *stream);
 
+/* ---- uneven batches (one launch per stage over mixed codes) ---------------
+ * Blocks of different code lengths, rates and constellations decoded
+ * together; every per-block array is on the device.  Replaces the per-MODCOD
+ * loops of lab/m9_fast.py:1117-1154 / lab/m44_ldm.py:2348-2390 when one
+ * frame carries several PLPs.
+ * atsc3_demap_batch: block b's cells at cells + 2*cell_off[b] floats, its
+ *   alphabet (3*2^nbits[b] floats) at pts + pts_off[b], its de-interleaver
+ *   at lq + lq_off[b], LLRs to llr + llr_off[b]; one sigma2 per block;
+ *   chunk_blk/chunk_start: one entry per 256-cell chunk (the grid).
+ * atsc3_ldpc_batch_prepare: device descriptors of float32 CSR plans built
+ *   with one common cluster size (desc: atsc3_ldpc_batch_desc_bytes bytes);
+ *   returns that cluster size and the shared bytes per CTA.
+ * atsc3_ldpc_batch_decode: one persistent cluster launch; clusters take
+ *   blocks from a device queue (counter zeroed before the launch, `order`
+ *   lists blocks most-work-first); kernel semantics of ldpc_minsum_f32.
+ * atsc3_bch_batch: per-block BCH length and remainder table (rtab +
+ *   rtab_off[b] words), descrambled payload to payload + pay_off[b]. */
+int32_t atsc3_demap_batch(const float *cells, const int64_t *cell_off,
+                          const int32_t *ncell, const int32_t *nbits,
+                          const float *pts, const int64_t *pts_off,
+                          const float *sigma2, const int32_t *lq,
+                          const int64_t *lq_off, float *llr,
+                          const int64_t *llr_off, const int32_t *chunk_blk,
+                          const int32_t *chunk_start, int32_t nchunks,
+                          int32_t max_nbits, void *stream);
+int32_t atsc3_ldpc_batch_desc_bytes(int32_t nplans, int64_t *bytes);
+int32_t atsc3_ldpc_batch_prepare(const atsc3_ldpc_plan *const *plans,
+                                 int32_t nplans, void *desc,
+                                 int32_t *cluster_out, int32_t *smem_out);
+int32_t atsc3_ldpc_batch_decode(const void *desc, int32_t cluster, int32_t smem,
+                                const int32_t *bplan, const int32_t *order,
+                                int32_t nblk, const float *llr,
+                                const int64_t *llr_off, uint8_t *hard,
+                                const int64_t *hard_off, uint8_t *conv,
+                                int32_t *its, int32_t *bad, int32_t iters,
+                                float alpha, int32_t *counter, int32_t threads,
+                                int32_t max_clusters, void *stream);
+int32_t atsc3_bch_batch(const uint8_t *hard, const int64_t *hard_off,
+                        const int32_t *kldpc, const uint32_t *rtab,
+                        const int64_t *rtab_off, const uint8_t *scr,
+                        const int32_t *kpay, uint8_t *payload,
+                        const int64_t *pay_off, uint32_t *syn, uint8_t *ok,
+                        int32_t nblk, void *stream);
+
 /* ---- decode without device allocation -------------------------------------
  * No counterpart in the reference (its decoders allocate through numpy and
  * torch).  For callers that must not allocate device memory on their decode
