@@ -12,7 +12,10 @@ with 256-NUC):
 2. training: per-iteration, per-check-degree scale/offset of the unrolled
    12-iteration weighted min-sum (``learned.train``) on fresh seeded blocks
    at Es/N0 uniform in [thr-0.5, thr+1.5], half AWGN, half Rayleigh gain;
-3. evaluation on held-out seeded blocks over an Es/N0 sweep: block errors
+3. the same threshold search for the learned decoder (the gain in dB at a
+   block error rate of 1e-2 is the difference);
+4. evaluation on held-out seeded blocks over an Es/N0 sweep from 0.5 dB below
+   the plain threshold in 0.25 dB steps: block errors
    (BCH syndrome nonzero or information bits wrong), mean iterations and
    decoded Mbit/s for the plain and the learned decoder, both the same
    flooding schedule with early stop (iterations past 12 reuse the last
@@ -71,9 +74,10 @@ def decode_count(plan, lam, cw, kldpc, n, weights=None, iters=50, alpha=0.75):
 
 
 def threshold(rate, mod, n=64800, target=1e-2, nblk=2000, seed=11, lo=-2.0,
-              hi=24.0, step=0.1):
-    """Lowest Es/N0 on a `step` grid in (lo, hi] where the plain decoder's
-    block error rate over `nblk` seeded blocks is <= target (bisection)."""
+              hi=24.0, step=0.1, weights=None):
+    """Lowest Es/N0 on a `step` grid in (lo, hi] where the decoder's block
+    error rate over `nblk` seeded blocks is <= target (bisection); the plain
+    decoder, or the weighted one when `weights` is given."""
     torch = _torch()
     tx = synth.Transmitter(n, mod, rate, device="cuda")
     plan = LDPC.plan_for(rate, n)
@@ -85,7 +89,7 @@ def threshold(rate, mod, n=64800, target=1e-2, nblk=2000, seed=11, lo=-2.0,
         errs = 0
         for lo_ in range(0, nblk, 500):
             lam, cw = blocks(tx, gen, min(500, nblk - lo_), e)
-            errs += decode_count(plan, lam, cw, K, n)[0]
+            errs += decode_count(plan, lam, cw, K, n, weights=weights)[0]
         return errs / nblk
 
     while hi - lo > step + 1e-9:
@@ -126,7 +130,7 @@ def sweep(rate, mod, weights, esn0s, nblk, n=64800, seed=99, chunk=2000):
     return out
 
 
-def run(steps=2000, batch=256, nblk=100000, points=6, out_dir=None, seed=1):
+def run(steps=2000, batch=256, nblk=100000, points=9, out_dir=None, seed=1):
     report = {}
     out_dir = out_dir or os.path.join(HERE, "data")
     for rate, mod in MODCODS:
@@ -141,12 +145,32 @@ def run(steps=2000, batch=256, nblk=100000, points=6, out_dir=None, seed=1):
         LR.save_weights(path, al, be, man)
         code = LR.WmsCode(rate, 64800)
         w = LR.inference_weights(al, be, code.buckets)
-        esn0s = [round(thr + 0.2 * i, 1) for i in range(points)]
+        lthr = threshold(rate, mod, lo=thr - 3.0, hi=thr, weights=w)
+        esn0s = [round(thr - 0.5 + 0.25 * i, 2) for i in range(points)]
         rows = sweep(rate, mod, w, esn0s, nblk // points)
-        report[f"{rate} {mod}"] = {"threshold_db": thr, "train_loss": hist,
-                                   "weights": path, "sweep": rows,
+        report[f"{rate} {mod}"] = {"threshold_db": thr,
+                                   "learned_threshold_db": lthr,
+                                   "gain_db_at_fer_1e-2": round(thr - lthr, 2),
+                                   "train_loss": hist,
+                                   "weights": os.path.basename(path),
+                                   "sweep": rows, "operating_point": summary(rows),
                                    "seconds": time.time() - t0}
     return report
+
+
+def summary(rows, target=1e-4):
+    """The plain decoder's operating point: the lowest Es/N0 of the sweep
+    where its block error rate is <= target; the learned decoder's block
+    error rate and mean iterations there."""
+    for r in rows:
+        if r["plain"]["fer"] <= target:
+            p, l = r["plain"], r["learned"]
+            return {"esn0_db": r["esn0_db"], "plain_fer": p["fer"],
+                    "learned_fer": l["fer"], "plain_mean_iters": p["mean_iters"],
+                    "learned_mean_iters": l["mean_iters"],
+                    "iteration_reduction": 1 - l["mean_iters"] / p["mean_iters"],
+                    "plain_mbit_s": p["mbit_s"], "learned_mbit_s": l["mbit_s"]}
+    return None
 
 
 def main(argv=None):
@@ -154,7 +178,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--blocks", type=int, default=100000)
-    ap.add_argument("--points", type=int, default=6)
+    ap.add_argument("--points", type=int, default=9)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     print(json.dumps(run(a.steps, a.batch, a.blocks, a.points, a.out)), flush=True)

@@ -60,12 +60,16 @@ class FecPipeline:
             self._ws[nblk] = ws
         return ws
 
-    def decode(self, cells, sigma2=None, iters=None, alpha=None, out=None):
+    def decode(self, cells, sigma2=None, iters=None, alpha=None, out=None,
+               weights=None):
         """cells: (nblk, ncell) complex64 CUDA tensor; sigma2: float, (nblk,)
         or (nblk, ncell) tensor, or None (per-row estimate).  Returns a dict
         of device tensors: the workspace (reused by the next call of the same
         batch size) overridden by any caller-owned buffers in `out` (keys
-        conv, its, bad, syn, ok, payload)."""
+        conv, its, bad, syn, ok, payload).  `weights`: learned per-iteration,
+        per-check-degree scale/offset tables (``learned.inference_weights``)
+        in place of the single `alpha`.  All launches go to the current
+        stream."""
         nblk = cells.shape[0]
         ws = dict(self._buffers(nblk))
         if out:
@@ -75,7 +79,8 @@ class FecPipeline:
         LDPC.decode_flood(self.plan, ws["lam"], iters=iters or self.iters,
                           alpha=self.alpha if alpha is None else alpha,
                           semantics=self.semantics, want_bits=False,
-                          want_hard=True, threads=self.threads, out=ws)
+                          want_hard=True, threads=self.threads, out=ws,
+                          weights=weights)
         BCH.bch_check(ws["hard"], self.kldpc, self.n, self.kpayload,
                       want_payload=True, out=ws)
         return ws

@@ -217,88 +217,160 @@ def config(blocks):
                   "0.93 GB over 64 steps"}
 
 
+def decode_frame(pipe, cells, sig, out, stream, weights=None):
+    """One frame on one stream: demap -> LDPC -> BCH into `out` (3 launches)."""
+    from atsc3_b200 import bch as BCH
+    from atsc3_b200 import demap as DM
+    from atsc3_b200 import ldpc as LDPC
+    nblk = cells.shape[0]
+    ws = pipe._buffers(nblk)
+    st = stream.cuda_stream
+    DM.demap(cells, MOD, RATE, sigma2=sig, n=N_INNER, out=ws["lam"], stream=st)
+    o = dict(ws)
+    o.update(out)
+    LDPC.decode_flood(pipe.plan, ws["lam"], iters=ITERS, alpha=ALPHA,
+                      want_bits=False, want_hard=True, threads=pipe.threads,
+                      out=o, stream=st, weights=weights)
+    BCH.bch_check(ws["hard"], pipe.kldpc, N_INNER, pipe.kpayload, out=o,
+                  stream=st)
+
+
+def learned_weights(dev):
+    """Committed learned weights for this code, if any: (weights, manifest)."""
+    path = os.path.join(HERE, "atsc3_b200", "data",
+                        f"weights_{RATE.replace('/', '_')}_{MOD}.pt")
+    if not os.path.exists(path):
+        return None, None
+    from atsc3_b200 import learned as LR
+    al, be, man = LR.load_weights(path, dev)
+    code = LR.WmsCode(RATE, N_INNER, dev)
+    return LR.inference_weights(al, be, code.buckets, dev), man
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
-    from atsc3_b200 import codes as C
+    from atsc3_b200 import shard
     from atsc3_b200.pipeline import FecPipeline
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     K, W = args.steps, args.warmup
     nframes = K + W
     cells, sig, nblk, kp = make_frames(nframes, args.seed + 1000 * rank, dev)
-    pipe = FecPipeline(N_INNER, MOD, RATE, iters=ITERS, alpha=ALPHA,
-                       cluster=args.cluster, threads=args.threads, device=dev)
-    outs = []
-    for f in range(nframes):
-        outs.append({"conv": torch.empty(nblk, dtype=torch.uint8, device=dev),
-                     "its": torch.empty(nblk, dtype=torch.int32, device=dev),
-                     "bad": torch.empty(nblk, dtype=torch.int32, device=dev),
-                     "ok": torch.empty(nblk, dtype=torch.uint8, device=dev),
-                     "syn": torch.empty((nblk, 6), dtype=torch.int32, device=dev),
-                     "payload": torch.empty((nblk, kp // 8), dtype=torch.uint8,
-                                            device=dev)})
+    S = max(1, args.streams)
+    # one pipeline (workspace) per stream; they share the decoder plan
+    pipes = [FecPipeline(N_INNER, MOD, RATE, iters=ITERS, alpha=ALPHA,
+                         cluster=args.cluster, threads=args.threads, device=dev)
+             for _ in range(S)]
+    streams = [torch.cuda.Stream(dev) for _ in range(S)]
+
+    def new_out():
+        return {"conv": torch.empty(nblk, dtype=torch.uint8, device=dev),
+                "its": torch.empty(nblk, dtype=torch.int32, device=dev),
+                "bad": torch.empty(nblk, dtype=torch.int32, device=dev),
+                "ok": torch.empty(nblk, dtype=torch.uint8, device=dev),
+                "syn": torch.empty((nblk, 6), dtype=torch.int32, device=dev),
+                "payload": torch.empty((nblk, kp // 8), dtype=torch.uint8,
+                                       device=dev)}
+    outs = [new_out() for _ in range(nframes)]
+    main = torch.cuda.current_stream(dev)
     for f in range(W):
-        pipe.decode(cells[f], sig[f], out=outs[f])
+        decode_frame(pipes[f % S], cells[f], sig[f], outs[f], streams[f % S])
     torch.cuda.synchronize()
-    st = torch.cuda.current_stream(dev)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
-          for _ in range(K)]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    ends = [torch.cuda.Event() for _ in range(S)]
     clk = Clocks(local_rank) if rank == 0 else None
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     if clk:
         clk.start()
-    e0.record(st)
+    e0.record(main)
+    for st in streams:
+        st.wait_event(e0)
     for s in range(K):
         f = W + s
-        E = ev[s]
-        E[0].record(st)
-        ws = pipe._buffers(nblk)
-        from atsc3_b200 import demap as DM, ldpc as LDPC, bch as BCH
-        DM.demap(cells[f], MOD, RATE, sigma2=sig[f], n=N_INNER, out=ws["lam"])
-        E[1].record(st)
-        o = dict(ws)
-        o.update(outs[f])
-        LDPC.decode_flood(pipe.plan, ws["lam"], iters=ITERS, alpha=ALPHA,
-                          want_bits=False, want_hard=True,
-                          threads=args.threads, out=o)
-        E[2].record(st)
-        BCH.bch_check(ws["hard"], pipe.kldpc, N_INNER, kp, out=o)
-        E[3].record(st)
-    e1.record(st)
+        decode_frame(pipes[f % S], cells[f], sig[f], outs[f], streams[f % S])
+    for st, ev in zip(streams, ends):
+        ev.record(st)
+        main.wait_event(ev)
+    e1.record(main)
     torch.cuda.synchronize()
     clocks = clk.stop() if clk else None
     ms = e0.elapsed_time(e1)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = shard.max_over_ranks(ms, device=dev)
         dist.barrier()
-    stage = np.array([[E[0].elapsed_time(E[1]), E[1].elapsed_time(E[2]),
-                       E[2].elapsed_time(E[3])] for E in ev])
-    # results of the timed frames
     conv = torch.stack([outs[W + s]["conv"] for s in range(K)]).cpu().numpy()
     its = torch.stack([outs[W + s]["its"] for s in range(K)]).cpu().numpy()
     ok = torch.stack([outs[W + s]["ok"] for s in range(K)]).cpu().numpy()
     total_bits = world * K * nblk * kp
     value = total_bits / (ms / 1e3) / 1e6
+    # ---- per-stage device time, one stream, no overlap (roofline) ---------
+    nprof = min(K, 9)
+    E = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+         for _ in range(nprof)]
+    from atsc3_b200 import bch as BCH, demap as DM, ldpc as LDPC
+    p0 = pipes[0]
+    ws = p0._buffers(nblk)
+    for s in range(nprof):
+        f = W + s
+        E[s][0].record(main)
+        DM.demap(cells[f], MOD, RATE, sigma2=sig[f], n=N_INNER, out=ws["lam"])
+        E[s][1].record(main)
+        o = dict(ws)
+        LDPC.decode_flood(p0.plan, ws["lam"], iters=ITERS, alpha=ALPHA,
+                          want_bits=False, want_hard=True, threads=p0.threads,
+                          out=o)
+        E[s][2].record(main)
+        BCH.bch_check(ws["hard"], p0.kldpc, N_INNER, kp, out=o)
+        E[s][3].record(main)
+    torch.cuda.synchronize()
+    stage = np.array([[E[s][0].elapsed_time(E[s][1]), E[s][1].elapsed_time(E[s][2]),
+                       E[s][2].elapsed_time(E[s][3])] for s in range(nprof)])
     # ---- e2e: host buffers through the public API -------------------------
-    e2e = run_e2e(pipe, cells, sig, W, K, nblk, kp, dev, world)
-    # ---- roofline of the dominant kernel (the LDPC decoder) --------------
+    e2e = run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world)
+    # ---- learned weights on the same frames (same decoder, early stop) -----
+    learned = None
+    w, man = learned_weights(dev)
+    if w is not None:
+        louts = [new_out() for _ in range(K)]
+        torch.cuda.synchronize()
+        e0.record(main)
+        for st in streams:
+            st.wait_event(e0)
+        for s in range(K):
+            f = W + s
+            decode_frame(pipes[f % S], cells[f], sig[f], louts[s], streams[f % S],
+                         weights=w)
+        for st, ev in zip(streams, ends):
+            ev.record(st)
+            main.wait_event(ev)
+        e1.record(main)
+        torch.cuda.synchronize()
+        lms = e0.elapsed_time(e1)
+        lits = torch.stack([o["its"] for o in louts]).cpu().numpy()
+        lok = torch.stack([o["ok"] for o in louts]).cpu().numpy()
+        learned = {"value": world * K * nblk * kp / (lms / 1e3) / 1e6,
+                   "unit": "Mbit/s", "mean_iters": float(lits.mean()),
+                   "bch_fer": float((lok == 0).mean()),
+                   "weights": {k: man[k] for k in ("rate", "mod", "iters",
+                                                   "step", "seed")}}
+    # ---- roofline of the dominant kernel (the LDPC decoder) ---------------
     ldpc_ms = float(stage[:, 1].mean())
     b_ldpc = nblk * (4 * N_INNER + N_INNER // 8 + 9)
     hbm, peak_kind = peaks()
     achieved = b_ldpc / (ldpc_ms / 1e3) / 1e9
-    fer = {}
+    fer = {f"{e:.1f}": [0, 0] for e in ESN0}
     for s in range(K):
-        e = ESN0[(W + s) % len(ESN0)]
-        d = fer.setdefault(f"{e:.1f}", [0, 0])
+        d = fer[f"{ESN0[(W + s) % len(ESN0)]:.1f}"]
         d[0] += int((ok[s] == 0).sum())
         d[1] += nblk
+    if world > 1:   # block errors of every rank's frames
+        keys = sorted(fer)
+        tot = shard.sum_over_ranks([v for k in keys for v in fer[k]], device=dev)
+        fer = {k: [tot[2 * i], tot[2 * i + 1]] for i, k in enumerate(keys)}
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mbit/s",
@@ -308,62 +380,89 @@ def run_gpu(args, rank, world, local_rank):
                 "config": config(nblk),
                 "roofline": {"bound": "hbm", "achieved": achieved,
                              "peak": hbm, "unit": "GB/s",
-                             "frac": achieved / hbm, "traffic": None,
-                             "kernel": "ldpc_flood_kernel<float,16,false>",
+                             "frac": achieved / hbm,
+                             "traffic": (TRAFFIC_PER_BLOCK * nblk
+                                         if TRAFFIC_PER_BLOCK else None),
+                             "kernel": "ldpc_qc_kernel (quasi-cyclic flooding)",
                              "peak_kind": peak_kind,
                              "bytes_per_launch": b_ldpc,
                              "ms_per_launch": ldpc_ms},
                 "stage_ms": {"demap": float(stage[:, 0].mean()),
                              "ldpc": ldpc_ms,
                              "bch": float(stage[:, 2].mean())},
+                "streams": S,
                 "gpu_launches": 3 * K,
                 "clocks": clocks, "e2e": e2e,
                 "mean_iters": float(its.mean()),
                 "converged_frac": float(conv.mean()),
-                "fer_bch_by_esn0": {k: v[0] / v[1] for k, v in sorted(fer.items())},
-                "plan": pipe.plan.info}
+                "fer_bch_by_esn0": {k: v[0] / v[1] for k, v in sorted(fer.items())
+                                    if v[1]},
+                "learned": learned,
+                "plan": p0.plan.info}
     return line
 
 
-def run_e2e(pipe, cells, sig, W, K, nblk, kp, dev, world):
-    """Same metric through FecPipeline with pinned host buffers: H2D of the
-    step's cells + sigma2, decode, D2H of payload bytes and flags."""
+# DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch,
+# from the ncu capture summarised in profiles/ldpc_qc_flood_6_15_frame.md.
+TRAFFIC_PER_BLOCK = None
+
+
+def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
+    """Same metric through FecPipeline.decode with pinned host buffers: per
+    step the H2D copy of its cells + sigma2, the decode, and the D2H copy of
+    the payload bytes and per-block flags, all on the step's stream (steps
+    alternate over the pipelines' streams, so one step's copies overlap the
+    other's decode)."""
     import torch
+    S = len(pipes)
     nh = min(8, K)
     hc = [cells[W + s].cpu().pin_memory() for s in range(nh)]
     hs = [sig[W + s].cpu().pin_memory() for s in range(nh)]
     hp = torch.empty((K, nblk, kp // 8), dtype=torch.uint8).pin_memory()
     hf = torch.empty((K, 4, nblk), dtype=torch.int32).pin_memory()
-    dc = torch.empty_like(cells[0])
-    ds = torch.empty_like(sig[0])
-    st = torch.cuda.current_stream(dev)
+    dc = [torch.empty_like(cells[0]) for _ in range(S)]
+    ds = [torch.empty_like(sig[0]) for _ in range(S)]
+    flags = [torch.empty((4, nblk), dtype=torch.int32, device=dev)
+             for _ in range(S)]
+    main = torch.cuda.current_stream(dev)
+
+    def step(s):
+        i = s % S
+        with torch.cuda.stream(streams[i]):
+            dc[i].copy_(hc[s % nh], non_blocking=True)
+            ds[i].copy_(hs[s % nh], non_blocking=True)
+            ws = pipes[i].decode(dc[i], ds[i])
+            f = flags[i]
+            f[0].copy_(ws["conv"])
+            f[1].copy_(ws["its"])
+            f[2].copy_(ws["bad"])
+            f[3].copy_(ws["ok"])
+            hp[s].copy_(ws["payload"], non_blocking=True)
+            hf[s].copy_(f, non_blocking=True)
+
+    for s in range(2 * S):   # warm the pinned path
+        step(s % K)
+    torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    flags = torch.empty((4, nblk), dtype=torch.int32, device=dev)
-    for s in range(2):   # warm the pinned path
-        dc.copy_(hc[s % nh], non_blocking=True)
-        ds.copy_(hs[s % nh], non_blocking=True)
-        pipe.decode(dc, ds)
-    torch.cuda.synchronize()
-    e0.record(st)
+    ends = [torch.cuda.Event() for _ in range(S)]
+    e0.record(main)
+    for st in streams:
+        st.wait_event(e0)
     for s in range(K):
-        dc.copy_(hc[s % nh], non_blocking=True)
-        ds.copy_(hs[s % nh], non_blocking=True)
-        ws = pipe.decode(dc, ds)
-        flags[0].copy_(ws["conv"])
-        flags[1].copy_(ws["its"])
-        flags[2].copy_(ws["bad"])
-        flags[3].copy_(ws["ok"])
-        hp[s].copy_(ws["payload"], non_blocking=True)
-        hf[s].copy_(flags, non_blocking=True)
-    e1.record(st)
+        step(s)
+    for st, ev in zip(streams, ends):
+        ev.record(st)
+        main.wait_event(ev)
+    e1.record(main)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    h2d = nblk * pipe.ncell * (8 + 4)
+    h2d = nblk * pipes[0].ncell * (8 + 4)
     d2h = nblk * (kp // 8) + 4 * nblk * 4
     return {"value": world * K * nblk * kp / (ms / 1e3) / 1e6, "unit": "Mbit/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": ms / K}
+            "ms_per_step": ms / K, "streams": S,
+            "bch_ok_blocks": int(hf[:, 3].sum())}
 
 
 def cpu_baseline(args, nblk_per_esn0=6):
@@ -472,6 +571,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cluster", type=int, default=0)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--streams", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args(argv)
     if a.warmup < 3:
