@@ -402,9 +402,10 @@ def run_gpu(args, rank, world, local_rank):
     return line
 
 
-# DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch,
-# from the ncu capture summarised in profiles/ldpc_qc_flood_6_15_frame.md.
-TRAFFIC_PER_BLOCK = None
+# DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch:
+# dram__bytes_read.sum + dram__bytes_write.sum of one captured 75-block launch
+# (19,553,792 + 0 B) / 75, from profiles/ldpc_qc_flood_6_15_frame.md.
+TRAFFIC_PER_BLOCK = 19_553_792 / 75
 
 
 def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
