@@ -1,0 +1,793 @@
+// ldpc_qce.cu -- flooding normalised min-sum for the quasi-cyclic A/322 Type
+// B codes with an EDGE-BUFFER layout (sm_100a), bit-exact with
+// lab/ldpc_kernel.c (kernel semantics) and lab/m9_gpu.py:168-211 (torch
+// semantics), float32.
+//
+// The code structure used is the one of ldpc_qc.cu (360x360 circulants, at
+// most one per block, dual-diagonal parity part, edge order inside a check =
+// block-column order, a bit's summation order = its column's circulant list
+// sorted by (shift, row) and rotated at s0[col*360 + mm]).
+//
+// What differs is where the decoder state lives.  Every edge of the codeword
+// owns one float32 slot in the distributed shared memory of its cluster, in
+// the CTA that owns the edge's 360-bit column: column g's circulant slots are
+// contiguous 360-float blocks there, entry mm of slot i belongs to bit
+// (g, mm).  The slot holds
+//   * after the variable phase: q = tot - m, the variable-to-check value the
+//     reference computes inside its check update (ldpc_kernel.c:120,
+//     v = tot[j] - m[e]); the same rounded subtraction, done on the variable
+//     side;
+//   * after the check phase: m, the new check-to-variable message.
+// The check phase therefore reads each edge's q with one 4-byte remote load
+// (32 consecutive checks of a block row read 32 consecutive entries of a
+// circulant slot), forms min1/min2/first/signs in registers, and writes the
+// messages back into the same slots with posted remote stores.  The variable
+// phase is local: it sums its slots in the reference order, forms tot, and
+// rewrites every slot as tot - m.  No per-check records are kept.
+//
+// Hard decisions for the syndrome (ldpc_kernel.c:95-101 evaluates it on
+// tot before every update) live in a bitmap replicated in every CTA: 12
+// 32-bit words per 360-bit column (bit mm of column g = word g*12 + mm/32,
+// bit mm%32).  The variable phase writes each 32-bit ballot to every CTA of
+// the cluster; the check phase looks up its bits locally.
+//
+// Shared memory per CTA: bitmap (nb*48 B) | syndrome exchange (256 B) | the
+// edge slots of the CTA's columns (1440 B per slot).  For the 64800-bit codes
+// (about 281k edges, 1.1 MB of slots) an 8-CTA cluster holds a codeword.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/atsc3_fec.h"
+#include "common.cuh"
+
+namespace atsc3 {
+
+constexpr int EZ = 360;
+constexpr int ECHUNK = 12;                // ceil(360 / 32) warps per row/column
+constexpr int EMAXCL = 16;
+constexpr int EWRAP = 1 << 8;
+constexpr int ESLOT = EZ * 4;             // bytes of one circulant slot
+constexpr int EPART = 256;                // syndrome exchange bytes
+
+struct QcePlan {
+  int n = 0, K = 0, Q = 0, nb = 0;
+  int cluster = 1, smem = 0, part_off = 0;
+  int dr_max = 0, dc_max = 0, max_slots = 0, device = 0;
+  int64_t table_bytes = 0;
+  int rb[EMAXCL + 1] = {0};     // block rows of CTA c (check phase)
+  int cb[EMAXCL + 1] = {0};     // columns of CTA c (variable phase, slots)
+  int4 *d_rdesc = nullptr;      // per row edge slot
+  int32_t *d_rptr = nullptr;    // (Q+1)
+  int4 *d_cdesc = nullptr;      // per column
+  uint8_t *d_s0 = nullptr;      // (nb*360) rotation start
+};
+
+// Row slot (block row r, position j):  x = owner CTA | WRAP << 8 | j << 16,
+// y = byte offset of the edge's circulant slot in the owner's shared memory,
+// z = circulant shift u, w = byte offset of the column's bitmap words.
+// Check (r, k) reads entry (k - u) mod 360 of the slot.
+// Column descriptor (column g): x = slots d, y = byte offset of slot 0 in
+// the owner's shared memory (slots follow at 1440-byte steps, sorted by
+// (u, row)), z = index of the dual-diagonal wrap slot (absent for bit 359)
+// or -1, w = owner CTA.
+struct QceTables {
+  std::vector<int4> rdesc;
+  std::vector<int32_t> rptr;
+  std::vector<int4> cdesc;
+  std::vector<uint8_t> s0;
+};
+
+int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
+              int cluster, QcePlan *p, QceTables *t) {
+  if (n % EZ || K % EZ || Q <= 0 || (n - K) != Q * EZ) {
+    set_error("invalid argument: not a 360-circulant Type B code");
+    return -3;
+  }
+  if (cluster < 1 || cluster > EMAXCL || (cluster & (cluster - 1))) {
+    set_error("invalid argument: cluster must be 1, 2, 4, 8 or 16");
+    return -3;
+  }
+  const int nbi = K / EZ, nb = n / EZ;
+  struct Slot { int col, row, u, pos, wrap, idx; };
+  std::vector<std::vector<Slot>> rows(Q), cols(nb);
+  for (int g = 0; g < nbi; ++g)
+    for (int e = rowptr[g]; e < rowptr[g + 1]; ++e) {
+      const int x = addr[e];
+      if (x < 0 || x >= n - K) {
+        set_error("invalid argument: address outside the parity range");
+        return -3;
+      }
+      rows[x % Q].push_back(Slot{g, x % Q, x / Q, 0, 0, 0});
+    }
+  int drm = 0;
+  for (int r = 0; r < Q; ++r) {
+    auto &R = rows[r];
+    std::sort(R.begin(), R.end(),
+              [](const Slot &a, const Slot &b) { return a.col < b.col; });
+    for (size_t i = 1; i < R.size(); ++i)
+      if (R[i].col == R[i - 1].col) {
+        set_error("unsupported: two circulants share a block (use the CSR "
+                  "decoder)");
+        return -4;
+      }
+    // dual diagonal: bits K+360(r-1)+k and K+360r+k (r >= 1); K+k and
+    // K+360(Q-1)+k-1 (r = 0, absent for k = 0)
+    if (r >= 1) {
+      R.push_back(Slot{nbi + r - 1, r, 0, 0, 0, 0});
+      R.push_back(Slot{nbi + r, r, 0, 0, 0, 0});
+    } else {
+      R.push_back(Slot{nbi, 0, 0, 0, 0, 0});
+      R.push_back(Slot{nbi + Q - 1, 0, 1, 0, EWRAP, 0});
+    }
+    for (int i = 0; i < (int)R.size(); ++i) R[i].pos = i;
+    drm = std::max(drm, (int)R.size());
+  }
+  if (drm > 56) {
+    set_error("unsupported: block-row degree above 56");
+    return -4;
+  }
+  for (int r = 0; r < Q; ++r)
+    for (auto &sl : rows[r]) cols[sl.col].push_back(sl);
+  int dcm = 0, total = 0;
+  for (int g = 0; g < nb; ++g) {
+    auto &Cc = cols[g];
+    std::sort(Cc.begin(), Cc.end(), [](const Slot &a, const Slot &c) {
+      return a.u != c.u ? a.u < c.u : a.row < c.row;
+    });
+    for (int i = 0; i < (int)Cc.size(); ++i) {
+      Cc[i].idx = i;
+      for (auto &rs : rows[Cc[i].row])      // back-reference row slot -> idx
+        if (rs.col == g) rs.idx = i;
+    }
+    dcm = std::max(dcm, (int)Cc.size());
+    total += (int)Cc.size();
+  }
+  // columns split over the cluster in contiguous runs of about equal slots
+  p->cb[0] = 0;
+  {
+    int acc = 0, c = 1;
+    for (int g = 0; g < nb && c < cluster; ++g) {
+      acc += (int)cols[g].size();
+      while (c < cluster && (int64_t)acc * cluster >= (int64_t)total * c)
+        p->cb[c++] = g + 1;
+    }
+    while (c <= cluster) p->cb[c++] = nb;
+  }
+  const int per = (Q + cluster - 1) / cluster;
+  for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
+  const int bm_bytes = (nb * ECHUNK * 4 + 15) & ~15;
+  const int part_off = bm_bytes;
+  const int buf_off = bm_bytes + EPART;
+  std::vector<int> owner(nb), base(nb);
+  int maxs = 0;
+  for (int c = 0; c < cluster; ++c) {
+    int s = 0;
+    for (int g = p->cb[c]; g < p->cb[c + 1]; ++g) {
+      owner[g] = c;
+      base[g] = buf_off + s * ESLOT;
+      s += (int)cols[g].size();
+    }
+    maxs = std::max(maxs, s);
+  }
+  p->n = n; p->K = K; p->Q = Q; p->nb = nb;
+  p->cluster = cluster;
+  p->dr_max = drm;
+  p->dc_max = dcm;
+  p->max_slots = maxs;
+  p->part_off = part_off;
+  p->smem = buf_off + maxs * ESLOT;
+  t->rptr.assign(Q + 1, 0);
+  t->rdesc.clear();
+  for (int r = 0; r < Q; ++r) {
+    for (auto &sl : rows[r])
+      t->rdesc.push_back(make_int4(owner[sl.col] | sl.wrap | (sl.pos << 16),
+                                   base[sl.col] + sl.idx * ESLOT, sl.u,
+                                   sl.col * ECHUNK * 4));
+    t->rptr[r + 1] = (int)t->rdesc.size();
+  }
+  t->cdesc.assign(nb, make_int4(0, 0, -1, 0));
+  t->s0.assign((size_t)nb * EZ, 0);
+  for (int g = 0; g < nb; ++g) {
+    auto &Cc = cols[g];
+    int wrap = -1;
+    for (auto &sl : Cc)
+      if (sl.wrap) wrap = sl.idx;
+    t->cdesc[g] = make_int4((int)Cc.size(), base[g], wrap, owner[g]);
+    for (int mm = 0; mm < EZ; ++mm) {
+      int s = 0;
+      for (auto &sl : Cc) s += (sl.u + mm < EZ) ? 1 : 0;
+      t->s0[(size_t)g * EZ + mm] = (uint8_t)s;
+    }
+  }
+  return 0;
+}
+
+struct QceArgs {
+  const float *llr;
+  int64_t ld_llr;
+  int nblk, n, iters;
+  float alpha;
+  int part_off;
+  int rb[EMAXCL + 1];
+  int cb[EMAXCL + 1];
+  const int4 *rdesc;
+  const int32_t *rptr;
+  const int4 *cdesc;
+  const uint8_t *s0;
+  // optional learned weights, as ldpc_qc.cu: minima become
+  // relu(min*w_a - w_b), (w_a, w_b) = (walpha, wbeta)[min(it, wT-1)][
+  // dbucket[check degree]]; null -> (alpha, 0), bit-identical to min*alpha
+  const float *walpha;
+  const float *wbeta;
+  const int8_t *dbucket;
+  int wT, wnb;
+  uint8_t *bits;
+  int64_t ld_bits;
+  uint8_t *hard;
+  int64_t ld_hard;
+  uint8_t *conv;
+  int32_t *its;
+  int32_t *bad;
+};
+
+// NCH: chunks of 8 edge positions per block row (compile-time positions);
+// MASK: per-check bit-mask type (>= NCH*8 bits); NT: threads per CTA.
+template <bool TORCH, int NCH, typename MASK, int NT>
+__global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
+  constexpr int NS = NCH * 8;
+  constexpr int VB = 4;                               // variable-phase loads in flight
+  constexpr int MB = (int)sizeof(MASK) * 8;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int rank = (int)cluster_ctarank();
+  const int CL = (int)cluster_nctarank();
+  const uint32_t *bm = reinterpret_cast<const uint32_t *>(smem);
+  int *part = reinterpret_cast<int *>(smem + a.part_off);
+  int *sbad = part + 32;
+  const uint32_t sm_sa = smem_u32(smem);
+  const uint32_t part_sa = smem_u32(part);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int r0 = a.rb[rank], r1 = a.rb[rank + 1];
+  const int c0 = a.cb[rank], c1 = a.cb[rank + 1];
+  const int ncitems = (r1 - r0) * ECHUNK;
+  const int nvitems = (c1 - c0) * ECHUNK;
+  const uint32_t dummy = sm_sa;                       // own, always mapped
+
+  if (tid == 0) *sbad = 0;
+
+  for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
+    const float *lam = a.llr + (size_t)b * a.ld_llr;
+    // ---- prologue: q = lam - 0 = lam on every slot, hard bits of lam ------
+    for (int w = warp; w < nvitems; w += nwarps) {
+      const int gl = w / ECHUNK;
+      const int ch = w - gl * ECHUNK;
+      const int g = c0 + gl;
+      const int mm0 = ch * 32 + lane;
+      const bool mv = mm0 < EZ;
+      const int mm = mv ? mm0 : EZ - 1;
+      const int4 cd = __ldg(a.cdesc + g);
+      const float li = lam[g * EZ + mm];
+      float *col = reinterpret_cast<float *>(smem + cd.y) + mm;
+      if (mv)
+        for (int i = 0; i < cd.x; ++i) col[i * EZ] = li;
+      const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < 0.f);
+      if (lane < CL)
+        dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((g * ECHUNK + ch) * 4),
+                               (uint32_t)lane), hb);
+    }
+    __syncthreads();
+    cluster_sync_all();
+
+    for (int it = 0;; ++it) {
+      const bool upd = it < a.iters;   // the last pass only needs the syndrome
+      // ---------------- check phase ----------------------------------------
+      int mybad = 0;
+      for (int w = warp; w < ncitems; w += nwarps) {
+        const int rl = w / ECHUNK;
+        const int r = r0 + rl;
+        const int k0 = (w - rl * ECHUNK) * 32 + lane;
+        const bool kv = k0 < EZ;
+        const int k = kv ? k0 : EZ - 1;
+        const int rp = __ldg(a.rptr + r);
+        const int deg = __ldg(a.rptr + r + 1) - rp;
+        const int4 *ds = a.rdesc + rp;
+        uint32_t ad[NS];
+        uint32_t syn = 0;
+        MASK live = 0;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          const int4 d = __ldg(ds + min(j, deg - 1));
+          const bool on = j < deg && !((d.x & EWRAP) && k == 0);
+          int o = k - d.z;
+          o += o < 0 ? EZ : 0;
+          const uint32_t hw = bm[(d.w >> 2) + (o >> 5)];
+          syn ^= on ? (hw >> (o & 31)) & 1u : 0u;
+          ad[j] = on ? dsmem_map(sm_sa + (uint32_t)(d.y + 4 * o), (uint32_t)(d.x & 0xFF))
+                     : dummy;
+          if (on) live |= (MASK)1 << j;
+        }
+        mybad += kv ? (int)syn : 0;
+        if (upd) {
+          float min1 = __int_as_float(0x7f800000), min2 = min1;
+          uint32_t first = 0;
+          MASK sv = 0;
+#pragma unroll
+          for (int c = 0; c < NCH; ++c) {
+            float t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = dsmem_ld_f32(ad[c * 8 + u]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int j = c * 8 + u;
+              const MASK bit = (MASK)1 << j;
+              if (live & bit) {
+                if (t[u] < 0.f) sv |= bit;
+                const float mag = fabsf(t[u]);
+                if (mag < min1) { min2 = min1; min1 = mag; first = (uint32_t)j; }
+                else if (mag < min2) { min2 = mag; }
+              }
+            }
+          }
+          int par;
+          if constexpr (MB > 32) par = __popcll((unsigned long long)sv) & 1;
+          else par = __popc((uint32_t)sv) & 1;
+          if (kv) {
+            float wa = a.alpha, wb = 0.f;
+            if (a.walpha) {
+              int nl;
+              if constexpr (MB > 32) nl = __popcll((unsigned long long)live);
+              else nl = __popc((uint32_t)live);
+              const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+              wa = __ldg(a.walpha + wi);
+              wb = __ldg(a.wbeta + wi);
+            }
+            float A = __fsub_rn(__fmul_rn(min1, wa), wb);
+            float B = __fsub_rn(__fmul_rn(min2, wa), wb);
+            A = A > 0.f ? A : 0.f;
+            B = B > 0.f ? B : 0.f;
+            const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
+            const MASK neg = par ? (sv ^ live) : sv;   // message signs
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+              if (live & ((MASK)1 << j)) {
+                const uint32_t mg = ((uint32_t)j == first) ? ub : ua;
+                const uint32_t s = (uint32_t)(neg >> j) & 1u;
+                dsmem_st_u32(ad[j], mg | (s << 31));
+              }
+            }
+          }
+        }
+      }
+      mybad = __reduce_add_sync(0xffffffffu, mybad);
+      if (lane == 0 && mybad) atomicAdd(sbad, mybad);
+      __syncthreads();
+      if (tid < CL)
+        dsmem_st_u32(dsmem_map(part_sa + (uint32_t)(((it & 1) * 16 + rank) * 4),
+                               (uint32_t)tid),
+                     (uint32_t)*sbad);
+      cluster_sync_all();
+      int badct = 0;
+      for (int q = 0; q < CL; ++q) badct += part[(it & 1) * 16 + q];
+      if (tid == 0) *sbad = 0;
+      const bool done = (badct == 0) && (!TORCH || it > 0);
+      if (done || it >= a.iters) {
+        // outputs of this CTA's columns from its bitmap replica
+        if (a.hard) {
+          uint8_t *ho = a.hard + (size_t)b * a.ld_hard;
+          for (int by = c0 * 45 + tid; by < c1 * 45; by += blockDim.x) {
+            const int g = by / 45;
+            const int bb = (by - g * 45) * 8;
+            const uint32_t v = (bm[g * ECHUNK + (bb >> 5)] >> (bb & 31)) & 0xFFu;
+            ho[by] = (uint8_t)(__brev(v) >> 24);
+          }
+        }
+        if (a.bits) {
+          uint8_t *bo = a.bits + (size_t)b * a.ld_bits;
+          for (int i = c0 * EZ + tid; i < c1 * EZ; i += blockDim.x) {
+            const int g = i / EZ;
+            const int mm = i - g * EZ;
+            bo[i] = (uint8_t)((bm[g * ECHUNK + (mm >> 5)] >> (mm & 31)) & 1u);
+          }
+        }
+        if (rank == 0 && tid == 0) {
+          a.conv[b] = done ? 1 : 0;
+          a.its[b] = it;
+          a.bad[b] = done ? 0 : badct;
+        }
+        // every CTA has read its replica before the next codeword's prologue
+        // writes the replicas of the whole cluster
+        __syncthreads();
+        cluster_sync_all();
+        break;
+      }
+      // ---------------- variable phase (local) -----------------------------
+      for (int w = warp; w < nvitems; w += nwarps) {
+        const int gl = w / ECHUNK;
+        const int ch = w - gl * ECHUNK;
+        const int g = c0 + gl;
+        const int mm0 = ch * 32 + lane;
+        const bool mv = mm0 < EZ;
+        const int mm = mv ? mm0 : EZ - 1;
+        const int4 cd = __ldg(a.cdesc + g);
+        const int d = cd.x;
+        const int lamidx = g * EZ + mm;
+        const float li = lam[lamidx];
+        const int s0 = __ldg(a.s0 + lamidx);
+        const int skip = (mm == EZ - 1) ? cd.z : -1;   // absent wrap edge
+        float *col = reinterpret_cast<float *>(smem + cd.y) + mm;
+        float acc = TORCH ? li : 0.f;
+        if (d == 2) {
+          // dual-diagonal parity column (warp-uniform)
+          const int i0 = s0 >= 2 ? s0 - 2 : s0;
+          const int i1 = i0 == 0 ? 1 : 0;
+          const float m0 = col[i0 * EZ], m1 = col[i1 * EZ];
+          if (i0 != skip) acc = __fadd_rn(acc, m0);
+          if (i1 != skip) acc = __fadd_rn(acc, m1);
+          const float tot = TORCH ? acc : __fadd_rn(li, acc);
+          if (mv) {
+            if (i0 != skip) col[i0 * EZ] = __fsub_rn(tot, m0);
+            if (i1 != skip) col[i1 * EZ] = __fsub_rn(tot, m1);
+          }
+          const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
+          if (lane < CL)
+            dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((g * ECHUNK + ch) * 4),
+                                   (uint32_t)lane), hb);
+          continue;
+        }
+        for (int t0 = 0; t0 < d; t0 += VB) {
+          float m[VB];
+          bool on[VB];
+#pragma unroll
+          for (int u = 0; u < VB; ++u) {
+            int i = s0 + t0 + u;
+            i -= i >= d ? d : 0;
+            on[u] = (t0 + u < d) && i != skip;
+            i = t0 + u < d ? i : 0;
+            m[u] = col[i * EZ];
+          }
+#pragma unroll
+          for (int u = 0; u < VB; ++u)
+            if (on[u]) acc = __fadd_rn(acc, m[u]);
+        }
+        const float tot = TORCH ? acc : __fadd_rn(li, acc);
+        if (mv) {
+          for (int i0 = 0; i0 < d; i0 += VB) {
+            float m[VB];
+#pragma unroll
+            for (int u = 0; u < VB; ++u) m[u] = col[min(i0 + u, d - 1) * EZ];
+#pragma unroll
+            for (int u = 0; u < VB; ++u)
+              if (i0 + u < d && i0 + u != skip) col[(i0 + u) * EZ] = __fsub_rn(tot, m[u]);
+          }
+        }
+        const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
+        if (lane < CL)
+          dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((g * ECHUNK + ch) * 4),
+                                 (uint32_t)lane), hb);
+      }
+      __syncthreads();
+      cluster_sync_all();
+    }
+  }
+  __syncthreads();
+  cluster_sync_all();
+}
+
+typedef void (*QceFn)(const QceArgs);
+
+#define ATSC3_QCE_FN(NCH, MASK)                                             \
+  (nt == 1024 ? (semantics ? ldpc_qce_kernel<true, NCH, MASK, 1024>          \
+                           : ldpc_qce_kernel<false, NCH, MASK, 1024>)        \
+              : (semantics ? ldpc_qce_kernel<true, NCH, MASK, 512>           \
+                           : ldpc_qce_kernel<false, NCH, MASK, 512>))
+
+// > 512 threads -> the 1024-thread build (64 registers), else 512 (128).
+static QceFn qce_fn(int semantics, int dr, int threads) {
+  const int nt = threads > 512 ? 1024 : 512;
+  if (dr <= 8) return ATSC3_QCE_FN(1, uint32_t);
+  if (dr <= 16) return ATSC3_QCE_FN(2, uint32_t);
+  if (dr <= 24) return ATSC3_QCE_FN(3, uint32_t);
+  if (dr <= 32) return ATSC3_QCE_FN(4, uint32_t);
+  if (dr <= 40) return ATSC3_QCE_FN(5, unsigned long long);
+  if (dr <= 56) return ATSC3_QCE_FN(7, unsigned long long);
+  return nullptr;
+}
+
+// default CTA size: 1024 threads while a check's slot addresses fit the
+// 64-register budget without spilling (block-row degree <= 8), else 512
+static int qce_default_threads(int dr) { return dr <= 8 ? 1024 : 512; }
+
+static std::mutex g_qce_mu;
+static std::unordered_map<uint64_t, int> g_qce_occ;
+static std::unordered_map<uint64_t, int> g_qce_attr;
+
+static int32_t qce_prepare(QceFn fn, int dev) {
+  const uint64_t key = (uint64_t)(uintptr_t)fn ^ ((uint64_t)dev << 56);
+  {
+    std::lock_guard<std::mutex> g(g_qce_mu);
+    if (g_qce_attr.count(key)) return 0;
+  }
+  int smax = 0;
+  ATSC3_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  ATSC3_CUDA(cudaFuncSetAttribute((const void *)fn,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  ATSC3_CUDA(cudaFuncSetAttribute(
+      (const void *)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  std::lock_guard<std::mutex> g(g_qce_mu);
+  g_qce_attr[key] = 1;
+  return 0;
+}
+
+static int32_t qce_max_clusters(QceFn fn, int cl, int smem, int threads, int dev,
+                                int *out) {
+  const uint64_t key = ((uint64_t)(uintptr_t)fn * 1315423911ull) ^
+                       ((uint64_t)cl << 1) ^ ((uint64_t)smem << 8) ^
+                       ((uint64_t)threads << 30) ^ ((uint64_t)dev << 44);
+  {
+    std::lock_guard<std::mutex> g(g_qce_mu);
+    auto it = g_qce_occ.find(key);
+    if (it != g_qce_occ.end()) {
+      *out = it->second;
+      return 0;
+    }
+  }
+  int32_t rc = qce_prepare(fn, dev);
+  if (rc) return rc;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  ATSC3_CUDA(cudaOccupancyMaxActiveClusters(&n, (const void *)fn, &cfg));
+  std::lock_guard<std::mutex> g(g_qce_mu);
+  g_qce_occ[key] = n;
+  *out = n;
+  return 0;
+}
+
+}  // namespace atsc3
+
+struct atsc3_ldpc_qce_plan {
+  atsc3::QcePlan p;
+};
+
+extern "C" {
+
+int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
+                                   const int32_t *rowptr, const int32_t *addr,
+                                   int32_t cluster, atsc3_ldpc_qce_plan **out) {
+  using namespace atsc3;
+  ATSC3_ARG(out && rowptr && addr, "null argument");
+  *out = nullptr;
+  int dev = 0;
+  ATSC3_CUDA(cudaGetDevice(&dev));
+  int smax = 0;
+  ATSC3_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  auto *h = new atsc3_ldpc_qce_plan();
+  QceTables t;
+  int rc = -4;
+  if (cluster == 0) {
+    // smallest cluster whose per-CTA shared memory fits; a structural
+    // rejection (-3, -4 from the build) ends the search with its message
+    bool fits = false;
+    for (int cl = 1; cl <= EMAXCL; cl <<= 1) {
+      rc = qce_build(n, kldpc, qldpc, rowptr, addr, cl, &h->p, &t);
+      if (rc) break;
+      if (h->p.smem <= smax) {
+        fits = true;
+        break;
+      }
+    }
+    if (rc == 0 && !fits) {
+      set_error("unsupported: no cluster size fits");
+      rc = -4;
+    }
+  } else {
+    rc = qce_build(n, kldpc, qldpc, rowptr, addr, cluster, &h->p, &t);
+    if (rc == 0 && h->p.smem > smax) {
+      set_error("unsupported: per-CTA shared memory above the device limit");
+      rc = -4;
+    }
+  }
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  h->p.device = dev;
+  auto up = [&](void **dst, const void *src, size_t bytes) -> cudaError_t {
+    cudaError_t e = cudaMalloc(dst, bytes ? bytes : 16);
+    if (e != cudaSuccess) return e;
+    h->p.table_bytes += (int64_t)bytes;
+    return bytes ? cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  cudaError_t e = up((void **)&h->p.d_rdesc, t.rdesc.data(), t.rdesc.size() * 16);
+  if (e == cudaSuccess) e = up((void **)&h->p.d_rptr, t.rptr.data(), t.rptr.size() * 4);
+  if (e == cudaSuccess) e = up((void **)&h->p.d_cdesc, t.cdesc.data(), t.cdesc.size() * 16);
+  if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
+  if (e != cudaSuccess) {
+    atsc3_ldpc_qce_plan_destroy(h);
+    return cuda_fail(e, "qce plan upload");
+  }
+  *out = h;
+  return 0;
+}
+
+void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
+  if (!h) return;
+  cudaFree(h->p.d_rdesc);
+  cudaFree(h->p.d_rptr);
+  cudaFree(h->p.d_cdesc);
+  cudaFree(h->p.d_s0);
+  delete h;
+}
+
+int32_t atsc3_ldpc_qce_plan_info(const atsc3_ldpc_qce_plan *h, int64_t *info) {
+  ATSC3_ARG(h && info, "null argument");
+  info[0] = h->p.n;
+  info[1] = h->p.K;
+  info[2] = h->p.Q;
+  info[3] = h->p.cluster;
+  info[4] = h->p.smem;
+  info[5] = h->p.dr_max;
+  info[6] = h->p.dc_max;
+  info[7] = h->p.table_bytes;
+  info[8] = h->p.max_slots;
+  info[9] = h->p.cb[1] - h->p.cb[0];
+  return 0;
+}
+
+int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
+                                   const int32_t *rowptr, const int32_t *addr,
+                                   int32_t cluster, int32_t *meta,
+                                   int32_t *rdesc, int32_t *rptr,
+                                   int32_t *cdesc, uint8_t *s0) {
+  using namespace atsc3;
+  ATSC3_ARG(meta && rowptr && addr, "null argument");
+  QcePlan p;
+  QceTables t;
+  int rc = qce_build(n, kldpc, qldpc, rowptr, addr, cluster, &p, &t);
+  if (rc) return rc;
+  meta[0] = (int32_t)t.rdesc.size();
+  meta[1] = p.nb;
+  meta[2] = p.smem;
+  meta[3] = p.part_off;
+  meta[4] = p.dr_max;
+  meta[5] = p.dc_max;
+  meta[6] = p.max_slots;
+  for (int c = 0; c <= EMAXCL; ++c) {
+    meta[8 + c] = p.rb[c];
+    meta[25 + c] = p.cb[c];
+  }
+  if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
+  if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
+  if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
+  if (s0) std::memcpy(s0, t.s0.data(), t.s0.size());
+  return 0;
+}
+
+int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *h, int32_t threads,
+                              int32_t semantics, int32_t *out) {
+  using namespace atsc3;
+  ATSC3_ARG(h && out, "null argument");
+  if (threads <= 0) threads = qce_default_threads(h->p.dr_max);
+  QceFn fn = qce_fn(semantics, h->p.dr_max, threads);
+  ATSC3_ARG(fn != nullptr, "no kernel for this degree");
+  int ncl = 0;
+  int32_t rc = qce_max_clusters(fn, h->p.cluster, h->p.smem, threads, h->p.device, &ncl);
+  if (rc) return rc;
+  out[0] = ncl;
+  out[1] = h->p.cluster;
+  out[2] = h->p.smem;
+  out[3] = threads;
+  return 0;
+}
+
+int32_t atsc3_ldpc_qce_decode_weighted(
+    const atsc3_ldpc_qce_plan *h, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream) {
+  using namespace atsc3;
+  ATSC3_ARG(h != nullptr, "null plan");
+  const QcePlan &p = h->p;
+  ATSC3_ARG(nblk >= 0 && iters >= 0, "negative size");
+  ATSC3_ARG(semantics == 0 || semantics == 1, "semantics must be 0 or 1");
+  ATSC3_ARG(!(semantics == 1 && iters == 0), "semantics 1 needs iters >= 1");
+  ATSC3_ARG(ld_llr >= p.n, "ld_llr < n");
+  ATSC3_ARG(bits == nullptr || ld_bits >= p.n, "ld_bits < n");
+  ATSC3_ARG(hard == nullptr || ld_hard >= (p.n + 7) / 8, "ld_hard < ceil(n/8)");
+  if (nblk == 0) return 0;
+  ATSC3_ARG(conv && its && bad, "null status output");
+  ATSC3_ARG(llr != nullptr, "null llr");
+  if (threads <= 0) threads = qce_default_threads(p.dr_max);
+  ATSC3_ARG(threads == 512 || threads == 1024, "threads must be 512 or 1024");
+  QceFn fn = qce_fn(semantics, p.dr_max, threads);
+  if (!fn) {
+    set_error("unsupported: block-row degree too high");
+    return -4;
+  }
+  int ncl = 0;
+  int32_t rc = qce_max_clusters(fn, p.cluster, p.smem, threads, p.device, &ncl);
+  if (rc) return rc;
+  if (ncl <= 0) {
+    set_error("unsupported: cluster configuration cannot be resident");
+    return -4;
+  }
+  ncl = std::min(ncl, nblk);
+  QceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.llr = llr;
+  a.ld_llr = ld_llr;
+  a.nblk = nblk;
+  a.n = p.n;
+  a.iters = iters;
+  a.alpha = alpha;
+  a.part_off = p.part_off;
+  for (int c = 0; c <= EMAXCL; ++c) {
+    a.rb[c] = p.rb[c];
+    a.cb[c] = p.cb[c];
+  }
+  a.rdesc = p.d_rdesc;
+  a.rptr = p.d_rptr;
+  a.cdesc = p.d_cdesc;
+  a.s0 = p.d_s0;
+  if (walpha) {
+    ATSC3_ARG(wbeta && dbucket && wT > 0 && wnb > 0,
+              "weights need wbeta, dbucket, wT > 0, wnb > 0");
+    a.walpha = walpha;
+    a.wbeta = wbeta;
+    a.dbucket = dbucket;
+    a.wT = wT;
+    a.wnb = wnb;
+  }
+  a.bits = bits;
+  a.ld_bits = ld_bits;
+  a.hard = hard;
+  a.ld_hard = ld_hard;
+  a.conv = conv;
+  a.its = its;
+  a.bad = bad;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ncl * p.cluster, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = p.smem;
+  cfg.stream = (cudaStream_t)stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = p.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ATSC3_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
+  return 0;
+}
+
+int32_t atsc3_ldpc_qce_decode(const atsc3_ldpc_qce_plan *h, const float *llr,
+                              int64_t ld_llr, int32_t nblk, int32_t iters,
+                              float alpha, int32_t semantics, uint8_t *bits,
+                              int64_t ld_bits, uint8_t *hard, int64_t ld_hard,
+                              uint8_t *conv, int32_t *its, int32_t *bad,
+                              int32_t threads, void *stream) {
+  return atsc3_ldpc_qce_decode_weighted(h, llr, ld_llr, nblk, iters, alpha,
+                                        semantics, nullptr, nullptr, 0, 0,
+                                        nullptr, bits, ld_bits, hard, ld_hard,
+                                        conv, its, bad, threads, stream);
+}
+
+}  // extern "C"

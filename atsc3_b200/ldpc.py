@@ -118,25 +118,68 @@ class QcPlan:
             self._h = None
 
 
+class QcePlan(QcPlan):
+    """Quasi-cyclic plan with the edge-buffer state layout (csrc/ldpc_qce.cu):
+    one float32 slot per edge in the distributed shared memory of the edge's
+    column owner, no per-check records.  Same codes, semantics and outputs
+    as QcPlan; cluster 0 picks the smallest cluster that holds a codeword."""
+
+    kind = "qce"
+
+    def __init__(self, rate, n, cluster=0):
+        typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+        if typ != "B":
+            raise ValueError("the quasi-cyclic decoder serves Type B codes")
+        rowptr, addr = C.address_rows(rate, n)
+        rowptr = np.ascontiguousarray(rowptr, np.int32)
+        addr = np.ascontiguousarray(addr, np.int32)
+        h = ctypes.c_void_p()
+        N.call("atsc3_ldpc_qce_plan_create", n, K, Q2, rowptr.ctypes.data,
+               addr.ctypes.data, int(cluster), ctypes.byref(h))
+        self._h = h
+        self.n, self.nc, self.dtype = n, n - K, "float32"
+        info = np.zeros(10, np.int64)
+        N.call("atsc3_ldpc_qce_plan_info", h, info.ctypes.data)
+        self.info = dict(zip(("n", "K", "Q", "cluster", "smem_bytes",
+                              "dr_max", "dc_max", "table_bytes",
+                              "max_slots_per_cta", "cols_cta0"),
+                             info.tolist()))
+        self.info["kind"] = "qce"
+        self.cluster = self.info["cluster"]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                N.lib().atsc3_ldpc_qce_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
 _PLANS = {}
 _PLANS_LOCK = threading.Lock()
 
 
 def plan_for(rate, n, dtype="float32", cluster=0, kind="auto"):
-    """Cached plan of an A/322 code.  kind "auto" picks the quasi-cyclic
-    decoder for the Type B codes it accepts (float32), else the CSR one."""
+    """Cached plan of an A/322 code.  kind "auto" picks, for the Type B codes
+    in float32, the edge-buffer quasi-cyclic decoder, then the record-layout
+    one, whichever first accepts the code; else the CSR decoder.  kind "qce"
+    or "qc" asks for that decoder (raising if it rejects a Type B code);
+    codes outside its reach (Type A, float64) get the CSR decoder."""
     torch = _torch()
     key = (rate, n, dtype, cluster, kind, torch.cuda.current_device())
     with _PLANS_LOCK:
         p = _PLANS.get(key)
         if p is None:
-            if kind in ("auto", "qc") and dtype == "float32" and \
-                    C.ldpc_params(rate, n)[0] == "B":
-                try:
-                    p = QcPlan(rate, n, cluster=cluster)
-                except N.FecError as e:
-                    if kind == "qc" or e.rc != -4:
-                        raise
+            qc_ok = dtype == "float32" and C.ldpc_params(rate, n)[0] == "B"
+            for k, cls in (("qce", QcePlan), ("qc", QcPlan)):
+                if p is None and kind in ("auto", k) and qc_ok:
+                    try:
+                        p = cls(rate, n, cluster=cluster)
+                    except N.FecError as e:
+                        if kind == k or e.rc != -4:
+                            raise
             if p is None:
                 p = Plan(*C.csr(rate, n), n, dtype=dtype, cluster=cluster)
             _PLANS[key] = p
@@ -171,15 +214,18 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     bits = o.get("bits") if want_bits else None
     hard = o.get("hard") if want_hard else None
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
-    if weights is not None and getattr(plan, "kind", "csr") != "qc":
-        raise ValueError("learned weights run on the quasi-cyclic decoder")
-    if getattr(plan, "kind", "csr") == "qc":
+    kind = getattr(plan, "kind", "csr")
+    if weights is not None and kind not in ("qc", "qce"):
+        raise ValueError("learned weights run on the quasi-cyclic decoders")
+    if kind in ("qc", "qce"):
         wa = wb = db = None
         wT = wnb = 0
         if weights is not None:
             wa, wb, db = weights
             wT, wnb = wa.shape
-        N.call("atsc3_ldpc_qc_decode_weighted", plan.handle, llr.data_ptr(),
+        fn = ("atsc3_ldpc_qc_decode_weighted" if kind == "qc"
+              else "atsc3_ldpc_qce_decode_weighted")
+        N.call(fn, plan.handle, llr.data_ptr(),
                llr.stride(0), nblk, int(iters), float(alpha),
                SEMANTICS[semantics], N.ptr(wa), N.ptr(wb), wT, wnb, N.ptr(db),
                N.ptr(bits),

@@ -24,10 +24,11 @@ def _torch():
 
 
 class FecPipeline:
-    """One (Ninner, constellation, rate) PLP configuration."""
+    """One (Ninner, constellation, rate) PLP configuration.  kind selects the
+    LDPC decoder ("auto", "qce", "qc" or "csr"; see ldpc.plan_for)."""
 
     def __init__(self, n, mod, rate, iters=50, alpha=0.75, semantics="kernel",
-                 cluster=0, threads=0, device="cuda"):
+                 cluster=0, threads=0, device="cuda", kind="auto"):
         torch = _torch()
         self.n, self.mod, self.rate = int(n), mod, rate
         self.nb = C.MOD_BITS[mod]
@@ -39,7 +40,7 @@ class FecPipeline:
         self.threads = threads
         self.device = torch.device(device)
         with torch.cuda.device(self.device):
-            self.plan = LDPC.plan_for(rate, n, "float32", cluster)
+            self.plan = LDPC.plan_for(rate, n, "float32", cluster, kind=kind)
         self._ws = {}
 
     def _buffers(self, nblk):

@@ -260,7 +260,8 @@ def run_gpu(args, rank, world, local_rank):
     S = max(1, args.streams)
     # one pipeline (workspace) per stream; they share the decoder plan
     pipes = [FecPipeline(N_INNER, MOD, RATE, iters=ITERS, alpha=ALPHA,
-                         cluster=args.cluster, threads=args.threads, device=dev)
+                         cluster=args.cluster, threads=args.threads, device=dev,
+                         kind=args.decoder)
              for _ in range(S)]
     streams = [torch.cuda.Stream(dev) for _ in range(S)]
 
@@ -383,7 +384,8 @@ def run_gpu(args, rank, world, local_rank):
                              "frac": achieved / hbm,
                              "traffic": (TRAFFIC_PER_BLOCK * nblk
                                          if TRAFFIC_PER_BLOCK else None),
-                             "kernel": "ldpc_qc_kernel (quasi-cyclic flooding)",
+                             "kernel": KERNEL_NAMES.get(p0.plan.info.get("kind"),
+                                                        "ldpc_flood_kernel (CSR flooding)"),
                              "peak_kind": peak_kind,
                              "bytes_per_launch": b_ldpc,
                              "ms_per_launch": ldpc_ms},
@@ -401,6 +403,9 @@ def run_gpu(args, rank, world, local_rank):
                 "plan": p0.plan.info}
     return line
 
+
+KERNEL_NAMES = {"qce": "ldpc_qce_kernel (quasi-cyclic flooding, edge-buffer layout)",
+                "qc": "ldpc_qc_kernel (quasi-cyclic flooding, record layout)"}
 
 # DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch:
 # dram__bytes_read.sum + dram__bytes_write.sum of one captured 75-block launch
@@ -573,6 +578,8 @@ def main(argv=None):
     ap.add_argument("--cluster", type=int, default=0)
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--streams", type=int, default=2)
+    ap.add_argument("--decoder", default="auto", choices=["auto", "qce", "qc", "csr"],
+                    help="LDPC decoder (auto = edge-buffer quasi-cyclic)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args(argv)
     if a.warmup < 3:

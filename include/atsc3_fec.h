@@ -176,6 +176,67 @@ int32_t atsc3_ldpc_qc_decode_weighted(
     int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
     int32_t threads, void *stream);
 
+/* ---- quasi-cyclic decoder, edge-buffer layout ------------------------------
+ * Same codes, semantics, arguments and outputs as the atsc3_ldpc_qc_*
+ * functions above (they replace the same reference entry points:
+ * lab/ldpc_kernel.c:65 ldpc_minsum_f32 and lab/m9_gpu.py:138-220
+ * GpuMinSum.decode for the Type B codes), with a different state layout
+ * (csrc/ldpc_qce.cu): one float32 slot per edge, owned by the edge's column,
+ * holding the variable-to-check value after the variable phase and the
+ * check-to-variable message after the check phase; hard decisions in a
+ * bitmap replicated per CTA; no per-check records.  cluster 0 picks the
+ * smallest cluster whose per-CTA shared memory fits (8 for the 64800-bit
+ * codes, 2 for the 16200-bit ones). */
+typedef struct atsc3_ldpc_qce_plan atsc3_ldpc_qce_plan;
+
+int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
+                                   const int32_t *rowptr, const int32_t *addr,
+                                   int32_t cluster, atsc3_ldpc_qce_plan **out);
+void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *plan);
+
+/* info[0]=n [1]=K [2]=Q [3]=cluster [4]=shared bytes per CTA [5]=max
+ * block-row degree [6]=max block-column degree [7]=table bytes [8]=most edge
+ * slots (360 edges each) held by one CTA [9]=360-bit columns of CTA 0 */
+int32_t atsc3_ldpc_qce_plan_info(const atsc3_ldpc_qce_plan *plan, int64_t *info);
+
+/* Host-only descriptor build for the CPU tests (no CUDA call).  meta (42
+ * ints): [0] row slots [1] 360-bit columns [2] shared bytes per CTA [3]
+ * byte offset of the syndrome exchange words [4] max row degree [5] max
+ * column degree [6] most slots per CTA [8..24] block-row split [25..41]
+ * column split.  rdesc: int4 per row slot (owner | wrap<<8 | position<<16,
+ * slot byte offset in the owner, shift, bitmap byte offset of the column);
+ * cdesc: int4 per column (slots, byte offset of slot 0, wrap slot or -1,
+ * owner).  Array outputs may be null. */
+int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
+                                   const int32_t *rowptr, const int32_t *addr,
+                                   int32_t cluster, int32_t *meta,
+                                   int32_t *rdesc, int32_t *rptr,
+                                   int32_t *cdesc, uint8_t *s0);
+
+/* out[0] = clusters resident at once, [1] = CTAs per cluster, [2] = shared
+ * bytes per CTA, [3] = threads per CTA (threads 0 = the default). */
+int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *plan, int32_t threads,
+                              int32_t semantics, int32_t *out);
+
+/* threads: 0 (default: 1024 for block-row degree <= 8, else 512), 512 or
+ * 1024.  ld_hard >= ceil(n/8). */
+int32_t atsc3_ldpc_qce_decode(const atsc3_ldpc_qce_plan *plan, const float *llr,
+                              int64_t ld_llr, int32_t nblk, int32_t iters,
+                              float alpha, int32_t semantics, uint8_t *bits,
+                              int64_t ld_bits, uint8_t *hard, int64_t ld_hard,
+                              uint8_t *conv, int32_t *its, int32_t *bad,
+                              int32_t threads, void *stream);
+
+/* As atsc3_ldpc_qce_decode with learned weights (the weighting of
+ * atsc3_ldpc_qc_decode_weighted). */
+int32_t atsc3_ldpc_qce_decode_weighted(
+    const atsc3_ldpc_qce_plan *plan, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream);
+
 /* ---- layered decoder for the A/322 Type B codes ----------------------------
  * Layered normalised min-sum: the Q block rows are the layers, the posterior
  * is updated in place after each layer, syndrome before the first and after

@@ -177,12 +177,13 @@ def test_known_answer_all_erasure(torch):
 
 
 @pytest.mark.parametrize("n,kind", [(16200, "auto"), (64800, "auto"),
-                                    (64800, "csr")])
+                                    (64800, "qc"), (64800, "csr")])
 def test_all_codes_random_llr_vs_oracle(n, kind, torch):
     """Every A/322 rate (Type A and B), random LLRs near the waterfall,
     few iterations: the GPU decoder equals the oracle field by field.  kind
-    "auto" runs the quasi-cyclic decoder on the 64800 Type B codes, "csr"
-    forces the CSR decoder on all of them."""
+    "auto" runs the edge-buffer quasi-cyclic decoder on the Type B codes it
+    accepts, "qc" the record-layout one, "csr" forces the CSR decoder on all
+    of them (Type A codes always take the CSR decoder)."""
     from atsc3_b200 import ldpc as LDPC
     rng = np.random.default_rng(n)
     for rate in C.RATES:
@@ -296,17 +297,20 @@ def test_demap_llr_fast_dropin(torch):
     assert np.array_equal(got.astype(np.float32), q2[1])
 
 
-@pytest.mark.parametrize("cluster", [4, 8, 16])
+@pytest.mark.parametrize("kind,cluster,threads", [
+    ("qc", 4, 0), ("qc", 8, 0), ("qc", 16, 0),
+    ("qce", 8, 0), ("qce", 16, 0), ("qce", 8, 512)])
 @pytest.mark.parametrize("rate", ["6/15", "8/15", "9/15", "10/15", "11/15",
                                   "12/15", "13/15"])
-def test_qc_decoder_vs_oracle(rate, cluster, torch):
-    """Quasi-cyclic decoder, every 64800 Type B rate, several cluster sizes,
+def test_qc_decoder_vs_oracle(rate, kind, cluster, threads, torch):
+    """Both quasi-cyclic decoders (record layout "qc", edge-buffer layout
+    "qce"), every 64800 Type B rate, several cluster sizes and CTA sizes,
     both semantics, against the oracle (30 iterations, mixed convergence)."""
     from atsc3_b200 import native as N
-    from atsc3_b200.ldpc import QcPlan, decode_flood
+    from atsc3_b200.ldpc import QcePlan, QcPlan, decode_flood
     n = 64800
     try:
-        plan = QcPlan(rate, n, cluster=cluster)
+        plan = (QcPlan if kind == "qc" else QcePlan)(rate, n, cluster=cluster)
     except N.FecError as e:
         assert e.rc == -4
         pytest.skip(str(e))
@@ -317,7 +321,7 @@ def test_qc_decoder_vs_oracle(rate, cluster, torch):
     for sem, code in (("kernel", 0), ("torch", 1)):
         want = oracle.flood(llr, tabs, n, iters=30, alpha=0.75, semantics=code)
         o = decode_flood(plan, x, iters=30, alpha=0.75, semantics=sem,
-                         want_hard=True)
+                         want_hard=True, threads=threads)
         bits = o["bits"].cpu().numpy()
         assert np.array_equal(bits, want[0]), (rate, sem)
         assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
@@ -327,7 +331,7 @@ def test_qc_decoder_vs_oracle(rate, cluster, torch):
                               np.packbits(bits, axis=1))
 
 
-@pytest.mark.parametrize("kind", ["qc", "csr"])
+@pytest.mark.parametrize("kind", ["qce", "qc", "csr"])
 def test_many_codewords_per_cluster_outputs_consistent(kind, torch):
     """More codewords than resident clusters: every cluster decodes several
     codewords in turn; packed hard decisions, bits and status of every block
@@ -347,3 +351,47 @@ def test_many_codewords_per_cluster_outputs_consistent(kind, torch):
     want = oracle.flood(llr[sel], C.csr(rate, n), n, iters=8)
     assert np.array_equal(bits[sel], want[0])
     assert o["its"].cpu().numpy()[sel].tolist() == want[2].tolist()
+
+
+@pytest.mark.parametrize("rate", ["7/15", "9/15", "11/15"])
+@pytest.mark.parametrize("cluster", [2, 4])
+def test_qce_16200_codes_vs_oracle(rate, cluster, torch):
+    """Edge-buffer decoder on the 16200-bit Type B codes it accepts, both
+    semantics, packed and unpacked outputs, against the oracle."""
+    from atsc3_b200.ldpc import QcePlan, decode_flood
+    n = 16200
+    plan = QcePlan(rate, n, cluster=cluster)
+    rng = np.random.default_rng(cluster + 7 * len(rate))
+    tabs = C.csr(rate, n)
+    llr = (rng.standard_normal((9, n)) * 2.0 + 1.5).astype(np.float32)
+    llr[4] = np.abs(llr[4])                          # clean block: its == 0
+    x = torch.from_numpy(llr).cuda()
+    for sem, code in (("kernel", 0), ("torch", 1)):
+        want = oracle.flood(llr, tabs, n, iters=25, alpha=0.75, semantics=code)
+        o = decode_flood(plan, x, iters=25, alpha=0.75, semantics=sem,
+                         want_hard=True)
+        bits = o["bits"].cpu().numpy()
+        assert np.array_equal(bits, want[0]), (rate, sem)
+        assert o["its"].cpu().numpy().tolist() == want[2].tolist(), (rate, sem)
+        assert o["bad"].cpu().numpy().tolist() == want[3].tolist(), (rate, sem)
+        assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
+        assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
+                              np.packbits(bits, axis=1))
+
+
+def test_qce_iters_zero_and_empty_batch(torch):
+    """iters=0 only evaluates the syndrome of the channel LLRs (its 0); an
+    empty batch launches nothing."""
+    from atsc3_b200.ldpc import QcePlan, decode_flood
+    rate, n = "10/15", 64800
+    plan = QcePlan(rate, n)
+    rng = np.random.default_rng(5)
+    llr = (rng.standard_normal((3, n)) * 2.0 + 1.0).astype(np.float32)
+    llr[1] = np.abs(llr[1])
+    want = oracle.flood(llr, C.csr(rate, n), n, iters=0, alpha=0.75)
+    o = decode_flood(plan, torch.from_numpy(llr).cuda(), iters=0)
+    assert np.array_equal(o["bits"].cpu().numpy(), want[0])
+    assert o["its"].cpu().numpy().tolist() == [0, 0, 0]
+    assert o["bad"].cpu().numpy().tolist() == want[3].tolist()
+    e = decode_flood(plan, torch.zeros((0, n), dtype=torch.float32, device="cuda"))
+    assert e["its"].numel() == 0

@@ -89,10 +89,12 @@ def test_wms_bf16_messages_close_to_fp32():
     assert abs(l16 - l32) <= 0.05 * abs(l32) + 1e-4
 
 
-def test_weighted_qc_decoder_matches_wms_forward():
-    """The inference decoder with learned weights (quasi-cyclic, torch
-    semantics) computes the same posterior as the differentiable forward for
-    blocks that run all T iterations: identical hard decisions."""
+@pytest.mark.parametrize("kind", ["qce", "qc"])
+def test_weighted_qc_decoder_matches_wms_forward(kind):
+    """The inference decoder with learned weights (both quasi-cyclic layouts,
+    torch semantics) computes the same posterior as the differentiable
+    forward for blocks that run all T iterations: identical hard
+    decisions."""
     import torch
     from atsc3_b200.ldpc import decode_flood, plan_for
     from atsc3_b200.learned import WeightedMinSum, WmsCode, inference_weights
@@ -105,7 +107,7 @@ def test_weighted_qc_decoder_matches_wms_forward():
     b = torch.tensor(0.1 * rng.random((T, code.nbucket)), dtype=torch.float32, device="cuda")
     x = torch.from_numpy(lam).cuda()
     ref = (WeightedMinSum.apply(x, a, b, code, False) < 0).to(torch.uint8).cpu().numpy()
-    plan = plan_for(rate, n)
+    plan = plan_for(rate, n, kind=kind)
     o = decode_flood(plan, x, iters=T, semantics="torch",
                      weights=inference_weights(a, b, code.buckets))
     its = o["its"].cpu().numpy()
@@ -117,7 +119,8 @@ def test_weighted_qc_decoder_matches_wms_forward():
         assert np.array_equal(bits[i], ref[i])
 
 
-def test_weighted_qc_with_zero_offset_is_plain():
+@pytest.mark.parametrize("kind", ["qce", "qc"])
+def test_weighted_qc_with_zero_offset_is_plain(kind):
     import torch
     from atsc3_b200.ldpc import decode_flood, plan_for
     from atsc3_b200.learned import WmsCode, inference_weights
@@ -126,8 +129,28 @@ def test_weighted_qc_with_zero_offset_is_plain():
     code = WmsCode(rate, n)
     a, b = code.init_params(5, 0.75, 0.0)
     x = torch.from_numpy(lam).cuda()
-    plan = plan_for(rate, n)
+    plan = plan_for(rate, n, kind=kind)
     p = decode_flood(plan, x, iters=50)
     w = decode_flood(plan, x, iters=50, weights=inference_weights(a, b, code.buckets))
     for k in ("bits", "conv", "its", "bad"):
         assert torch.equal(p[k], w[k]), k
+
+
+def test_weighted_layouts_agree():
+    """Learned weights with a nonzero offset: the edge-buffer and the
+    record-layout decoders give identical outputs (same arithmetic)."""
+    import torch
+    from atsc3_b200.ldpc import decode_flood, plan_for
+    from atsc3_b200.learned import WmsCode, inference_weights
+    rate, n, T = "8/15", 64800, 12
+    lam, cw = _case(seed=17, nb=5)
+    code = WmsCode(rate, n)
+    rng = np.random.default_rng(8)
+    a = torch.tensor(0.7 + 0.25 * rng.random((T, code.nbucket)), dtype=torch.float32, device="cuda")
+    b = torch.tensor(0.15 * rng.random((T, code.nbucket)), dtype=torch.float32, device="cuda")
+    w = inference_weights(a, b, code.buckets)
+    x = torch.from_numpy(lam).cuda()
+    o1 = decode_flood(plan_for(rate, n, kind="qce"), x, iters=40, weights=w)
+    o2 = decode_flood(plan_for(rate, n, kind="qc"), x, iters=40, weights=w)
+    for k in ("bits", "conv", "its", "bad"):
+        assert torch.equal(o1[k], o2[k]), k

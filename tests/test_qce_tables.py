@@ -1,0 +1,129 @@
+"""The edge-buffer quasi-cyclic decoder's descriptors, expanded on the CPU with
+the kernel's own index formulas (csrc/ldpc_qce.cu), must reproduce the CSR
+tables exactly: every check's columns in position order, every bit's checks
+in the reference summation order (vedge), each edge owning exactly one slot
+entry, and every slot inside its owner's shared memory."""
+import numpy as np
+import pytest
+
+from atsc3_b200 import codes as C
+from atsc3_b200 import native as N
+
+QZ = 360
+WRAP = 1 << 8
+SLOT = QZ * 4
+
+
+def qce_tables(rate, n, cluster):
+    typ, K, M1, M2, Q1, Q = C.ldpc_params(rate, n)
+    rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows(rate, n)]
+    meta = np.zeros(48, np.int32)
+    args = [n, K, Q, rowptr.ctypes.data, addr.ctypes.data, cluster]
+    N.call("atsc3_ldpc_qce_tables_host", *args, meta.ctypes.data, None, None,
+           None, None)
+    nb = n // QZ
+    rdesc = np.zeros((meta[0], 4), np.int32)
+    rptr = np.zeros(Q + 1, np.int32)
+    cdesc = np.zeros((nb, 4), np.int32)
+    s0 = np.zeros(nb * QZ, np.uint8)
+    N.call("atsc3_ldpc_qce_tables_host", *args, meta.ctypes.data,
+           rdesc.ctypes.data, rptr.ctypes.data, cdesc.ctypes.data,
+           s0.ctypes.data)
+    return K, Q, meta, rdesc, rptr, cdesc, s0
+
+
+@pytest.mark.parametrize("rate,n,cluster", [("6/15", 64800, 8), ("10/15", 64800, 8),
+                                            ("13/15", 64800, 16), ("8/15", 64800, 4),
+                                            ("11/15", 16200, 2), ("7/15", 16200, 1)])
+def test_qce_descriptors_reproduce_csr(rate, n, cluster):
+    K, Q, meta, rdesc, rptr, cdesc, s0 = qce_tables(rate, n, cluster)
+    ccp, cidx, vptr, vedge = C.csr(rate, n)
+    nb = n // QZ
+    smem, part_off, maxs = meta[2], meta[3], meta[6]
+    cb = meta[25:25 + cluster + 1]
+    rb = meta[8:8 + cluster + 1]
+    assert cb[0] == 0 and cb[-1] == nb and (np.diff(cb) >= 0).all()
+    assert rb[0] == 0 and rb[-1] == Q
+    buf_off = part_off + 256
+    assert part_off >= nb * 12 * 4 and smem == buf_off + maxs * SLOT
+    owner = np.searchsorted(cb, np.arange(nb), side="right") - 1
+    # column descriptors: slots contiguous from buf_off in every owner
+    for c in range(cluster):
+        off = buf_off
+        for g in range(cb[c], cb[c + 1]):
+            d, base, wrap, own = cdesc[g]
+            assert own == c and base == off
+            off += d * SLOT
+        assert off <= smem
+    # (owner, byte offset) -> (column, slot index), to decode row slots
+    slot_of = {}
+    for g in range(nb):
+        d, base, wrap, own = cdesc[g]
+        for i in range(d):
+            slot_of[(own, base + i * SLOT)] = (g, i)
+    chk = np.repeat(np.arange(len(ccp) - 1), np.diff(ccp))
+    pos = np.arange(len(cidx)) - ccp[chk]
+    seen = {}
+    # check side: columns in position order, one slot entry per edge
+    for r in range(Q):
+        for k in list(range(0, QZ, 7)) + [1, QZ - 1]:
+            cols = []
+            for j, (x, off, u, bmo) in enumerate(rdesc[rptr[r]:rptr[r + 1]]):
+                assert (x >> 16) == j
+                if (x & WRAP) and k == 0:
+                    continue
+                g, i = slot_of[(x & 0xFF, off)]
+                assert bmo == g * 12 * 4
+                mm = (k - u) % QZ
+                cols.append(g * QZ + mm)
+                key = (g, i, mm)
+                assert key not in seen
+                seen[key] = (Q * k + r, j)
+            a = Q * k + r
+            assert cols == cidx[ccp[a]:ccp[a + 1]].tolist(), (r, k)
+    # variable side: rotated slot order = vedge order, and the slot entry
+    # read for each (check, position) is the one that check writes
+    for lam in list(range(0, n, 53)) + [n - 1, n - 2, K, K - 1]:
+        g, mm = divmod(lam, QZ)
+        d, base, wrap, own = cdesc[g]
+        got = []
+        for t in range(d):
+            i = s0[g * QZ + mm] + t
+            i = i - d if i >= d else i
+            if i == wrap and mm == QZ - 1:
+                continue
+            if (g, i, mm) in seen:
+                got.append(seen[(g, i, mm)])
+            else:
+                got.append(("unvisited", g, i, mm))
+        want = [(int(chk[e]), int(pos[e])) for e in vedge[vptr[lam]:vptr[lam + 1]]]
+        sampled = [w for w in want if (w[0] % Q, w[0] // Q) and
+                   (w[0] // Q) in set(range(0, QZ, 7)) | {1, QZ - 1}]
+        got_s = [x for x in got if x[0] != "unvisited"]
+        assert got_s == sampled, lam
+        assert len(got) == len(want), lam
+
+
+def test_qce_rejects_shared_blocks_and_bad_cluster():
+    typ, K, M1, M2, Q1, Q = C.ldpc_params("6/15", 16200)
+    rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows("6/15", 16200)]
+    meta = np.zeros(48, np.int32)
+    f = N.lib().atsc3_ldpc_qce_tables_host
+    assert f(16200, K, Q, rowptr.ctypes.data, addr.ctypes.data, 2,
+             meta.ctypes.data, None, None, None, None) == -4
+    typ, K, M1, M2, Q1, Q = C.ldpc_params("10/15", 64800)
+    rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows("10/15", 64800)]
+    assert f(64800, K, Q, rowptr.ctypes.data, addr.ctypes.data, 3,
+             meta.ctypes.data, None, None, None, None) == -3
+
+
+def test_qce_shared_memory_fits_b200_at_cluster_8():
+    """Every 64800 Type B code fits an 8-CTA cluster within the 227 KB
+    opt-in limit; every 16200 code the decoder accepts (7/15, 9/15, 11/15:
+    the others put two circulants in one block) fits 2 CTAs."""
+    for num in (6, 8, 9, 10, 11, 12, 13):
+        meta = qce_tables(f"{num}/15", 64800, 8)[2]
+        assert meta[2] <= 232448, (num, meta[2])
+    for num in (7, 9, 11):
+        meta = qce_tables(f"{num}/15", 16200, 2)[2]
+        assert meta[2] <= 232448, (num, meta[2])

@@ -35,7 +35,11 @@ def _noalloc(torch, p, cells, s2):
            "bad": torch.empty(nblk, dtype=torch.int32, device=dev),
            "syn": torch.empty((nblk, 6), dtype=torch.int32, device=dev),
            "ok": torch.empty(nblk, dtype=torch.uint8, device=dev)}
-    kind = 1 if getattr(p.plan, "kind", "csr") == "qc" else 0
+    # the entry point takes CSR (0) and record-layout quasi-cyclic (1) plans
+    kinds = {"csr": 0, "qc": 1}
+    plan_kind = getattr(p.plan, "kind", "csr")
+    assert plan_kind in kinds, f"no-alloc entry point has no {plan_kind} plans"
+    kind = kinds[plan_kind]
     N.call("atsc3_fec_decode_noalloc", p.plan.handle, kind, zf.data_ptr(),
            zf.stride(0) // 2, nblk, ncell,
            DM.device_points(p.mod, p.rate, dev).data_ptr(), p.nb, mode,
@@ -51,6 +55,12 @@ def _noalloc(torch, p, cells, s2):
     return {k: v.cpu().numpy() for k, v in out.items()}
 
 
+def _kind(c):
+    """Record-layout quasi-cyclic plan for Type B codes, else CSR."""
+    from atsc3_b200 import codes as C
+    return "qc" if C.ldpc_params(c["rate"], c["n"])[0] == "B" else "csr"
+
+
 def test_noalloc_matches_regular_path_twice():
     import torch
     from atsc3_b200.pipeline import FecPipeline
@@ -58,7 +68,8 @@ def test_noalloc_matches_regular_path_twice():
     # second call reuses the scratch the first one left behind
     for name in ("c64_16qam_6_15_ray", "c64_64qam_7_15", "c64_16qam_6_15_ray"):
         c, pay, cw, cells, s2, q, lam = oracle_case(name)
-        p = FecPipeline(c["n"], c["mod"], c["rate"], iters=50, alpha=0.75)
+        p = FecPipeline(c["n"], c["mod"], c["rate"], iters=50, alpha=0.75,
+                        kind=_kind(c))
         s2d = float(s2) if np.ndim(s2) == 0 else \
             torch.from_numpy(np.ascontiguousarray(s2, np.float32)).cuda()
         ws = p.decode(torch.from_numpy(cells).cuda(), s2d)
@@ -74,7 +85,7 @@ def test_noalloc_rejects_oversize_batch():
     import torch
     from atsc3_b200 import native as N
     from atsc3_b200.pipeline import FecPipeline
-    p = FecPipeline(64800, "16QAM", "6/15")
+    p = FecPipeline(64800, "16QAM", "6/15", kind="qc")
     cells = np.zeros((17, p.ncell), np.complex64)
     with pytest.raises(N.FecError) as e:
         _noalloc(torch, p, cells, 1.0)
