@@ -61,8 +61,9 @@ struct QcePlan {
   int dr_max = 0, dc_max = 0, max_slots = 0, device = 0;
   int64_t table_bytes = 0;
   int rb[EMAXCL + 1] = {0};     // block rows of CTA c (check phase)
-  int cb[EMAXCL + 1] = {0};     // columns of CTA c (variable phase, slots)
+  int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
+  int32_t *d_ccols = nullptr;   // (nb) columns grouped by owner CTA
   int32_t *d_rptr = nullptr;    // (Q+1)
   int4 *d_cdesc = nullptr;      // per column
   uint8_t *d_s0 = nullptr;      // (nb*360) rotation start
@@ -75,11 +76,12 @@ struct QcePlan {
 // Column descriptor (column g): x = slots d, y = byte offset of slot 0 in
 // the owner's shared memory (slots follow at 1440-byte steps, sorted by
 // (u, row)), z = index of the dual-diagonal wrap slot (absent for bit 359)
-// or -1, w = owner CTA.
+// or -1, w = owner CTA.  ccols lists each CTA's columns (cb[c] .. cb[c+1]).
 struct QceTables {
   std::vector<int4> rdesc;
   std::vector<int32_t> rptr;
   std::vector<int4> cdesc;
+  std::vector<int32_t> ccols;
   std::vector<uint8_t> s0;
 };
 
@@ -89,8 +91,8 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     set_error("invalid argument: not a 360-circulant Type B code");
     return -3;
   }
-  if (cluster < 1 || cluster > EMAXCL || (cluster & (cluster - 1))) {
-    set_error("invalid argument: cluster must be 1, 2, 4, 8 or 16");
+  if (cluster < 1 || cluster > EMAXCL) {
+    set_error("invalid argument: cluster must be in 1..16");
     return -3;
   }
   const int nbi = K / EZ, nb = n / EZ;
@@ -148,17 +150,30 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     dcm = std::max(dcm, (int)Cc.size());
     total += (int)Cc.size();
   }
-  // columns split over the cluster in contiguous runs of about equal slots
-  p->cb[0] = 0;
-  {
-    int acc = 0, c = 1;
-    for (int g = 0; g < nb && c < cluster; ++g) {
-      acc += (int)cols[g].size();
-      while (c < cluster && (int64_t)acc * cluster >= (int64_t)total * c)
-        p->cb[c++] = g + 1;
-    }
-    while (c <= cluster) p->cb[c++] = nb;
+  // columns assigned to the cluster's CTAs by longest-processing-time
+  // greedy on their slot counts (largest column first, to the CTA holding
+  // the fewest slots): the per-CTA slot totals differ by at most one column
+  std::vector<int> order(nb), load(cluster, 0), who(nb);
+  for (int g = 0; g < nb; ++g) order[g] = g;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return cols[x].size() > cols[y].size();
+  });
+  for (int g : order) {
+    int c = 0;
+    for (int q = 1; q < cluster; ++q)
+      if (load[q] < load[c]) c = q;
+    who[g] = c;
+    load[c] += (int)cols[g].size();
   }
+  t->ccols.clear();
+  p->cb[0] = 0;
+  for (int c = 0; c < cluster; ++c) {
+    for (int g = 0; g < nb; ++g)
+      if (who[g] == c) t->ccols.push_back(g);
+    p->cb[c + 1] = (int)t->ccols.size();
+  }
+  for (int c = cluster + 1; c <= EMAXCL; ++c) p->cb[c] = nb;
+  (void)total;
   const int per = (Q + cluster - 1) / cluster;
   for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
   const int bm_bytes = (nb * ECHUNK * 4 + 15) & ~15;
@@ -168,7 +183,8 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   int maxs = 0;
   for (int c = 0; c < cluster; ++c) {
     int s = 0;
-    for (int g = p->cb[c]; g < p->cb[c + 1]; ++g) {
+    for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) {
+      const int g = t->ccols[q];
       owner[g] = c;
       base[g] = buf_off + s * ESLOT;
       s += (int)cols[g].size();
@@ -216,6 +232,7 @@ struct QceArgs {
   int part_off;
   int rb[EMAXCL + 1];
   int cb[EMAXCL + 1];
+  const int32_t *ccols;
   const int4 *rdesc;
   const int32_t *rptr;
   const int4 *cdesc;
@@ -254,7 +271,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
   const int r0 = a.rb[rank], r1 = a.rb[rank + 1];
-  const int c0 = a.cb[rank], c1 = a.cb[rank + 1];
+  const int c0 = a.cb[rank], c1 = a.cb[rank + 1];   // into ccols
   const int ncitems = (r1 - r0) * ECHUNK;
   const int nvitems = (c1 - c0) * ECHUNK;
   const uint32_t dummy = sm_sa;                       // own, always mapped
@@ -267,7 +284,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
     for (int w = warp; w < nvitems; w += nwarps) {
       const int gl = w / ECHUNK;
       const int ch = w - gl * ECHUNK;
-      const int g = c0 + gl;
+      const int g = __ldg(a.ccols + c0 + gl);
       const int mm0 = ch * 32 + lane;
       const bool mv = mm0 < EZ;
       const int mm = mv ? mm0 : EZ - 1;
@@ -377,10 +394,14 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       if (tid == 0) *sbad = 0;
       const bool done = (badct == 0) && (!TORCH || it > 0);
       if (done || it >= a.iters) {
-        // outputs of this CTA's columns from its bitmap replica
+        // outputs from this CTA's bitmap replica (complete in every CTA):
+        // CTA `rank` writes its share of the codeword's bytes / bits
+        const int nby = a.n >> 3;
+        const int by0 = (int)((int64_t)nby * rank / CL);
+        const int by1 = (int)((int64_t)nby * (rank + 1) / CL);
         if (a.hard) {
           uint8_t *ho = a.hard + (size_t)b * a.ld_hard;
-          for (int by = c0 * 45 + tid; by < c1 * 45; by += blockDim.x) {
+          for (int by = by0 + tid; by < by1; by += blockDim.x) {
             const int g = by / 45;
             const int bb = (by - g * 45) * 8;
             const uint32_t v = (bm[g * ECHUNK + (bb >> 5)] >> (bb & 31)) & 0xFFu;
@@ -389,7 +410,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         }
         if (a.bits) {
           uint8_t *bo = a.bits + (size_t)b * a.ld_bits;
-          for (int i = c0 * EZ + tid; i < c1 * EZ; i += blockDim.x) {
+          for (int i = by0 * 8 + tid; i < by1 * 8; i += blockDim.x) {
             const int g = i / EZ;
             const int mm = i - g * EZ;
             bo[i] = (uint8_t)((bm[g * ECHUNK + (mm >> 5)] >> (mm & 31)) & 1u);
@@ -410,7 +431,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       for (int w = warp; w < nvitems; w += nwarps) {
         const int gl = w / ECHUNK;
         const int ch = w - gl * ECHUNK;
-        const int g = c0 + gl;
+        const int g = __ldg(a.ccols + c0 + gl);
         const int mm0 = ch * 32 + lane;
         const bool mv = mm0 < EZ;
         const int mm = mv ? mm0 : EZ - 1;
@@ -583,7 +604,7 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
     // smallest cluster whose per-CTA shared memory fits; a structural
     // rejection (-3, -4 from the build) ends the search with its message
     bool fits = false;
-    for (int cl = 1; cl <= EMAXCL; cl <<= 1) {
+    for (int cl = 1; cl <= EMAXCL; ++cl) {
       rc = qce_build(n, kldpc, qldpc, rowptr, addr, cl, &h->p, &t);
       if (rc) break;
       if (h->p.smem <= smax) {
@@ -616,6 +637,7 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
   cudaError_t e = up((void **)&h->p.d_rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_rptr, t.rptr.data(), t.rptr.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_cdesc, t.cdesc.data(), t.cdesc.size() * 16);
+  if (e == cudaSuccess) e = up((void **)&h->p.d_ccols, t.ccols.data(), t.ccols.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
   if (e != cudaSuccess) {
     atsc3_ldpc_qce_plan_destroy(h);
@@ -630,6 +652,7 @@ void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
   cudaFree(h->p.d_rdesc);
   cudaFree(h->p.d_rptr);
   cudaFree(h->p.d_cdesc);
+  cudaFree(h->p.d_ccols);
   cudaFree(h->p.d_s0);
   delete h;
 }
@@ -645,7 +668,7 @@ int32_t atsc3_ldpc_qce_plan_info(const atsc3_ldpc_qce_plan *h, int64_t *info) {
   info[6] = h->p.dc_max;
   info[7] = h->p.table_bytes;
   info[8] = h->p.max_slots;
-  info[9] = h->p.cb[1] - h->p.cb[0];
+  info[9] = h->p.cb[1] - h->p.cb[0];   // columns of CTA 0
   return 0;
 }
 
@@ -653,7 +676,8 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
                                    const int32_t *rowptr, const int32_t *addr,
                                    int32_t cluster, int32_t *meta,
                                    int32_t *rdesc, int32_t *rptr,
-                                   int32_t *cdesc, uint8_t *s0) {
+                                   int32_t *cdesc, int32_t *ccols,
+                                   uint8_t *s0) {
   using namespace atsc3;
   ATSC3_ARG(meta && rowptr && addr, "null argument");
   QcePlan p;
@@ -674,6 +698,7 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
   if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
+  if (ccols) std::memcpy(ccols, t.ccols.data(), t.ccols.size() * 4);
   if (s0) std::memcpy(s0, t.s0.data(), t.s0.size());
   return 0;
 }
@@ -742,6 +767,7 @@ int32_t atsc3_ldpc_qce_decode_weighted(
     a.rb[c] = p.rb[c];
     a.cb[c] = p.cb[c];
   }
+  a.ccols = p.d_ccols;
   a.rdesc = p.d_rdesc;
   a.rptr = p.d_rptr;
   a.cdesc = p.d_cdesc;

@@ -58,7 +58,7 @@ SIGNATURES = {
     "atsc3_ldpc_qce_plan_info": (c_i32, [c_vp, c_vp]),
     "atsc3_ldpc_qce_tables_host": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp,
                                            c_i32, c_vp, c_vp, c_vp, c_vp,
-                                           c_vp]),
+                                           c_vp, c_vp]),
     "atsc3_ldpc_qce_config": (c_i32, [c_vp, c_i32, c_i32, c_vp]),
     "atsc3_ldpc_qce_decode": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32, c_f32,
                                       c_i32, c_vp, c_i64, c_vp, c_i64, c_vp,

@@ -184,9 +184,10 @@ int32_t atsc3_ldpc_qc_decode_weighted(
  * (csrc/ldpc_qce.cu): one float32 slot per edge, owned by the edge's column,
  * holding the variable-to-check value after the variable phase and the
  * check-to-variable message after the check phase; hard decisions in a
- * bitmap replicated per CTA; no per-check records.  cluster 0 picks the
- * smallest cluster whose per-CTA shared memory fits (8 for the 64800-bit
- * codes, 2 for the 16200-bit ones). */
+ * bitmap replicated per CTA; no per-check records.  cluster: any size in
+ * 1..16 (not only powers of two); 0 picks the smallest cluster whose per-CTA
+ * shared memory fits (6 for the 64800-bit codes, 2 for the 16200-bit
+ * ones). */
 typedef struct atsc3_ldpc_qce_plan atsc3_ldpc_qce_plan;
 
 int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
@@ -203,15 +204,17 @@ int32_t atsc3_ldpc_qce_plan_info(const atsc3_ldpc_qce_plan *plan, int64_t *info)
  * ints): [0] row slots [1] 360-bit columns [2] shared bytes per CTA [3]
  * byte offset of the syndrome exchange words [4] max row degree [5] max
  * column degree [6] most slots per CTA [8..24] block-row split [25..41]
- * column split.  rdesc: int4 per row slot (owner | wrap<<8 | position<<16,
- * slot byte offset in the owner, shift, bitmap byte offset of the column);
- * cdesc: int4 per column (slots, byte offset of slot 0, wrap slot or -1,
- * owner).  Array outputs may be null. */
+ * CTA c owns columns ccols[meta[25+c] .. meta[26+c]).  rdesc: int4 per row
+ * slot (owner | wrap<<8 | position<<16, slot byte offset in the owner,
+ * shift, bitmap byte offset of the column); cdesc: int4 per column (slots,
+ * byte offset of slot 0, wrap slot or -1, owner); ccols: the nb columns
+ * grouped by owner.  Array outputs may be null. */
 int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
                                    const int32_t *rowptr, const int32_t *addr,
                                    int32_t cluster, int32_t *meta,
                                    int32_t *rdesc, int32_t *rptr,
-                                   int32_t *cdesc, uint8_t *s0);
+                                   int32_t *cdesc, int32_t *ccols,
+                                   uint8_t *s0);
 
 /* out[0] = clusters resident at once, [1] = CTAs per cluster, [2] = shared
  * bytes per CTA, [3] = threads per CTA (threads 0 = the default). */

@@ -20,23 +20,25 @@ def qce_tables(rate, n, cluster):
     meta = np.zeros(48, np.int32)
     args = [n, K, Q, rowptr.ctypes.data, addr.ctypes.data, cluster]
     N.call("atsc3_ldpc_qce_tables_host", *args, meta.ctypes.data, None, None,
-           None, None)
+           None, None, None)
     nb = n // QZ
     rdesc = np.zeros((meta[0], 4), np.int32)
     rptr = np.zeros(Q + 1, np.int32)
     cdesc = np.zeros((nb, 4), np.int32)
+    ccols = np.zeros(nb, np.int32)
     s0 = np.zeros(nb * QZ, np.uint8)
     N.call("atsc3_ldpc_qce_tables_host", *args, meta.ctypes.data,
            rdesc.ctypes.data, rptr.ctypes.data, cdesc.ctypes.data,
-           s0.ctypes.data)
-    return K, Q, meta, rdesc, rptr, cdesc, s0
+           ccols.ctypes.data, s0.ctypes.data)
+    return K, Q, meta, rdesc, rptr, cdesc, ccols, s0
 
 
 @pytest.mark.parametrize("rate,n,cluster", [("6/15", 64800, 8), ("10/15", 64800, 8),
+                                            ("6/15", 64800, 6), ("12/15", 64800, 7),
                                             ("13/15", 64800, 16), ("8/15", 64800, 4),
                                             ("11/15", 16200, 2), ("7/15", 16200, 1)])
 def test_qce_descriptors_reproduce_csr(rate, n, cluster):
-    K, Q, meta, rdesc, rptr, cdesc, s0 = qce_tables(rate, n, cluster)
+    K, Q, meta, rdesc, rptr, cdesc, ccols, s0 = qce_tables(rate, n, cluster)
     ccp, cidx, vptr, vedge = C.csr(rate, n)
     nb = n // QZ
     smem, part_off, maxs = meta[2], meta[3], meta[6]
@@ -44,13 +46,16 @@ def test_qce_descriptors_reproduce_csr(rate, n, cluster):
     rb = meta[8:8 + cluster + 1]
     assert cb[0] == 0 and cb[-1] == nb and (np.diff(cb) >= 0).all()
     assert rb[0] == 0 and rb[-1] == Q
+    assert sorted(ccols.tolist()) == list(range(nb))
     buf_off = part_off + 256
     assert part_off >= nb * 12 * 4 and smem == buf_off + maxs * SLOT
-    owner = np.searchsorted(cb, np.arange(nb), side="right") - 1
+    # slot totals per CTA differ by at most one column's slots
+    tot = [int(cdesc[ccols[cb[c]:cb[c + 1]], 0].sum()) for c in range(cluster)]
+    assert max(tot) == maxs and max(tot) - min(tot) <= cdesc[:, 0].max()
     # column descriptors: slots contiguous from buf_off in every owner
     for c in range(cluster):
         off = buf_off
-        for g in range(cb[c], cb[c + 1]):
+        for g in ccols[cb[c]:cb[c + 1]]:
             d, base, wrap, own = cdesc[g]
             assert own == c and base == off
             off += d * SLOT
@@ -110,19 +115,19 @@ def test_qce_rejects_shared_blocks_and_bad_cluster():
     meta = np.zeros(48, np.int32)
     f = N.lib().atsc3_ldpc_qce_tables_host
     assert f(16200, K, Q, rowptr.ctypes.data, addr.ctypes.data, 2,
-             meta.ctypes.data, None, None, None, None) == -4
+             meta.ctypes.data, None, None, None, None, None) == -4
     typ, K, M1, M2, Q1, Q = C.ldpc_params("10/15", 64800)
     rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows("10/15", 64800)]
-    assert f(64800, K, Q, rowptr.ctypes.data, addr.ctypes.data, 3,
-             meta.ctypes.data, None, None, None, None) == -3
+    assert f(64800, K, Q, rowptr.ctypes.data, addr.ctypes.data, 17,
+             meta.ctypes.data, None, None, None, None, None) == -3
 
 
-def test_qce_shared_memory_fits_b200_at_cluster_8():
-    """Every 64800 Type B code fits an 8-CTA cluster within the 227 KB
+def test_qce_shared_memory_fits_b200_at_cluster_6():
+    """Every 64800 Type B code fits a 6-CTA cluster within the 227 KB
     opt-in limit; every 16200 code the decoder accepts (7/15, 9/15, 11/15:
     the others put two circulants in one block) fits 2 CTAs."""
     for num in (6, 8, 9, 10, 11, 12, 13):
-        meta = qce_tables(f"{num}/15", 64800, 8)[2]
+        meta = qce_tables(f"{num}/15", 64800, 6)[2]
         assert meta[2] <= 232448, (num, meta[2])
     for num in (7, 9, 11):
         meta = qce_tables(f"{num}/15", 16200, 2)[2]
