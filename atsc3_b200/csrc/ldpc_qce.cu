@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -55,9 +56,17 @@ constexpr int EWRAP = 1 << 8;
 constexpr int ESLOT = EZ * 4;             // bytes of one circulant slot
 constexpr int EPART = 256;                // syndrome exchange bytes
 
+// Compile-time slot counts per block row (NS >= the code's largest block-row
+// degree; rows with fewer edges mask the rest) (the kernel templates).
+__host__ __device__ constexpr int qce_ns(int dr) {
+  return dr <= 8 ? 8 : dr <= 10 ? 10 : dr <= 11 ? 11 : dr <= 14 ? 14
+       : dr <= 17 ? 17 : dr <= 22 ? 22 : dr <= 33 ? 33 : dr <= 56 ? 56 : 0;
+}
+
 struct QcePlan {
   int n = 0, K = 0, Q = 0, nb = 0;
-  int cluster = 1, smem = 0, part_off = 0;
+  int cluster = 1, smem = 0, part_off = 0, rt_off = 0, ri_off = 0, ct_off = 0;
+  int buf_off = 0;
   int dr_max = 0, dc_max = 0, max_slots = 0, device = 0;
   int64_t table_bytes = 0;
   int rb[EMAXCL + 1] = {0};     // block rows of CTA c (check phase)
@@ -176,9 +185,17 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   (void)total;
   const int per = (Q + cluster - 1) / cluster;
   for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
+  // shared memory: bitmap | syndrome exchange | row-slot table (per row,
+  // chunk and slot, 8 B) | row masks | column table (16 B per column) | slots
+  int maxcols = 0;
+  for (int c = 0; c < cluster; ++c) maxcols = std::max(maxcols, p->cb[c + 1] - p->cb[c]);
+  const int ns = qce_ns(drm);
   const int bm_bytes = (nb * ECHUNK * 4 + 15) & ~15;
   const int part_off = bm_bytes;
-  const int buf_off = bm_bytes + EPART;
+  const int rt_off = part_off + EPART;
+  const int ri_off = rt_off + per * ECHUNK * ns * 8;
+  const int ct_off = ri_off + ((per * 2 * (ns > 32 ? 8 : 4) + 15) & ~15);
+  const int buf_off = ct_off + maxcols * 16;
   std::vector<int> owner(nb), base(nb);
   int maxs = 0;
   for (int c = 0; c < cluster; ++c) {
@@ -197,6 +214,10 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   p->dc_max = dcm;
   p->max_slots = maxs;
   p->part_off = part_off;
+  p->rt_off = rt_off;
+  p->ri_off = ri_off;
+  p->ct_off = ct_off;
+  p->buf_off = buf_off;
   p->smem = buf_off + maxs * ESLOT;
   t->rptr.assign(Q + 1, 0);
   t->rdesc.clear();
@@ -229,7 +250,9 @@ struct QceArgs {
   int64_t ld_llr;
   int nblk, n, iters;
   float alpha;
-  int part_off;
+  // shared-memory layout (byte offsets): syndrome exchange words, per-chunk
+  // row-slot table, per-row masks, column table; the bitmap sits at 0
+  int part_off, rt_off, ri_off, ct_off;
   int rb[EMAXCL + 1];
   int cb[EMAXCL + 1];
   const int32_t *ccols;
@@ -253,30 +276,134 @@ struct QceArgs {
   int32_t *bad;
 };
 
-// NCH: chunks of 8 edge positions per block row (compile-time positions);
-// MASK: per-check bit-mask type (>= NCH*8 bits); NT: threads per CTA.
-template <bool TORCH, int NCH, typename MASK, int NT>
+
+// Variable phase of one bit for a column of exactly D edges: the D slot
+// entries are loaded in storage order, the sum is formed in the reference
+// order (slots s0 .. D-1, then 0 .. s0-1) by selecting the rotated value for
+// each position, and every slot is rewritten as tot - m.
+template <bool TORCH, int D>
+__device__ __forceinline__ float qce_var_exact(float *col, int s0, float li,
+                                               bool mv) {
+  float m[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) m[i] = col[i * EZ];
+  const int s = s0 >= D ? s0 - D : s0;
+  float acc = TORCH ? li : 0.f;
+#pragma unroll
+  for (int t = 0; t < D; ++t) {
+    float v = m[t];
+#pragma unroll
+    for (int c = 1; c < D; ++c) v = (s == c) ? m[(c + t) % D] : v;
+    acc = __fadd_rn(acc, v);
+  }
+  const float tot = TORCH ? acc : __fadd_rn(li, acc);
+  if (mv) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) col[i * EZ] = __fsub_rn(tot, m[i]);
+  }
+  return tot;
+}
+
+// Variable phase of one bit for a column of d edges (any d >= 1): byte
+// offsets walk the slots from s0 with a wrap at d (unsigned min trick:
+// off - span underflows while off < span).
+template <bool TORCH>
+__device__ __forceinline__ float qce_var_generic(float *col, int d, int s0,
+                                                 float li, bool mv) {
+  const char *cb = reinterpret_cast<const char *>(col);
+  const uint32_t span = (uint32_t)d * (uint32_t)ESLOT;
+  uint32_t off = (uint32_t)(s0 < d ? s0 : 0) * (uint32_t)ESLOT;
+  float acc = TORCH ? li : 0.f;
+  int t = 0;
+  for (; t + 4 <= d; t += 4) {
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      v[u] = *reinterpret_cast<const float *>(cb + off);
+      off += ESLOT;
+      off = min(off, off - span);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc = __fadd_rn(acc, v[u]);
+  }
+  for (; t < d; ++t) {
+    acc = __fadd_rn(acc, *reinterpret_cast<const float *>(cb + off));
+    off += ESLOT;
+    off = min(off, off - span);
+  }
+  const float tot = TORCH ? acc : __fadd_rn(li, acc);
+  if (mv) {
+    int i = 0;
+    for (; i + 4 <= d; i += 4) {
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = col[(i + u) * EZ];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) col[(i + u) * EZ] = __fsub_rn(tot, v[u]);
+    }
+    for (; i < d; ++i) col[i * EZ] = __fsub_rn(tot, col[i * EZ]);
+  }
+  return tot;
+}
+
+// NS: compile-time slots per block row (qce_ns); NT: threads per CTA.
+template <bool TORCH, int NS, int NT>
 __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
-  constexpr int NS = NCH * 8;
-  constexpr int VB = 4;                               // variable-phase loads in flight
-  constexpr int MB = (int)sizeof(MASK) * 8;
+  using MASK = typename std::conditional<(NS > 32), unsigned long long,
+                                         uint32_t>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   const int rank = (int)cluster_ctarank();
   const int CL = (int)cluster_nctarank();
   const uint32_t *bm = reinterpret_cast<const uint32_t *>(smem);
   int *part = reinterpret_cast<int *>(smem + a.part_off);
   int *sbad = part + 32;
+  uint2 *rtab = reinterpret_cast<uint2 *>(smem + a.rt_off);
+  MASK *rinfo = reinterpret_cast<MASK *>(smem + a.ri_off);
+  int4 *ctab = reinterpret_cast<int4 *>(smem + a.ct_off);
   const uint32_t sm_sa = smem_u32(smem);
   const uint32_t part_sa = smem_u32(part);
+  const uint32_t dummy = part_sa + 40 * 4;   // junk word for masked slots
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  const int r0 = a.rb[rank], r1 = a.rb[rank + 1];
-  const int c0 = a.cb[rank], c1 = a.cb[rank + 1];   // into ccols
-  const int ncitems = (r1 - r0) * ECHUNK;
-  const int nvitems = (c1 - c0) * ECHUNK;
-  const uint32_t dummy = sm_sa;                       // own, always mapped
+  const int r0 = a.rb[rank], nr = a.rb[rank + 1] - r0;
+  const int c0 = a.cb[rank], ncol = a.cb[rank + 1] - c0;   // into ccols
+  const int ncitems = nr * ECHUNK;
+  const int nvitems = ncol * ECHUNK;
 
+  // ---- per-launch tables ---------------------------------------------------
+  // row slot (rl, chunk, j): {shared::cluster address of the slot block in
+  // its owner, (first entry index b = (32*chunk - u) mod 360) << 16 | bitmap
+  // word index of the column}; slots past the row degree repeat the last one
+  for (int e = tid; e < nr * NS; e += blockDim.x) {
+    const int rl = e / NS;
+    const int j = e - rl * NS;
+    const int rp = __ldg(a.rptr + r0 + rl);
+    const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
+    const int4 d = __ldg(a.rdesc + rp + min(j, deg - 1));
+    const uint32_t base = dsmem_map(sm_sa + (uint32_t)d.y, (uint32_t)(d.x & 0xFF));
+    const uint32_t wb = (uint32_t)d.w >> 2;
+#pragma unroll 1
+    for (int ch = 0; ch < ECHUNK; ++ch) {
+      int bb = ch * 32 - d.z;
+      bb += bb < 0 ? EZ : 0;
+      rtab[(rl * ECHUNK + ch) * NS + j] = make_uint2(base, ((uint32_t)bb << 16) | wb);
+    }
+    if (j == 0) {
+      MASK wm = 0;
+      for (int q = 0; q < deg; ++q)
+        if (__ldg(a.rdesc + rp + q).x & EWRAP) wm |= (MASK)1 << q;
+      rinfo[2 * rl] = deg >= (int)(8 * sizeof(MASK)) ? ~(MASK)0
+                                                      : (((MASK)1 << deg) - 1);
+      rinfo[2 * rl + 1] = wm;
+    }
+  }
+  for (int q = tid; q < ncol; q += blockDim.x) {
+    const int g = __ldg(a.ccols + c0 + q);
+    const int4 cd = __ldg(a.cdesc + g);
+    ctab[q] = make_int4(cd.x, cd.y, cd.z, g);
+  }
   if (tid == 0) *sbad = 0;
+  __syncthreads();
 
   for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
     const float *lam = a.llr + (size_t)b * a.ld_llr;
@@ -284,18 +411,17 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
     for (int w = warp; w < nvitems; w += nwarps) {
       const int gl = w / ECHUNK;
       const int ch = w - gl * ECHUNK;
-      const int g = __ldg(a.ccols + c0 + gl);
+      const int4 cd = ctab[gl];
       const int mm0 = ch * 32 + lane;
       const bool mv = mm0 < EZ;
       const int mm = mv ? mm0 : EZ - 1;
-      const int4 cd = __ldg(a.cdesc + g);
-      const float li = lam[g * EZ + mm];
+      const float li = lam[cd.w * EZ + mm];
       float *col = reinterpret_cast<float *>(smem + cd.y) + mm;
       if (mv)
         for (int i = 0; i < cd.x; ++i) col[i * EZ] = li;
       const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < 0.f);
       if (lane < CL)
-        dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((g * ECHUNK + ch) * 4),
+        dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((cd.w * ECHUNK + ch) * 4),
                                (uint32_t)lane), hb);
     }
     __syncthreads();
@@ -307,77 +433,65 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       int mybad = 0;
       for (int w = warp; w < ncitems; w += nwarps) {
         const int rl = w / ECHUNK;
-        const int r = r0 + rl;
-        const int k0 = (w - rl * ECHUNK) * 32 + lane;
-        const bool kv = k0 < EZ;
-        const int k = kv ? k0 : EZ - 1;
-        const int rp = __ldg(a.rptr + r);
-        const int deg = __ldg(a.rptr + r + 1) - rp;
-        const int4 *ds = a.rdesc + rp;
+        const int ch = w - rl * ECHUNK;
+        const int k0 = ch * 32 + lane;
+        MASK live = rinfo[2 * rl];
+        if (k0 == 0) live &= ~rinfo[2 * rl + 1];   // check (0, 0): no wrap edge
+        if (k0 >= EZ) live = 0;                    // lanes past the circulant
+        const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
         uint32_t ad[NS];
         uint32_t syn = 0;
-        MASK live = 0;
 #pragma unroll
         for (int j = 0; j < NS; ++j) {
-          const int4 d = __ldg(ds + min(j, deg - 1));
-          const bool on = j < deg && !((d.x & EWRAP) && k == 0);
-          int o = k - d.z;
-          o += o < 0 ? EZ : 0;
-          const uint32_t hw = bm[(d.w >> 2) + (o >> 5)];
+          const uint2 e = te[j];
+          int o = (int)(e.y >> 16) + lane;
+          o -= o >= EZ ? EZ : 0;
+          const bool on = (live >> j) & 1;
+          const uint32_t hw = bm[(e.y & 0xFFFFu) + (uint32_t)(o >> 5)];
           syn ^= on ? (hw >> (o & 31)) & 1u : 0u;
-          ad[j] = on ? dsmem_map(sm_sa + (uint32_t)(d.y + 4 * o), (uint32_t)(d.x & 0xFF))
-                     : dummy;
-          if (on) live |= (MASK)1 << j;
+          ad[j] = on ? e.x + 4u * (uint32_t)o : dummy;
         }
-        mybad += kv ? (int)syn : 0;
+        mybad += (int)syn;
         if (upd) {
+          float t[NS];
+#pragma unroll
+          for (int j = 0; j < NS; ++j) t[j] = dsmem_ld_f32(ad[j]);
           float min1 = __int_as_float(0x7f800000), min2 = min1;
           uint32_t first = 0;
           MASK sv = 0;
 #pragma unroll
-          for (int c = 0; c < NCH; ++c) {
-            float t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = dsmem_ld_f32(ad[c * 8 + u]);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              const int j = c * 8 + u;
-              const MASK bit = (MASK)1 << j;
-              if (live & bit) {
-                if (t[u] < 0.f) sv |= bit;
-                const float mag = fabsf(t[u]);
-                if (mag < min1) { min2 = min1; min1 = mag; first = (uint32_t)j; }
-                else if (mag < min2) { min2 = mag; }
-              }
-            }
+          for (int j = 0; j < NS; ++j) {
+            const bool on = (live >> j) & 1;
+            if (on && t[j] < 0.f) sv |= (MASK)1 << j;
+            const float mag = on ? fabsf(t[j]) : __int_as_float(0x7f800000);
+            const bool lt = mag < min1;
+            min2 = lt ? min1 : fminf(min2, mag);
+            first = lt ? (uint32_t)j : first;
+            min1 = fminf(min1, mag);
           }
           int par;
-          if constexpr (MB > 32) par = __popcll((unsigned long long)sv) & 1;
+          if constexpr (NS > 32) par = __popcll((unsigned long long)sv) & 1;
           else par = __popc((uint32_t)sv) & 1;
-          if (kv) {
-            float wa = a.alpha, wb = 0.f;
-            if (a.walpha) {
-              int nl;
-              if constexpr (MB > 32) nl = __popcll((unsigned long long)live);
-              else nl = __popc((uint32_t)live);
-              const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
-              wa = __ldg(a.walpha + wi);
-              wb = __ldg(a.wbeta + wi);
-            }
-            float A = __fsub_rn(__fmul_rn(min1, wa), wb);
-            float B = __fsub_rn(__fmul_rn(min2, wa), wb);
-            A = A > 0.f ? A : 0.f;
-            B = B > 0.f ? B : 0.f;
-            const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
-            const MASK neg = par ? (sv ^ live) : sv;   // message signs
+          float wa = a.alpha, wb = 0.f;
+          if (a.walpha) {
+            int nl;
+            if constexpr (NS > 32) nl = __popcll((unsigned long long)live);
+            else nl = __popc((uint32_t)live);
+            const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+            wa = __ldg(a.walpha + wi);
+            wb = __ldg(a.wbeta + wi);
+          }
+          float A = __fsub_rn(__fmul_rn(min1, wa), wb);
+          float B = __fsub_rn(__fmul_rn(min2, wa), wb);
+          A = A > 0.f ? A : 0.f;
+          B = B > 0.f ? B : 0.f;
+          const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
+          const MASK neg = par ? (sv ^ live) : sv;   // message signs
+          // masked slots and lanes store to the junk word
 #pragma unroll
-            for (int j = 0; j < NS; ++j) {
-              if (live & ((MASK)1 << j)) {
-                const uint32_t mg = ((uint32_t)j == first) ? ub : ua;
-                const uint32_t s = (uint32_t)(neg >> j) & 1u;
-                dsmem_st_u32(ad[j], mg | (s << 31));
-              }
-            }
+          for (int j = 0; j < NS; ++j) {
+            const uint32_t mg = ((uint32_t)j == first) ? ub : ua;
+            dsmem_st_u32(ad[j], mg | (((uint32_t)(neg >> j) & 1u) << 31));
           }
         }
       }
@@ -431,65 +545,40 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       for (int w = warp; w < nvitems; w += nwarps) {
         const int gl = w / ECHUNK;
         const int ch = w - gl * ECHUNK;
-        const int g = __ldg(a.ccols + c0 + gl);
+        const int4 cd = ctab[gl];                 // {d, slot base, wrap, g}
+        const int d = cd.x;
         const int mm0 = ch * 32 + lane;
         const bool mv = mm0 < EZ;
         const int mm = mv ? mm0 : EZ - 1;
-        const int4 cd = __ldg(a.cdesc + g);
-        const int d = cd.x;
-        const int lamidx = g * EZ + mm;
+        const int lamidx = cd.w * EZ + mm;
         const float li = lam[lamidx];
         const int s0 = __ldg(a.s0 + lamidx);
-        const int skip = (mm == EZ - 1) ? cd.z : -1;   // absent wrap edge
         float *col = reinterpret_cast<float *>(smem + cd.y) + mm;
-        float acc = TORCH ? li : 0.f;
+        float tot;
         if (d == 2) {
-          // dual-diagonal parity column (warp-uniform)
+          // dual-diagonal parity column; its wrap slot is absent for bit 359
+          const int skip = (mm == EZ - 1) ? cd.z : -1;
           const int i0 = s0 >= 2 ? s0 - 2 : s0;
           const int i1 = i0 == 0 ? 1 : 0;
           const float m0 = col[i0 * EZ], m1 = col[i1 * EZ];
+          float acc = TORCH ? li : 0.f;
           if (i0 != skip) acc = __fadd_rn(acc, m0);
           if (i1 != skip) acc = __fadd_rn(acc, m1);
-          const float tot = TORCH ? acc : __fadd_rn(li, acc);
+          tot = TORCH ? acc : __fadd_rn(li, acc);
           if (mv) {
             if (i0 != skip) col[i0 * EZ] = __fsub_rn(tot, m0);
             if (i1 != skip) col[i1 * EZ] = __fsub_rn(tot, m1);
           }
-          const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
-          if (lane < CL)
-            dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((g * ECHUNK + ch) * 4),
-                                   (uint32_t)lane), hb);
-          continue;
-        }
-        for (int t0 = 0; t0 < d; t0 += VB) {
-          float m[VB];
-          bool on[VB];
-#pragma unroll
-          for (int u = 0; u < VB; ++u) {
-            int i = s0 + t0 + u;
-            i -= i >= d ? d : 0;
-            on[u] = (t0 + u < d) && i != skip;
-            i = t0 + u < d ? i : 0;
-            m[u] = col[i * EZ];
-          }
-#pragma unroll
-          for (int u = 0; u < VB; ++u)
-            if (on[u]) acc = __fadd_rn(acc, m[u]);
-        }
-        const float tot = TORCH ? acc : __fadd_rn(li, acc);
-        if (mv) {
-          for (int i0 = 0; i0 < d; i0 += VB) {
-            float m[VB];
-#pragma unroll
-            for (int u = 0; u < VB; ++u) m[u] = col[min(i0 + u, d - 1) * EZ];
-#pragma unroll
-            for (int u = 0; u < VB; ++u)
-              if (i0 + u < d && i0 + u != skip) col[(i0 + u) * EZ] = __fsub_rn(tot, m[u]);
-          }
+        } else if (d == 3) {
+          tot = qce_var_exact<TORCH, 3>(col, s0, li, mv);
+        } else if (d == 4) {
+          tot = qce_var_exact<TORCH, 4>(col, s0, li, mv);
+        } else {
+          tot = qce_var_generic<TORCH>(col, d, s0, li, mv);
         }
         const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
         if (lane < CL)
-          dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((g * ECHUNK + ch) * 4),
+          dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((cd.w * ECHUNK + ch) * 4),
                                  (uint32_t)lane), hb);
       }
       __syncthreads();
@@ -502,27 +591,37 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
 
 typedef void (*QceFn)(const QceArgs);
 
-#define ATSC3_QCE_FN(NCH, MASK)                                             \
-  (nt == 1024 ? (semantics ? ldpc_qce_kernel<true, NCH, MASK, 1024>          \
-                           : ldpc_qce_kernel<false, NCH, MASK, 1024>)        \
-              : (semantics ? ldpc_qce_kernel<true, NCH, MASK, 512>           \
-                           : ldpc_qce_kernel<false, NCH, MASK, 512>))
-
-// > 512 threads -> the 1024-thread build (64 registers), else 512 (128).
-static QceFn qce_fn(int semantics, int dr, int threads) {
-  const int nt = threads > 512 ? 1024 : 512;
-  if (dr <= 8) return ATSC3_QCE_FN(1, uint32_t);
-  if (dr <= 16) return ATSC3_QCE_FN(2, uint32_t);
-  if (dr <= 24) return ATSC3_QCE_FN(3, uint32_t);
-  if (dr <= 32) return ATSC3_QCE_FN(4, uint32_t);
-  if (dr <= 40) return ATSC3_QCE_FN(5, unsigned long long);
-  if (dr <= 56) return ATSC3_QCE_FN(7, unsigned long long);
-  return nullptr;
+// NS <= 17 keeps a check's slot addresses and values in the 64 registers of
+// the 1024-thread build; larger NS run 512 threads (128 registers) only.
+template <int NS>
+static QceFn qce_pick(int semantics, bool big) {
+  if constexpr (NS <= 17) {
+    if (big)
+      return semantics ? ldpc_qce_kernel<true, NS, 1024>
+                       : ldpc_qce_kernel<false, NS, 1024>;
+  }
+  return semantics ? ldpc_qce_kernel<true, NS, 512>
+                   : ldpc_qce_kernel<false, NS, 512>;
 }
 
-// default CTA size: 1024 threads while a check's slot addresses fit the
-// 64-register budget without spilling (block-row degree <= 8), else 512
-static int qce_default_threads(int dr) { return dr <= 8 ? 1024 : 512; }
+static QceFn qce_fn(int semantics, int dr, int threads) {
+  const bool big = threads > 512;
+  switch (qce_ns(dr)) {
+    case 8: return qce_pick<8>(semantics, big);
+    case 10: return qce_pick<10>(semantics, big);
+    case 11: return qce_pick<11>(semantics, big);
+    case 14: return qce_pick<14>(semantics, big);
+    case 17: return qce_pick<17>(semantics, big);
+    case 22: return qce_pick<22>(semantics, big);
+    case 33: return qce_pick<33>(semantics, big);
+    case 56: return qce_pick<56>(semantics, big);
+    default: return nullptr;
+  }
+}
+
+// default CTA size: 1024 threads while a check's slot addresses and values
+// fit the 64-register budget (NS <= 17), else 512
+static int qce_default_threads(int dr) { return qce_ns(dr) <= 17 ? 1024 : 512; }
 
 static std::mutex g_qce_mu;
 static std::unordered_map<uint64_t, int> g_qce_occ;
@@ -691,6 +790,7 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
   meta[4] = p.dr_max;
   meta[5] = p.dc_max;
   meta[6] = p.max_slots;
+  meta[7] = p.buf_off;
   for (int c = 0; c <= EMAXCL; ++c) {
     meta[8 + c] = p.rb[c];
     meta[25 + c] = p.cb[c];
@@ -708,6 +808,7 @@ int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *h, int32_t threads,
   using namespace atsc3;
   ATSC3_ARG(h && out, "null argument");
   if (threads <= 0) threads = qce_default_threads(h->p.dr_max);
+  if (qce_ns(h->p.dr_max) > 17) threads = std::min(threads, 512);
   QceFn fn = qce_fn(semantics, h->p.dr_max, threads);
   ATSC3_ARG(fn != nullptr, "no kernel for this degree");
   int ncl = 0;
@@ -741,6 +842,7 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   ATSC3_ARG(llr != nullptr, "null llr");
   if (threads <= 0) threads = qce_default_threads(p.dr_max);
   ATSC3_ARG(threads == 512 || threads == 1024, "threads must be 512 or 1024");
+  if (qce_ns(p.dr_max) > 17) threads = 512;   // only the 512-thread build
   QceFn fn = qce_fn(semantics, p.dr_max, threads);
   if (!fn) {
     set_error("unsupported: block-row degree too high");
@@ -763,6 +865,9 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   a.iters = iters;
   a.alpha = alpha;
   a.part_off = p.part_off;
+  a.rt_off = p.rt_off;
+  a.ri_off = p.ri_off;
+  a.ct_off = p.ct_off;
   for (int c = 0; c <= EMAXCL; ++c) {
     a.rb[c] = p.rb[c];
     a.cb[c] = p.cb[c];

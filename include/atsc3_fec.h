@@ -203,7 +203,8 @@ int32_t atsc3_ldpc_qce_plan_info(const atsc3_ldpc_qce_plan *plan, int64_t *info)
 /* Host-only descriptor build for the CPU tests (no CUDA call).  meta (42
  * ints): [0] row slots [1] 360-bit columns [2] shared bytes per CTA [3]
  * byte offset of the syndrome exchange words [4] max row degree [5] max
- * column degree [6] most slots per CTA [8..24] block-row split [25..41]
+ * column degree [6] most slots per CTA [7] byte offset of the first slot
+ * [8..24] block-row split [25..41]
  * CTA c owns columns ccols[meta[25+c] .. meta[26+c]).  rdesc: int4 per row
  * slot (owner | wrap<<8 | position<<16, slot byte offset in the owner,
  * shift, bitmap byte offset of the column); cdesc: int4 per column (slots,
@@ -221,8 +222,8 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
 int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *plan, int32_t threads,
                               int32_t semantics, int32_t *out);
 
-/* threads: 0 (default: 1024 for block-row degree <= 8, else 512), 512 or
- * 1024.  ld_hard >= ceil(n/8). */
+/* threads: 0 (default), 512 or 1024; codes with a block-row degree above
+ * 17 always run 512 threads.  ld_hard >= ceil(n/8). */
 int32_t atsc3_ldpc_qce_decode(const atsc3_ldpc_qce_plan *plan, const float *llr,
                               int64_t ld_llr, int32_t nblk, int32_t iters,
                               float alpha, int32_t semantics, uint8_t *bits,

@@ -47,8 +47,9 @@ def test_qce_descriptors_reproduce_csr(rate, n, cluster):
     assert cb[0] == 0 and cb[-1] == nb and (np.diff(cb) >= 0).all()
     assert rb[0] == 0 and rb[-1] == Q
     assert sorted(ccols.tolist()) == list(range(nb))
-    buf_off = part_off + 256
-    assert part_off >= nb * 12 * 4 and smem == buf_off + maxs * SLOT
+    buf_off = meta[7]
+    assert part_off >= nb * 12 * 4 and buf_off >= part_off + 256
+    assert smem == buf_off + maxs * SLOT
     # slot totals per CTA differ by at most one column's slots
     tot = [int(cdesc[ccols[cb[c]:cb[c + 1]], 0].sum()) for c in range(cluster)]
     assert max(tot) == maxs and max(tot) - min(tot) <= cdesc[:, 0].max()
