@@ -70,9 +70,11 @@ struct QcePlan {
   int dr_max = 0, dc_max = 0, max_slots = 0, device = 0;
   int64_t table_bytes = 0;
   int rb[EMAXCL + 1] = {0};     // block rows of CTA c (check phase)
+  int ib[EMAXCL + 1] = {0};     // variable-phase items of CTA c in d_itab
   int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
   int32_t *d_ccols = nullptr;   // (nb) columns grouped by owner CTA
+  int4 *d_itab = nullptr;       // variable-phase items, grouped by CTA
   int32_t *d_rptr = nullptr;    // (Q+1)
   int4 *d_cdesc = nullptr;      // per column
   uint8_t *d_s0 = nullptr;      // (nb*360) rotation start
@@ -91,6 +93,7 @@ struct QceTables {
   std::vector<int32_t> rptr;
   std::vector<int4> cdesc;
   std::vector<int32_t> ccols;
+  std::vector<int4> itab;
   std::vector<uint8_t> s0;
 };
 
@@ -185,17 +188,26 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   (void)total;
   const int per = (Q + cluster - 1) / cluster;
   for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
+  // variable-phase items per CTA: a column of 2..4 edges is cut into six
+  // 64-bit items (lane L takes bits 64p + L and 64p + 32 + L), a larger one
+  // into twelve 32-bit items
+  auto items_of = [&](int g) { const int d = (int)cols[g].size(); return d <= 4 ? 6 : ECHUNK; };
+  int maxitems = 0;
+  for (int c = 0; c < cluster; ++c) {
+    int ni = 0;
+    for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) ni += items_of(t->ccols[q]);
+    maxitems = std::max(maxitems, ni);
+  }
   // shared memory: bitmap | syndrome exchange | row-slot table (per row,
-  // chunk and slot, 8 B) | row masks | column table (16 B per column) | slots
-  int maxcols = 0;
-  for (int c = 0; c < cluster; ++c) maxcols = std::max(maxcols, p->cb[c + 1] - p->cb[c]);
+  // chunk and slot, 8 B) | row masks and degree | variable-phase item table
+  // (16 B per item) | slots
   const int ns = qce_ns(drm);
   const int bm_bytes = (nb * ECHUNK * 4 + 15) & ~15;
   const int part_off = bm_bytes;
   const int rt_off = part_off + EPART;
   const int ri_off = rt_off + per * ECHUNK * ns * 8;
-  const int ct_off = ri_off + ((per * 2 * (ns > 32 ? 8 : 4) + 15) & ~15);
-  const int buf_off = ct_off + maxcols * 16;
+  const int ct_off = ri_off + ((per * 3 * (ns > 32 ? 8 : 4) + 15) & ~15);
+  const int buf_off = ct_off + maxitems * 16;
   std::vector<int> owner(nb), base(nb);
   int maxs = 0;
   for (int c = 0; c < cluster; ++c) {
@@ -235,6 +247,12 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     int wrap = -1;
     for (auto &sl : Cc)
       if (sl.wrap) wrap = sl.idx;
+    // the kernel's parity path expects the wrap edge as slot 1 of a
+    // two-edge column (the last parity column of every Type B code)
+    if (wrap >= 0 && (wrap != 1 || Cc.size() != 2)) {
+      set_error("unsupported: dual-diagonal wrap edge outside a 2-edge column");
+      return -4;
+    }
     t->cdesc[g] = make_int4((int)Cc.size(), base[g], wrap, owner[g]);
     for (int mm = 0; mm < EZ; ++mm) {
       int s = 0;
@@ -242,6 +260,29 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
       t->s0[(size_t)g * EZ + mm] = (uint8_t)s;
     }
   }
+  // item {byte offset of slot 0's entry of the item's first bit, lam index
+  // of that bit, slots | valid lanes of sub-chunk 0 << 8 | of sub-chunk 1
+  // << 16 | absent wrap entry << 24, bitmap word of sub-chunk 0}
+  t->itab.clear();
+  p->ib[0] = 0;
+  for (int c = 0; c < cluster; ++c) {
+    for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) {
+      const int g = t->ccols[q];
+      const int d = (int)cols[g].size();
+      const int wrap = t->cdesc[g].z;
+      const int step = d <= 4 ? 64 : 32;
+      for (int mm0 = 0; mm0 < EZ; mm0 += step) {
+        const int v0 = std::min(32, EZ - mm0);
+        const int v1 = step == 64 ? std::max(0, std::min(32, EZ - mm0 - 32)) : 0;
+        const int absent = (wrap >= 0 && mm0 + step >= EZ) ? 1 : 0;
+        t->itab.push_back(make_int4(base[g] + 4 * mm0, g * EZ + mm0,
+                                    d | (v0 << 8) | (v1 << 16) | (absent << 24),
+                                    g * ECHUNK + mm0 / 32));
+      }
+    }
+    p->ib[c + 1] = (int)t->itab.size();
+  }
+  for (int c = cluster + 1; c <= EMAXCL; ++c) p->ib[c] = p->ib[cluster];
   return 0;
 }
 
@@ -255,7 +296,9 @@ struct QceArgs {
   int part_off, rt_off, ri_off, ct_off;
   int rb[EMAXCL + 1];
   int cb[EMAXCL + 1];
+  int ib[EMAXCL + 1];
   const int32_t *ccols;
+  const int4 *itab;
   const int4 *rdesc;
   const int32_t *rptr;
   const int4 *cdesc;
@@ -346,6 +389,95 @@ __device__ __forceinline__ float qce_var_generic(float *col, int d, int s0,
   return tot;
 }
 
+// One check item: block row rl, chunk ch (32 consecutive checks), D slots.
+// FULL: every slot is an edge of every lane's check and all 32 lanes are
+// checks (no masking at all); otherwise `live` masks absent slots (rows of
+// lower degree, the missing wrap edge of check (0, 0), lanes past 359), whose
+// loads and stores go to a junk word.  Returns the lane's syndrome bit.
+template <bool TORCH, int D, bool FULL, typename MASK>
+__device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
+                                              uint32_t lane,
+                                              const uint32_t *bm,
+                                              uint32_t dummy, bool upd,
+                                              const QceArgs &a, int it) {
+  // per slot: address, remote load (its value is first used by the update
+  // below, so the syndrome lookup overlaps its latency), syndrome bit; the
+  // syndrome-only final pass loads too (valid addresses, values unused)
+  uint32_t ad[D];
+  float t[D];
+  uint32_t synw = 0;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    const uint2 e = te[j];
+    const uint32_t x = (e.y >> 16) + lane;
+    const uint32_t o = min(x, x - (uint32_t)EZ);    // (b + lane) mod 360
+    if constexpr (FULL) {
+      ad[j] = e.x + 4u * o;
+    } else {
+      const uint32_t on = (uint32_t)(live >> j) & 1u;
+      ad[j] = on ? e.x + 4u * o : dummy;
+    }
+    t[j] = dsmem_ld_f32(ad[j]);
+    const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
+    if constexpr (FULL) {
+      synw ^= hw >> (o & 31);
+    } else {
+      synw ^= (hw >> (o & 31)) & ((uint32_t)(live >> j) & 1u);
+    }
+  }
+  if (upd) {
+    const float inf = __int_as_float(0x7f800000);
+    float min1 = inf, min2 = inf;
+    uint32_t first = 0;
+    MASK sv = 0;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      float mag = fabsf(t[j]);
+      bool ng = t[j] < 0.f;
+      if constexpr (!FULL) {
+        const bool on = (live >> j) & 1;
+        mag = on ? mag : inf;
+        ng = ng && on;
+      }
+      sv |= ng ? ((MASK)1 << j) : (MASK)0;
+      const bool lt = mag < min1;
+      min2 = lt ? min1 : fminf(min2, mag);
+      first = lt ? (uint32_t)j : first;
+      min1 = lt ? mag : min1;
+    }
+    constexpr bool WIDE = sizeof(MASK) > 4;
+    int par;
+    if constexpr (WIDE) par = __popcll((unsigned long long)sv) & 1;
+    else par = __popc((uint32_t)sv) & 1;
+    float wa = a.alpha, wb = 0.f;
+    if (a.walpha) {
+      int nl = D;
+      if constexpr (!FULL) {
+        if constexpr (WIDE) nl = __popcll((unsigned long long)live);
+        else nl = __popc((uint32_t)live);
+      }
+      const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+      wa = __ldg(a.walpha + wi);
+      wb = __ldg(a.wbeta + wi);
+    }
+    float A = __fsub_rn(__fmul_rn(min1, wa), wb);
+    float B = __fsub_rn(__fmul_rn(min2, wa), wb);
+    A = A > 0.f ? A : 0.f;
+    B = B > 0.f ? B : 0.f;
+    const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
+    MASK all;
+    if constexpr (FULL) all = (D >= 8 * (int)sizeof(MASK)) ? ~(MASK)0 : (((MASK)1 << D) - 1);
+    else all = live;
+    const MASK neg = par ? (sv ^ all) : sv;          // message signs
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      const uint32_t mg = ((uint32_t)j == first) ? ub : ua;
+      dsmem_st_u32(ad[j], mg | (((uint32_t)(neg >> j) & 1u) << 31));
+    }
+  }
+  return (int)(synw & 1u);
+}
+
 // NS: compile-time slots per block row (qce_ns); NT: threads per CTA.
 template <bool TORCH, int NS, int NT>
 __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
@@ -359,16 +491,17 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   int *sbad = part + 32;
   uint2 *rtab = reinterpret_cast<uint2 *>(smem + a.rt_off);
   MASK *rinfo = reinterpret_cast<MASK *>(smem + a.ri_off);
-  int4 *ctab = reinterpret_cast<int4 *>(smem + a.ct_off);
+  uint4 *itab = reinterpret_cast<uint4 *>(smem + a.ct_off);
   const uint32_t sm_sa = smem_u32(smem);
   const uint32_t part_sa = smem_u32(part);
   const uint32_t dummy = part_sa + 40 * 4;   // junk word for masked slots
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
   const int r0 = a.rb[rank], nr = a.rb[rank + 1] - r0;
-  const int c0 = a.cb[rank], ncol = a.cb[rank + 1] - c0;   // into ccols
+  const int i0 = a.ib[rank], nvitems = a.ib[rank + 1] - i0;
   const int ncitems = nr * ECHUNK;
-  const int nvitems = ncol * ECHUNK;
+  // this lane's cluster address of CTA `lane`'s bitmap (ballot broadcast)
+  const uint32_t bm_peer = lane < CL ? dsmem_map(sm_sa, (uint32_t)lane) : 0u;
 
   // ---- per-launch tables ---------------------------------------------------
   // row slot (rl, chunk, j): {shared::cluster address of the slot block in
@@ -392,37 +525,44 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       MASK wm = 0;
       for (int q = 0; q < deg; ++q)
         if (__ldg(a.rdesc + rp + q).x & EWRAP) wm |= (MASK)1 << q;
-      rinfo[2 * rl] = deg >= (int)(8 * sizeof(MASK)) ? ~(MASK)0
+      rinfo[3 * rl] = deg >= (int)(8 * sizeof(MASK)) ? ~(MASK)0
                                                       : (((MASK)1 << deg) - 1);
-      rinfo[2 * rl + 1] = wm;
+      rinfo[3 * rl + 1] = wm;
+      rinfo[3 * rl + 2] = (MASK)deg;
     }
   }
-  for (int q = tid; q < ncol; q += blockDim.x) {
-    const int g = __ldg(a.ccols + c0 + q);
-    const int4 cd = __ldg(a.cdesc + g);
-    ctab[q] = make_int4(cd.x, cd.y, cd.z, g);
+  // variable-phase items of this CTA (built on the host)
+  for (int q = tid; q < nvitems; q += blockDim.x) {
+    const int4 v = __ldg(a.itab + i0 + q);
+    itab[q] = make_uint4((uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z, (uint32_t)v.w);
   }
   if (tid == 0) *sbad = 0;
   __syncthreads();
 
+  // the absent wrap entry (last parity column, bit 359, its wrap slot) is
+  // lane 7 of sub-chunk 1 of that column's last item, slot 1 of the column
+  constexpr int ABSENT_LANE = EZ - 32 * (ECHUNK - 1) - 1;
+
   for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
     const float *lam = a.llr + (size_t)b * a.ld_llr;
-    // ---- prologue: q = lam - 0 = lam on every slot, hard bits of lam ------
+    // ---- prologue: q = lam - 0 = lam on every slot, hard bits of lam; the
+    // absent entry holds -0.0 (adding it is exact) ---------------------------
     for (int w = warp; w < nvitems; w += nwarps) {
-      const int gl = w / ECHUNK;
-      const int ch = w - gl * ECHUNK;
-      const int4 cd = ctab[gl];
-      const int mm0 = ch * 32 + lane;
-      const bool mv = mm0 < EZ;
-      const int mm = mv ? mm0 : EZ - 1;
-      const float li = lam[cd.w * EZ + mm];
-      float *col = reinterpret_cast<float *>(smem + cd.y) + mm;
-      if (mv)
-        for (int i = 0; i < cd.x; ++i) col[i * EZ] = li;
-      const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < 0.f);
-      if (lane < CL)
-        dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((cd.w * ECHUNK + ch) * 4),
-                               (uint32_t)lane), hb);
+      const uint4 iw = itab[w];
+      const int d = (int)(iw.z & 0xFFu);
+#pragma unroll
+      for (int sub = 0; sub < 2; ++sub) {
+        const uint32_t nval = (iw.z >> (8 + 8 * sub)) & 0xFFu;
+        if (nval == 0) break;                         // 32-bit item
+        const bool mv = (uint32_t)lane < nval;
+        const bool absent = sub == 1 && (iw.z >> 24) && lane == ABSENT_LANE;
+        const float li = mv ? lam[iw.y + 32 * sub + lane] : 0.f;
+        float *col = reinterpret_cast<float *>(smem + iw.x) + 32 * sub + lane;
+        if (mv)
+          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == 1) ? -0.f : li;
+        const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < 0.f);
+        if (lane < CL) dsmem_st_u32(bm_peer + (iw.w + sub) * 4u, hb);
+      }
     }
     __syncthreads();
     cluster_sync_all();
@@ -434,66 +574,24 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       for (int w = warp; w < ncitems; w += nwarps) {
         const int rl = w / ECHUNK;
         const int ch = w - rl * ECHUNK;
-        const int k0 = ch * 32 + lane;
-        MASK live = rinfo[2 * rl];
-        if (k0 == 0) live &= ~rinfo[2 * rl + 1];   // check (0, 0): no wrap edge
-        if (k0 >= EZ) live = 0;                    // lanes past the circulant
+        const MASK wm = rinfo[3 * rl + 1];
+        const int deg = (int)rinfo[3 * rl + 2];
         const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
-        uint32_t ad[NS];
-        uint32_t syn = 0;
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-          const uint2 e = te[j];
-          int o = (int)(e.y >> 16) + lane;
-          o -= o >= EZ ? EZ : 0;
-          const bool on = (live >> j) & 1;
-          const uint32_t hw = bm[(e.y & 0xFFFFu) + (uint32_t)(o >> 5)];
-          syn ^= on ? (hw >> (o & 31)) & 1u : 0u;
-          ad[j] = on ? e.x + 4u * (uint32_t)o : dummy;
+        const bool full = wm == 0 && ch < ECHUNK - 1;
+        int syn;
+        if (full && deg == NS) {
+          syn = qce_check_item<TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
+        } else if (full && deg == NS - 1) {
+          syn = qce_check_item<TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
+        } else {
+          const int k0 = ch * 32 + lane;
+          MASK live = rinfo[3 * rl];
+          if (k0 == 0) live &= ~wm;                  // check (0, 0): no wrap edge
+          if (k0 >= EZ) live = 0;                    // lanes past the circulant
+          syn = qce_check_item<TORCH, NS, false, MASK>(te, live, lane, bm, dummy, upd, a, it);
+          syn = k0 < EZ ? syn : 0;
         }
-        mybad += (int)syn;
-        if (upd) {
-          float t[NS];
-#pragma unroll
-          for (int j = 0; j < NS; ++j) t[j] = dsmem_ld_f32(ad[j]);
-          float min1 = __int_as_float(0x7f800000), min2 = min1;
-          uint32_t first = 0;
-          MASK sv = 0;
-#pragma unroll
-          for (int j = 0; j < NS; ++j) {
-            const bool on = (live >> j) & 1;
-            if (on && t[j] < 0.f) sv |= (MASK)1 << j;
-            const float mag = on ? fabsf(t[j]) : __int_as_float(0x7f800000);
-            const bool lt = mag < min1;
-            min2 = lt ? min1 : fminf(min2, mag);
-            first = lt ? (uint32_t)j : first;
-            min1 = fminf(min1, mag);
-          }
-          int par;
-          if constexpr (NS > 32) par = __popcll((unsigned long long)sv) & 1;
-          else par = __popc((uint32_t)sv) & 1;
-          float wa = a.alpha, wb = 0.f;
-          if (a.walpha) {
-            int nl;
-            if constexpr (NS > 32) nl = __popcll((unsigned long long)live);
-            else nl = __popc((uint32_t)live);
-            const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
-            wa = __ldg(a.walpha + wi);
-            wb = __ldg(a.wbeta + wi);
-          }
-          float A = __fsub_rn(__fmul_rn(min1, wa), wb);
-          float B = __fsub_rn(__fmul_rn(min2, wa), wb);
-          A = A > 0.f ? A : 0.f;
-          B = B > 0.f ? B : 0.f;
-          const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
-          const MASK neg = par ? (sv ^ live) : sv;   // message signs
-          // masked slots and lanes store to the junk word
-#pragma unroll
-          for (int j = 0; j < NS; ++j) {
-            const uint32_t mg = ((uint32_t)j == first) ? ub : ua;
-            dsmem_st_u32(ad[j], mg | (((uint32_t)(neg >> j) & 1u) << 31));
-          }
-        }
+        mybad += syn;
       }
       mybad = __reduce_add_sync(0xffffffffu, mybad);
       if (lane == 0 && mybad) atomicAdd(sbad, mybad);
@@ -543,43 +641,64 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       }
       // ---------------- variable phase (local) -----------------------------
       for (int w = warp; w < nvitems; w += nwarps) {
-        const int gl = w / ECHUNK;
-        const int ch = w - gl * ECHUNK;
-        const int4 cd = ctab[gl];                 // {d, slot base, wrap, g}
-        const int d = cd.x;
-        const int mm0 = ch * 32 + lane;
-        const bool mv = mm0 < EZ;
-        const int mm = mv ? mm0 : EZ - 1;
-        const int lamidx = cd.w * EZ + mm;
-        const float li = lam[lamidx];
-        const int s0 = __ldg(a.s0 + lamidx);
-        float *col = reinterpret_cast<float *>(smem + cd.y) + mm;
-        float tot;
-        if (d == 2) {
-          // dual-diagonal parity column; its wrap slot is absent for bit 359
-          const int skip = (mm == EZ - 1) ? cd.z : -1;
-          const int i0 = s0 >= 2 ? s0 - 2 : s0;
-          const int i1 = i0 == 0 ? 1 : 0;
-          const float m0 = col[i0 * EZ], m1 = col[i1 * EZ];
-          float acc = TORCH ? li : 0.f;
-          if (i0 != skip) acc = __fadd_rn(acc, m0);
-          if (i1 != skip) acc = __fadd_rn(acc, m1);
-          tot = TORCH ? acc : __fadd_rn(li, acc);
-          if (mv) {
-            if (i0 != skip) col[i0 * EZ] = __fsub_rn(tot, m0);
-            if (i1 != skip) col[i1 * EZ] = __fsub_rn(tot, m1);
+        const uint4 iw = itab[w];
+        const int d = (int)(iw.z & 0xFFu);
+        if (d <= 4) {
+          // 64-bit item: lane L takes bits y + L and y + 32 + L
+          const uint32_t nv0 = (iw.z >> 8) & 0xFFu, nv1 = (iw.z >> 16) & 0xFFu;
+          const bool mv0 = (uint32_t)lane < nv0, mv1 = (uint32_t)lane < nv1;
+          const int l0 = mv0 ? lane : 0, l1 = mv1 ? 32 + lane : 0;
+          const float li0 = lam[iw.y + l0], li1 = lam[iw.y + l1];
+          float *col0 = reinterpret_cast<float *>(smem + iw.x) + l0;
+          float *col1 = reinterpret_cast<float *>(smem + iw.x) + l1;
+          float t0, t1;
+          if (d == 2) {
+            // dual-diagonal parity column: slots in check order for every
+            // bit (u = 0 twice, or u = 0, 1 for the last column, whose wrap
+            // entry of bit 359 is absent and holds -0.0)
+            const float a0 = col0[0], b0 = col0[EZ], a1 = col1[0], b1 = col1[EZ];
+            float s0 = TORCH ? li0 : 0.f, s1 = TORCH ? li1 : 0.f;
+            s0 = __fadd_rn(__fadd_rn(s0, a0), b0);
+            s1 = __fadd_rn(__fadd_rn(s1, a1), b1);
+            t0 = TORCH ? s0 : __fadd_rn(li0, s0);
+            t1 = TORCH ? s1 : __fadd_rn(li1, s1);
+            const bool absent = (iw.z >> 24) && lane == ABSENT_LANE;
+            if (mv0) {
+              col0[0] = __fsub_rn(t0, a0);
+              col0[EZ] = __fsub_rn(t0, b0);
+            }
+            if (mv1) {
+              col1[0] = __fsub_rn(t1, a1);
+              col1[EZ] = absent ? -0.f : __fsub_rn(t1, b1);
+            }
+          } else {
+            const int r0s = __ldg(a.s0 + iw.y + l0), r1s = __ldg(a.s0 + iw.y + l1);
+            if (d == 3) {
+              t0 = qce_var_exact<TORCH, 3>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<TORCH, 3>(col1, r1s, li1, mv1);
+            } else {
+              t0 = qce_var_exact<TORCH, 4>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<TORCH, 4>(col1, r1s, li1, mv1);
+            }
           }
-        } else if (d == 3) {
-          tot = qce_var_exact<TORCH, 3>(col, s0, li, mv);
-        } else if (d == 4) {
-          tot = qce_var_exact<TORCH, 4>(col, s0, li, mv);
+          const uint32_t h0 = __ballot_sync(0xffffffffu, mv0 && t0 < 0.f);
+          const uint32_t h1 = __ballot_sync(0xffffffffu, mv1 && t1 < 0.f);
+          if (lane < CL) {
+            dsmem_st_u32(bm_peer + iw.w * 4u, h0);
+            if (nv1) dsmem_st_u32(bm_peer + (iw.w + 1) * 4u, h1);
+          }
         } else {
-          tot = qce_var_generic<TORCH>(col, d, s0, li, mv);
+          // 32-bit item of a column with more than four edges
+          const bool mv = (uint32_t)lane < ((iw.z >> 8) & 0xFFu);
+          const int ln = mv ? lane : 0;          // lanes past 359 read bit 0
+          const int lamidx = (int)iw.y + ln;
+          const float li = lam[lamidx];
+          float *col = reinterpret_cast<float *>(smem + iw.x) + ln;
+          const int s0 = __ldg(a.s0 + lamidx);
+          const float tot = qce_var_generic<TORCH>(col, d, s0, li, mv);
+          const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
+          if (lane < CL) dsmem_st_u32(bm_peer + iw.w * 4u, hb);
         }
-        const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
-        if (lane < CL)
-          dsmem_st_u32(dsmem_map(sm_sa + (uint32_t)((cd.w * ECHUNK + ch) * 4),
-                                 (uint32_t)lane), hb);
       }
       __syncthreads();
       cluster_sync_all();
@@ -737,6 +856,7 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
   if (e == cudaSuccess) e = up((void **)&h->p.d_rptr, t.rptr.data(), t.rptr.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_cdesc, t.cdesc.data(), t.cdesc.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_ccols, t.ccols.data(), t.ccols.size() * 4);
+  if (e == cudaSuccess) e = up((void **)&h->p.d_itab, t.itab.data(), t.itab.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
   if (e != cudaSuccess) {
     atsc3_ldpc_qce_plan_destroy(h);
@@ -752,6 +872,7 @@ void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
   cudaFree(h->p.d_rptr);
   cudaFree(h->p.d_cdesc);
   cudaFree(h->p.d_ccols);
+  cudaFree(h->p.d_itab);
   cudaFree(h->p.d_s0);
   delete h;
 }
@@ -873,6 +994,8 @@ int32_t atsc3_ldpc_qce_decode_weighted(
     a.cb[c] = p.cb[c];
   }
   a.ccols = p.d_ccols;
+  a.itab = p.d_itab;
+  for (int c = 0; c <= EMAXCL; ++c) a.ib[c] = p.ib[c];
   a.rdesc = p.d_rdesc;
   a.rptr = p.d_rptr;
   a.cdesc = p.d_cdesc;
