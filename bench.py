@@ -409,8 +409,10 @@ KERNEL_NAMES = {"qce": "ldpc_qce_kernel (quasi-cyclic flooding, edge-buffer layo
 
 # DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch:
 # dram__bytes_read.sum + dram__bytes_write.sum of one captured 75-block launch
-# (19,553,792 + 0 B) / 75, from profiles/ldpc_qc_flood_6_15_frame.md.
-TRAFFIC_PER_BLOCK = 19_553_792 / 75
+# of the edge-buffer decoder (19,549,184 + 0 B) / 75, from
+# profiles/ldpc_qce_flood_6_15_frame.md (the record-layout decoder's capture,
+# profiles/ldpc_qc_flood_6_15_frame.md, read 19,553,792 B).
+TRAFFIC_PER_BLOCK = 19_549_184 / 75
 
 
 def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
