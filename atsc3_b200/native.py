@@ -68,6 +68,10 @@ SIGNATURES = {
                                                c_vp, c_i32, c_i32, c_vp, c_vp,
                                                c_i64, c_vp, c_i64, c_vp, c_vp,
                                                c_vp, c_i32, c_vp]),
+    "atsc3_ldpc_sp_workspace": (c_i32, [c_i32, c_i32, c_i32, c_vp]),
+    "atsc3_ldpc_sp_decode": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32,
+                                     c_i32, c_vp, c_i64, c_i32, c_i32, c_vp,
+                                     c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "atsc3_ldpc_layered_plan_create": (c_i32, [c_i32, c_i32, c_i32, c_vp,
                                                c_vp, c_vp]),
     "atsc3_ldpc_layered_plan_destroy": (None, [c_vp]),
@@ -95,6 +99,9 @@ SIGNATURES = {
     "atsc3_bch_batch": (c_i32, [c_vp] * 11 + [c_i32, c_vp]),
     "atsc3_demap": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32, c_i32,
                             c_vp, c_i64, c_f32, c_vp, c_vp, c_i64, c_vp]),
+    "atsc3_demap_gather": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32,
+                                   c_i32, c_vp, c_i64, c_i64, c_i64, c_i32,
+                                   c_vp, c_f32, c_vp, c_vp, c_i64, c_vp]),
     "atsc3_demap_row_sigma2": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,
                                        c_i32, c_vp, c_vp]),
     "atsc3_bch_check": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_vp, c_vp,

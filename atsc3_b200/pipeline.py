@@ -25,10 +25,15 @@ def _torch():
 
 class FecPipeline:
     """One (Ninner, constellation, rate) PLP configuration.  kind selects the
-    LDPC decoder ("auto", "qce", "qc" or "csr"; see ldpc.plan_for)."""
+    LDPC decoder ("auto", "qce", "qc" or "csr"; see ldpc.plan_for).
+    rescue: None (off, as the reference's default) or a dict of
+    ldpc.rescue_near_misses arguments (near_max, max_blocks, iters): blocks
+    min-sum leaves a few checks short get the exact sum-product before BCH
+    (this adds a host read of the flags)."""
 
     def __init__(self, n, mod, rate, iters=50, alpha=0.75, semantics="kernel",
-                 cluster=0, threads=0, device="cuda", kind="auto"):
+                 cluster=0, threads=0, device="cuda", kind="auto",
+                 rescue=None):
         torch = _torch()
         self.n, self.mod, self.rate = int(n), mod, rate
         self.nb = C.MOD_BITS[mod]
@@ -41,6 +46,9 @@ class FecPipeline:
         self.device = torch.device(device)
         with torch.cuda.device(self.device):
             self.plan = LDPC.plan_for(rate, n, "float32", cluster, kind=kind)
+            self.rescue = dict(rescue) if rescue else None
+            self.sp_tab = (LDPC.sp_tables(C.csr(rate, n), n, self.device)
+                           if self.rescue else None)
         self._ws = {}
 
     def _buffers(self, nblk):
@@ -77,6 +85,31 @@ class FecPipeline:
             ws.update(out)
         DM.demap(cells, self.mod, self.rate, sigma2=sigma2, n=self.n,
                  deinterleave=True, out=ws["lam"])
+        LDPC.decode_flood(self.plan, ws["lam"], iters=iters or self.iters,
+                          alpha=self.alpha if alpha is None else alpha,
+                          semantics=self.semantics, want_bits=False,
+                          want_hard=True, threads=self.threads, out=ws,
+                          weights=weights)
+        if self.rescue:
+            LDPC.rescue_near_misses(self.sp_tab, ws["lam"], ws, **self.rescue)
+        BCH.bch_check(ws["hard"], self.kldpc, self.n, self.kpayload,
+                      want_payload=True, out=ws)
+        return ws
+
+    def decode_stream(self, stream, ti, sigma2, iters=None, alpha=None,
+                      out=None, weights=None):
+        """As decode, from a received PLP cell stream instead of FEC Block
+        rows: ``ti`` (timeint.HybridTI / ConvolutionalTI) is de-interleaved
+        inside the demapper's cell load (the reference de-interleaves on
+        the host first, lab/m9_fast.py:1087-1093, lab/m10_cti.py:126-141).
+        sigma2: float, per received cell, or per FEC Block."""
+        from . import timeint as TI
+        nblk = ti.nblk
+        ws = dict(self._buffers(nblk))
+        if out:
+            ws.update(out)
+        TI.demap_deinterleave(stream, ti, self.mod, self.rate, self.n,
+                              sigma2=sigma2, out=ws["lam"])
         LDPC.decode_flood(self.plan, ws["lam"], iters=iters or self.iters,
                           alpha=self.alpha if alpha is None else alpha,
                           semantics=self.semantics, want_bits=False,

@@ -250,6 +250,7 @@ def learned_weights(dev):
 def run_gpu(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
+    from atsc3_b200 import codes as C
     from atsc3_b200 import shard
     from atsc3_b200.pipeline import FecPipeline
     torch.cuda.set_device(local_rank)
@@ -310,6 +311,7 @@ def run_gpu(args, rank, world, local_rank):
     value = total_bits / (ms / 1e3) / 1e6
     # ---- per-stage device time, one stream, no overlap (roofline) ---------
     nprof = min(K, 9)
+    stage_its = []
     E = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
          for _ in range(nprof)]
     from atsc3_b200 import bch as BCH, demap as DM, ldpc as LDPC
@@ -327,6 +329,7 @@ def run_gpu(args, rank, world, local_rank):
         E[s][2].record(main)
         BCH.bch_check(ws["hard"], p0.kldpc, N_INNER, kp, out=o)
         E[s][3].record(main)
+        stage_its.append(int(o["its"].sum()))
     torch.cuda.synchronize()
     stage = np.array([[E[s][0].elapsed_time(E[s][1]), E[s][1].elapsed_time(E[s][2]),
                        E[s][2].elapsed_time(E[s][3])] for s in range(nprof)])
@@ -360,6 +363,21 @@ def run_gpu(args, rank, world, local_rank):
                                                    "step", "seed")}}
     # ---- roofline of the dominant kernel (the LDPC decoder) ---------------
     ldpc_ms = float(stage[:, 1].mean())
+    # on-chip exchange of the edge-buffer decoder: per edge and iteration one
+    # 4-byte load of the variable-to-check value and one 4-byte store of the
+    # message through distributed shared memory (the iterations of the
+    # stage-timing frames, read from their outputs)
+    nedges = int(C.csr(RATE, N_INNER)[1].shape[0])
+    its_stage = float(np.mean(stage_its)) if stage_its else 0.0
+    onchip = {"unit": "GB/s", "bytes_per_launch": 8 * nedges * its_stage,
+              "achieved": 8 * nedges * its_stage / (ldpc_ms / 1e3) / 1e9,
+              "what": "distributed-shared-memory exchange, 8 B per edge per "
+                      "iteration (edge-buffer decoder)",
+              "peak_ncu": 9300.0,
+              "peak_note": "xbar-to-L1 distributed shared memory bytes at "
+                           "25.8% of peak = 2.40 TB/s in the committed ncu "
+                           "capture, i.e. about 9.3 TB/s"}
+    onchip["frac"] = onchip["achieved"] / onchip["peak_ncu"]
     b_ldpc = nblk * (4 * N_INNER + N_INNER // 8 + 9)
     hbm, peak_kind = peaks()
     achieved = b_ldpc / (ldpc_ms / 1e3) / 1e9
@@ -388,7 +406,8 @@ def run_gpu(args, rank, world, local_rank):
                                                         "ldpc_flood_kernel (CSR flooding)"),
                              "peak_kind": peak_kind,
                              "bytes_per_launch": b_ldpc,
-                             "ms_per_launch": ldpc_ms},
+                             "ms_per_launch": ldpc_ms,
+                             "onchip": onchip},
                 "stage_ms": {"demap": float(stage[:, 0].mean()),
                              "ldpc": ldpc_ms,
                              "bch": float(stage[:, 2].mean())},

@@ -241,6 +241,28 @@ int32_t atsc3_ldpc_qce_decode_weighted(
     int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
     int32_t threads, void *stream);
 
+/* ---- exact sum-product (near-miss rescue) ----------------------------------
+ * Float64 log-tanh belief propagation over nblk codewords, replacing
+ * lab/m16_margin.py:325-390 sum_product_decode_batch (the rescue
+ * lab/m44_ldm.py:2527-2554 offers the blocks min-sum left a few checks
+ * short).  Same stopping rule: syndrome before each update, its = the
+ * iteration at which the syndrome is zero, else iters with bad = the
+ * unsatisfied count.  cptr/cidx/vptr/vedge: DEVICE CSR tables
+ * (lab/m3_ldpc.py:459-482 layout); llr (nblk, ld_llr) float64; bits (nblk,
+ * ld_bits) uint8; conv/its/bad per block; work: atsc3_ldpc_sp_workspace
+ * bytes, 8-byte aligned.  The reference's wall-clock deadline has no
+ * counterpart: the GPU runs to `iters`.  Launches 4*(iters+1)+1 kernels on
+ * `stream`; returns without synchronising. */
+int32_t atsc3_ldpc_sp_workspace(int32_t n, int32_t nedges, int32_t nblk,
+                                int64_t *work_bytes);
+int32_t atsc3_ldpc_sp_decode(const int32_t *cptr, const int32_t *cidx,
+                             const int32_t *vptr, const int32_t *vedge,
+                             int32_t n, int32_t nc, int32_t nedges,
+                             const double *llr, int64_t ld_llr, int32_t nblk,
+                             int32_t iters, uint8_t *bits, int64_t ld_bits,
+                             uint8_t *conv, int32_t *its, int32_t *bad,
+                             void *work, void *stream);
+
 /* ---- layered decoder for the A/322 Type B codes ----------------------------
  * Layered normalised min-sum: the Q block rows are the layers, the posterior
  * is updated in place after each layer, syndrome before the first and after
@@ -315,6 +337,31 @@ int32_t atsc3_demap(const float *cells, int64_t ld_cells, int32_t nblk,
                     int32_t sigma_mode, const float *sigma2, int64_t ld_sigma,
                     float sigma2_scalar, const int32_t *lam_of_q, float *out,
                     int64_t ld_out, void *stream);
+
+/* Time de-interleave fused into the demapper's load (csrc/timeint.cu):
+ * demaps FEC Block b's cell s from the received PLP cell stream `cells`
+ * (ncells complex64) at its source position, without writing the
+ * de-interleaved cells; otherwise as atsc3_demap (bit de-interleaver through
+ * lam_of_q, LLRs into out).  gather_mode:
+ *   0: src_index (nblk, ncell) int32 source positions (-1: no cell) -- any
+ *      map, e.g. a hybrid TI block with virtual FEC Blocks;
+ *   1: hybrid TI, twisted block de-interleaver without virtual Blocks
+ *      (replaces lab/m6_tbi.py:75-88 fec_block and its cached gather
+ *      lab/m9_fast.py:1087-1093): p0 = stream offset, p1 = Nc (FEC Blocks
+ *      per TI block), p2 = per_ti (cells per TI block); ncell = Nr;
+ *      block b = TI block b / Nc, FEC Block b mod Nc;
+ *   2: convolutional TI (replaces lab/m10_cti.py:126-141 deinterleave):
+ *      p0 = C (pre-CTI position of the first FEC Block's first cell),
+ *      p1 = Nrows, p2 = start_row.
+ * sigma_mode: 0 scalar, 1 per received cell (indexed like cells), 2 per FEC
+ * Block.  A cell whose source lies outside [0, ncells) is an erasure (LLR 0). */
+int32_t atsc3_demap_gather(const float *cells, int64_t ncells, int32_t nblk,
+                           int32_t ncell, const float *pts, int32_t nbits,
+                           int32_t gather_mode, const int32_t *src_index,
+                           int64_t p0, int64_t p1, int64_t p2,
+                           int32_t sigma_mode, const float *sigma2,
+                           float sigma2_scalar, const int32_t *lam_of_q,
+                           float *out, int64_t ld_out, void *stream);
 
 /* Per-row noise estimate of lab/m44_ldm.py:2480 / lab/m16_demap_fast.py:104:
  * sigma2[b] = max(mean_cells(|z|^2 + min_p metric), 1e-9), accumulated in

@@ -433,3 +433,124 @@ def layered(llr, rate, n, iters=50, alpha=0.75):
     if rc != 0:
         raise RuntimeError(f"oracle layered decode returned {rc}")
     return bits, conv.astype(bool), its, bad
+
+
+# ---------------------------------------------------------------------------
+# time de-interleavers (checkers of csrc/timeint.cu)
+# ---------------------------------------------------------------------------
+
+def tbi_read_order(nrows, ncols, n_virtual=0):
+    """Memory index of each transmitted cell of a twisted-block TI block,
+    virtual positions dropped.  Follows lab/m6_tbi.py:46-58 (A/322 7.1.5.4):
+    R = i mod Nr, C = ((R mod Nc) + i div Nr) mod Nc, theta = Nr*C + R."""
+    out = []
+    for i in range(nrows * ncols):
+        r = i % nrows
+        c = ((r % ncols) + i // nrows) % ncols
+        theta = nrows * c + r
+        if theta >= n_virtual * nrows:
+            out.append(theta - n_virtual * nrows)
+    return np.array(out, np.int64)
+
+
+def tbi_deinterleave(cells, nrows, ncols, n_virtual=0):
+    """Transmitted order -> memory order (FEC Block major); follows
+    lab/m6_tbi.py:61-68."""
+    order = tbi_read_order(nrows, ncols, n_virtual)
+    out = np.empty_like(np.asarray(cells))
+    out[order] = cells
+    return out
+
+
+def cti_deinterleave(recv, nrows, start_row, n_out):
+    """Pre-interleaver cells from the received stream, and the valid mask;
+    follows lab/m10_cti.py:97-100 and :126-141 (out[i] = recv[q(i)],
+    q(i) = i + Nrows*((start_row + i) mod Nrows))."""
+    recv = np.asarray(recv)
+    i = np.arange(n_out, dtype=np.int64)
+    q = i + nrows * ((start_row + i) % nrows)
+    valid = q < len(recv)
+    out = np.zeros(n_out, recv.dtype)
+    out[valid] = recv[q[valid]]
+    return out, valid
+
+
+# ---------------------------------------------------------------------------
+# exact sum-product (checker of csrc/sp.cu)
+# ---------------------------------------------------------------------------
+
+def sum_product(lam2d, tables, n, iters=100):
+    """Float64 log-tanh belief propagation with the stopping rule of
+    lab/m16_margin.py:325-390 (sum_product_decode_batch, deadline None):
+    padded (check, slot) view of the CSR tables as lab/m3_ldpc.py:228-242
+    `pack` builds it, syndrome before each update, messages
+    +-2 atanh(exp(clip(sum log|tanh(v/2)| - own, -700, -1e-16))), totals
+    rebuilt as llr + messages accumulated in (check, slot) order.
+    Returns (bits uint8, conv bool, its int32, bad int32)."""
+    cptr, cidx = np.asarray(tables[0]), np.asarray(tables[1])
+    nc = len(cptr) - 1
+    deg = np.diff(cptr)
+    dmax = int(deg.max())
+    idx = np.full((nc, dmax), n, np.int64)
+    mask = np.zeros((nc, dmax), bool)
+    for c in range(nc):
+        idx[c, :deg[c]] = cidx[cptr[c]:cptr[c + 1]]
+        mask[c, :deg[c]] = True
+    lam2d = np.asarray(lam2d, np.float64)
+    nblk = lam2d.shape[0]
+    tot = np.zeros((nblk, n + 1))
+    tot[:, :n] = lam2d
+    m = np.zeros((nblk, nc, dmax))
+    bits = (lam2d < 0).astype(np.uint8)
+    conv = np.zeros(nblk, bool)
+    its = np.full(nblk, iters, np.int32)
+    bad_out = np.full(nblk, -1, np.int32)
+    act = np.arange(nblk)
+    for it in range(iters + 1):
+        gg = tot[:, idx]
+        syn = np.bitwise_xor.reduce((gg < 0) & mask, axis=2)
+        bad = syn.sum(axis=1, dtype=np.int32)
+        done = bad == 0
+        if done.any():
+            sel = act[done]
+            bits[sel] = tot[done, :n] < 0
+            conv[sel] = True
+            its[sel] = it
+            bad_out[sel] = 0
+            keep = ~done
+            if not keep.any():
+                return bits, conv, its, bad_out
+            act, tot, m, gg, bad = act[keep], tot[keep], m[keep], gg[keep], bad[keep]
+        if it == iters:
+            bits[act] = tot[:, :n] < 0
+            bad_out[act] = bad
+            its[act] = it
+            break
+        v = gg - m
+        t = np.tanh(np.clip(v, -38.0, 38.0) * 0.5)
+        sg = t < 0
+        parity = np.bitwise_xor.reduce(sg & mask, axis=2)
+        lt = np.log(np.clip(np.abs(t), 1e-300, 1.0))
+        lt[:, ~mask] = 0.0
+        lsum = lt.sum(axis=2, keepdims=True)
+        le = np.clip(lsum - lt, -700.0, -1e-16)
+        mnew = 2.0 * np.arctanh(np.clip(np.exp(le), 0.0, 1.0 - 1e-16))
+        sgn = np.where(parity[:, :, None] ^ sg, -1.0, 1.0)
+        m = np.where(mask, sgn * mnew, 0.0)
+        na = len(act)
+        tot[:, :n] = lam2d[act]
+        tot[:, n] = 0.0
+        np.add.at(tot, (np.arange(na)[:, None, None], idx[None, :, :]), m)
+        tot[:, n] = 0.0
+    return bits, conv, its, bad_out
+
+
+def near_miss_llr(rate, n, nblk, mu, seed):
+    """Consistent-Gaussian LLRs of random codewords (llr = (1 - 2c)*mu +
+    N(0, 2*mu)): the seeded input of the sum-product checks."""
+    rng = np.random.default_rng(seed)
+    K = C.kldpc(rate, n)
+    info = rng.integers(0, 2, (nblk, K)).astype(np.uint8)
+    cw = ldpc_encode(info, rate, n)
+    lam = (1.0 - 2.0 * cw) * mu + rng.standard_normal(cw.shape) * np.sqrt(2.0 * mu)
+    return lam.astype(np.float32), cw
