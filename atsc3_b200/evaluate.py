@@ -130,18 +130,24 @@ def sweep(rate, mod, weights, esn0s, nblk, n=64800, seed=99, chunk=2000):
     return out
 
 
-def run(steps=2000, batch=256, nblk=100000, points=9, out_dir=None, seed=1):
+def run(steps=2000, batch=256, nblk=100000, points=9, out_dir=None, seed=1,
+        iters=12, window=(-0.5, 1.5), tag="", depths=None):
+    """iters: unrolled depth of the training decoder; window: training Es/N0
+    range relative to the plain threshold (dB); tag: weights file infix."""
     report = {}
     out_dir = out_dir or os.path.join(HERE, "data")
     for rate, mod in MODCODS:
         t0 = time.time()
         thr = threshold(rate, mod)
         al, be, hist, man = LR.train(rate, 64800, mod, steps=steps, nblk=batch,
-                                     iters=12, esn0=(thr - 0.5, thr + 1.5),
+                                     iters=iters,
+                                     esn0=(thr + window[0], thr + window[1]),
                                      channel="mixed", seed=seed,
-                                     log_every=max(1, steps // 10))
+                                     log_every=max(1, steps // 10),
+                                     depths=depths)
         man["threshold_db"] = thr
-        path = os.path.join(out_dir, f"weights_{rate.replace('/', '_')}_{mod}.pt")
+        name = f"weights_{tag + '_' if tag else ''}{rate.replace('/', '_')}_{mod}.pt"
+        path = os.path.join(out_dir, name)
         LR.save_weights(path, al, be, man)
         code = LR.WmsCode(rate, 64800)
         w = LR.inference_weights(al, be, code.buckets)
@@ -180,8 +186,18 @@ def main(argv=None):
     ap.add_argument("--blocks", type=int, default=100000)
     ap.add_argument("--points", type=int, default=9)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--iters", type=int, default=12,
+                    help="unrolled iterations of the training decoder")
+    ap.add_argument("--window", type=float, nargs=2, default=(-0.5, 1.5),
+                    help="training Es/N0 range relative to the plain threshold")
+    ap.add_argument("--tag", default="", help="weights file infix")
+    ap.add_argument("--depths", type=int, nargs="*", default=None,
+                    help="average the output BCE over these unrolled depths")
     a = ap.parse_args(argv)
-    print(json.dumps(run(a.steps, a.batch, a.blocks, a.points, a.out)), flush=True)
+    print(json.dumps(run(a.steps, a.batch, a.blocks, a.points, a.out,
+                         iters=a.iters, window=tuple(a.window), tag=a.tag,
+                         depths=a.depths)),
+          flush=True)
 
 
 if __name__ == "__main__":

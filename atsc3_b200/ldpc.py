@@ -380,3 +380,103 @@ def check_layered_error(plan):
         plan.err.zero_()
         raise N.FecError("atsc3_ldpc_layered_decode", -2,
                          "a staged copy did not complete (bounded wait)")
+
+
+# ---------------------------------------------------------------------------
+# exact sum-product: the near-miss rescue (csrc/sp.cu)
+# ---------------------------------------------------------------------------
+
+_SP_TABLES = {}
+_SP_LOCK = threading.Lock()
+
+
+def sp_tables(tables, n, device="cuda"):
+    """Device copies of CSR tables (cptr, cidx, vptr, vedge) for sp_decode,
+    cached by content."""
+    torch = _torch()
+    arrs = [np.ascontiguousarray(t, np.int32) for t in tables]
+    key = (n, str(torch.device(device)), tuple(hash(a.tobytes()) for a in arrs))
+    with _SP_LOCK:
+        d = _SP_TABLES.get(key)
+        if d is None:
+            d = {"n": int(n), "nc": len(arrs[0]) - 1, "nedges": len(arrs[1]),
+                 "t": [torch.from_numpy(a).to(device) for a in arrs]}
+            _SP_TABLES[key] = d
+    return d
+
+
+def sp_decode(tab, llr, iters=100, out=None, stream=None):
+    """Float64 log-tanh belief propagation of (nblk, n) CUDA float64 LLRs
+    (lab/m16_margin.py:325-390 semantics: syndrome before each update, its
+    = the iteration the syndrome vanished, else iters with bad = the
+    unsatisfied count).  Returns device tensors bits, conv, its, bad."""
+    torch = _torch()
+    if llr.dtype != torch.float64 or llr.device.type != "cuda" or \
+            llr.dim() != 2 or llr.shape[1] != tab["n"] or llr.stride(1) != 1:
+        raise TypeError("llr must be a (nblk, n) CUDA float64 tensor")
+    nblk, n = llr.shape
+    dev = llr.device
+    o = out if out is not None else {}
+    o.setdefault("bits", torch.empty((nblk, n), dtype=torch.uint8, device=dev))
+    o.setdefault("conv", torch.empty(nblk, dtype=torch.uint8, device=dev))
+    o.setdefault("its", torch.empty(nblk, dtype=torch.int32, device=dev))
+    o.setdefault("bad", torch.empty(nblk, dtype=torch.int32, device=dev))
+    nbytes = ctypes.c_int64()
+    N.call("atsc3_ldpc_sp_workspace", n, tab["nedges"], nblk, ctypes.byref(nbytes))
+    work = torch.empty(max(8, nbytes.value), dtype=torch.uint8, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    c, ci, v, ve = tab["t"]
+    N.call("atsc3_ldpc_sp_decode", c.data_ptr(), ci.data_ptr(), v.data_ptr(),
+           ve.data_ptr(), n, tab["nc"], tab["nedges"], llr.data_ptr(),
+           llr.stride(0), nblk, int(iters), o["bits"].data_ptr(),
+           o["bits"].stride(0), o["conv"].data_ptr(), o["its"].data_ptr(),
+           o["bad"].data_ptr(), work.data_ptr(), st)
+    o["_work"] = work            # alive until the stream has run the launches
+    return o
+
+
+def sum_product_decode_batch(lam2d, checks, n, iters=100, deadline=None,
+                             stats=None):
+    """Drop-in for ``lab/m16_margin.py:325`` ``sum_product_decode_batch``:
+    numpy (bits uint8, conv bool, its int32, bad int32).  ``deadline`` (a
+    wall-clock budget on the host) has no GPU counterpart: the decode runs
+    to ``iters``; ``stats`` is accepted and left untouched."""
+    torch = _torch()
+    tab = sp_tables(C.csr_from_checks(checks, n), n)
+    llr = torch.from_numpy(np.ascontiguousarray(lam2d, np.float64)).cuda()
+    o = sp_decode(tab, llr, iters=iters)
+    torch.cuda.synchronize()
+    return (o["bits"].cpu().numpy(), o["conv"].cpu().numpy().astype(bool),
+            o["its"].cpu().numpy(), o["bad"].cpu().numpy())
+
+
+def rescue_near_misses(tab, lam, out, near_max=1500, max_blocks=8, iters=100):
+    """The near-miss rescue of ``lab/m44_ldm.py:2527-2554``: the blocks a
+    min-sum decode left unconverged with at most ``near_max`` unsatisfied
+    checks (the ``max_blocks`` closest ones) are decoded again with the
+    exact float64 sum-product; those that converge replace their packed
+    hard decisions (``out["hard"]``) and flags (conv = 1, bad = 0; ``its``
+    keeps the min-sum count).  ``lam``: the (nblk, n) float32 LLRs of that
+    decode.  Selecting the blocks reads conv/bad on the host (as the
+    reference does).  Returns the indices of the rescued blocks."""
+    torch = _torch()
+    conv = out["conv"].cpu().numpy()
+    bad = out["bad"].cpu().numpy()
+    near = np.flatnonzero((conv == 0) & (bad <= near_max))
+    if len(near) > max_blocks:
+        near = near[np.argsort(bad[near], kind="stable")[:max_blocks]]
+    if not len(near):
+        return near
+    dev = lam.device
+    idx = torch.from_numpy(near.astype(np.int64)).to(dev)
+    o = sp_decode(tab, lam.index_select(0, idx).double(), iters=iters)
+    ok = o["conv"].bool()
+    sel = idx[ok]
+    if sel.numel():
+        n = tab["n"]
+        w = torch.tensor([128, 64, 32, 16, 8, 4, 2, 1], dtype=torch.int32, device=dev)
+        packed = (o["bits"][ok][:, :n // 8 * 8].view(-1, n // 8, 8).int() * w).sum(-1)
+        out["hard"][sel, :n // 8] = packed.to(torch.uint8)
+        out["conv"][sel] = 1
+        out["bad"][sel] = 0
+    return near[ok.cpu().numpy()]

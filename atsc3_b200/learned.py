@@ -240,9 +240,12 @@ def load_weights(path, device="cuda"):
 
 def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
           channel="awgn", seed=1, bf16=False, log_every=50, resume=None,
-          device="cuda"):
+          device="cuda", depths=None):
     """Adam on (alpha, beta) of the unrolled decoder; returns (alpha, beta,
-    history).  Fresh seeded blocks every step."""
+    history).  Fresh seeded blocks every step.  depths: None (the loss is the
+    BCE of the output after all `iters` iterations) or a list of unrolled
+    depths t <= iters whose output BCEs are averaged (each depth uses the
+    first t rows of the weights), which rewards being right early."""
     torch = _torch()
     from . import synth
     code = WmsCode(rate, n, device)
@@ -262,8 +265,13 @@ def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
     hist = []
     for step in range(start, start + steps):
         lam, cw = make_batch(tx, gen, nblk, esn0[0], esn0[1], channel, device)
-        out = WeightedMinSum.apply(lam, alpha, beta, code, bf16)
-        loss = bce_loss(out, cw)
+        if depths:
+            loss = sum(bce_loss(WeightedMinSum.apply(lam, alpha[:t], beta[:t],
+                                                     code, bf16), cw)
+                       for t in depths) / len(depths)
+        else:
+            out = WeightedMinSum.apply(lam, alpha, beta, code, bf16)
+            loss = bce_loss(out, cw)
         opt.zero_grad()
         loss.backward()
         opt.step()
@@ -274,7 +282,7 @@ def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
     manifest = {"rate": rate, "n": n, "mod": mod, "iters": iters,
                 "buckets": [int(x) for x in code.buckets], "seed": seed,
                 "step": start + steps, "esn0": list(esn0), "channel": channel,
-                "bf16": bool(bf16)}
+                "bf16": bool(bf16), "depths": list(depths) if depths else None}
     return alpha.detach(), beta.detach(), hist, manifest
 
 

@@ -72,6 +72,10 @@ SIGNATURES = {
     "atsc3_ldpc_sp_decode": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32,
                                      c_i32, c_vp, c_i64, c_i32, c_i32, c_vp,
                                      c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "atsc3_cpe_workspace": (c_i32, [c_vp]),
+    "atsc3_cpe_correct": (c_i32, [c_vp, c_i64, c_vp, c_i32, c_vp, c_vp, c_i32,
+                                  c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp,
+                                  c_vp]),
     "atsc3_ldpc_layered_plan_create": (c_i32, [c_i32, c_i32, c_i32, c_vp,
                                                c_vp, c_vp]),
     "atsc3_ldpc_layered_plan_destroy": (None, [c_vp]),

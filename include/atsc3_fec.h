@@ -263,6 +263,25 @@ int32_t atsc3_ldpc_sp_decode(const int32_t *cptr, const int32_t *cidx,
                              uint8_t *conv, int32_t *its, int32_t *bad,
                              void *work, void *stream);
 
+/* ---- common phase error correction ----------------------------------------
+ * Replaces lab/m6_cells.py:176-209 cpe_correct (also lab/m9_gpu.py:283-299
+ * GpuBicm.cpe): the pool (ncells complex128, interleaved re/im doubles) is
+ * normalised to unit mean power, then per OFDM symbol s (cells
+ * sym_ptr[s] .. sym_ptr[s+1]-1, contiguous) `iters` times: hard decisions
+ * (region 0: nearest point of alphabet0, m0 points; region 1: alphabet1, m1
+ * points; region 2: dummy[i], the known value; other values are ignored),
+ * c = sum conj(hard) z / max(sum |hard|^2, 1e-12), z /= c.  out: the
+ * corrected pool (complex128); gains: per-symbol total gain (complex128).
+ * work: atsc3_cpe_workspace bytes.  Float64; agreement with the numpy
+ * reference is to rounding (its sums run in other orders). */
+int32_t atsc3_cpe_workspace(int64_t *work_bytes);
+int32_t atsc3_cpe_correct(const double *pool, int64_t ncells,
+                          const int32_t *sym_ptr, int32_t nsym,
+                          const uint8_t *region, const double *alphabet0,
+                          int32_t m0, const double *alphabet1, int32_t m1,
+                          const double *dummy, int32_t iters, double *out,
+                          double *gains, void *work, void *stream);
+
 /* ---- layered decoder for the A/322 Type B codes ----------------------------
  * Layered normalised min-sum: the Q block rows are the layers, the posterior
  * is updated in place after each layer, syndrome before the first and after

@@ -554,3 +554,63 @@ def near_miss_llr(rate, n, nblk, mu, seed):
     cw = ldpc_encode(info, rate, n)
     lam = (1.0 - 2.0 * cw) * mu + rng.standard_normal(cw.shape) * np.sqrt(2.0 * mu)
     return lam.astype(np.float32), cw
+
+
+# ---------------------------------------------------------------------------
+# common phase error correction (checker of csrc/cpe.cu)
+# ---------------------------------------------------------------------------
+
+def cpe_correct(pool, symbol_of, alphabets, region, dummy_values, iters=3):
+    """Per-OFDM-symbol decision-directed complex gain, lab/m6_cells.py:176-209:
+    normalise the pool to unit mean power, then per symbol `iters` times:
+    hard decisions (nearest point of the cell's region alphabet, region 2 =
+    known dummy values), c = <hard, z> / max(<hard, hard>, 1e-12), z /= c.
+    Returns (out complex128, {symbol: total gain})."""
+    out = pool / np.sqrt(np.mean(np.abs(pool) ** 2))
+    gains = {}
+    for sym in np.unique(symbol_of):
+        m = np.flatnonzero(symbol_of == sym)
+        z = out[m]
+        r = region[m]
+        c_tot = 1.0 + 0j
+        for _ in range(iters):
+            hard = np.empty_like(z)
+            for rid, pts in enumerate(alphabets):
+                sel = r == rid
+                if sel.any():
+                    d = np.abs(z[sel][:, None] - pts[None, :])
+                    hard[sel] = pts[d.argmin(1)]
+            sel = r == 2
+            if sel.any():
+                hard[sel] = dummy_values[m[sel]]
+            c = np.vdot(hard, z) / max(np.vdot(hard, hard).real, 1e-12)
+            z = z / c
+            c_tot *= c
+        out[m] = z
+        gains[int(sym)] = complex(c_tot)
+    return out, gains
+
+
+def cpe_pool(nsym, per_sym, mods, seed, esn0_db=18.0):
+    """Seeded synthetic cell pool for the CPE checks: per symbol a block of
+    region-0 cells (alphabet mods[0]), region-1 cells (mods[1]) and known
+    +-1 dummy cells, each symbol rotated by its own complex gain, AWGN.
+    Returns (pool, symbol_of, alphabets, region, dummy_values)."""
+    rng = np.random.default_rng(seed)
+    alph = [np.asarray(C.points_for(m, r), np.complex128) for m, r in mods]
+    n = nsym * per_sym
+    symbol_of = np.repeat(np.arange(nsym), per_sym)
+    region = rng.choice(np.array([0, 0, 0, 1, 2], np.uint8), n)
+    x = np.empty(n, np.complex128)
+    for rid in (0, 1):
+        sel = region == rid
+        x[sel] = alph[rid][rng.integers(0, len(alph[rid]), sel.sum())]
+    dummy = np.zeros(n, np.complex128)
+    sel = region == 2
+    dummy[sel] = 1.0 - 2.0 * rng.integers(0, 2, sel.sum())
+    x[sel] = dummy[sel]
+    g = (1.0 + 0.1 * rng.standard_normal(nsym)) * np.exp(1j * rng.uniform(-0.3, 0.3, nsym))
+    n0 = 10 ** (-esn0_db / 10.0)
+    nz = (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * np.sqrt(n0 / 2)
+    pool = x * g[symbol_of] * 1.7 + nz
+    return pool, symbol_of, alph, region, dummy

@@ -1,0 +1,65 @@
+"""GPU exact sum-product (csrc/sp.cu) against the oracle on the golden
+near-miss cases: convergence, iteration, unsatisfied count and hard
+decisions equal (messages agree to float64 rounding: CUDA's tanh/log/exp/
+atanh are not the host libm's, so the comparison is on decisions)."""
+import numpy as np
+import pytest
+
+import oracle
+from atsc3_b200 import codes as C
+from test_sp_oracle import cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(cases()))
+def test_gpu_sum_product_matches_oracle(name):
+    import torch
+    from atsc3_b200 import ldpc as LDPC
+    c = cases()[name]
+    n = c["n"]
+    lam, cw = oracle.near_miss_llr(c["rate"], n, c["nblk"], c["mu"], c["seed"])
+    tabs = C.csr(c["rate"], n)
+    tab = LDPC.sp_tables(tabs, n)
+    o = LDPC.sp_decode(tab, torch.from_numpy(lam.astype(np.float64)).cuda(),
+                       iters=c["iters"])
+    torch.cuda.synchronize()
+    assert o["conv"].cpu().numpy().astype(bool).tolist() == c["conv"]
+    assert o["its"].cpu().numpy().tolist() == c["its"]
+    assert o["bad"].cpu().numpy().tolist() == c["bad"]
+    want = oracle.sum_product(lam, tabs, n, iters=c["iters"])[0]
+    assert np.array_equal(o["bits"].cpu().numpy(), want)
+
+
+def test_sum_product_dropin_signature():
+    from atsc3_b200 import ldpc as LDPC
+    c = cases()["sp_4_15"]
+    lam, cw = oracle.near_miss_llr(c["rate"], c["n"], c["nblk"], c["mu"], c["seed"])
+    bits, conv, its, bad = LDPC.sum_product_decode_batch(
+        lam, C.parity_check(c["rate"], c["n"]), c["n"], iters=c["iters"])
+    assert bits.dtype == np.uint8 and conv.dtype == bool
+    assert conv.tolist() == c["conv"] and its.tolist() == c["its"]
+    assert np.array_equal(bits, cw)
+
+
+def test_rescue_replaces_min_sum_failures():
+    """Blocks min-sum leaves unconverged get the sum-product; those it
+    closes carry the sum-product's hard decisions (packed) and conv = 1."""
+    import torch
+    from atsc3_b200 import ldpc as LDPC
+    c = cases()["sp_8_15_a"]
+    n = c["n"]
+    lam, cw = oracle.near_miss_llr(c["rate"], n, c["nblk"], c["mu"], c["seed"])
+    tabs = C.csr(c["rate"], n)
+    plan = LDPC.plan_for(c["rate"], n)
+    x = torch.from_numpy(lam).cuda()
+    o = LDPC.decode_flood(plan, x, iters=50, want_hard=True)
+    assert not o["conv"].bool().any()                # min-sum fails them all
+    got = LDPC.rescue_near_misses(LDPC.sp_tables(tabs, n), x, o,
+                                  near_max=100000, max_blocks=8, iters=c["iters"])
+    assert sorted(got.tolist()) == [b for b, ok in enumerate(c["conv"]) if ok]
+    sp_bits = oracle.sum_product(lam, tabs, n, iters=c["iters"])[0]
+    hard = o["hard"].cpu().numpy()[:, :n // 8]
+    for b in got:
+        assert np.array_equal(hard[b], np.packbits(sp_bits[b]))
+        assert int(o["conv"][b]) == 1 and int(o["bad"][b]) == 0
