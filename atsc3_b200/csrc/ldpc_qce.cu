@@ -347,32 +347,29 @@ __device__ __forceinline__ float qce_var_exact(float *col, int s0, float li,
   return tot;
 }
 
-// Variable phase of one bit for a column of d edges (any d >= 1): byte
-// offsets walk the slots from s0 with a wrap at d (unsigned min trick:
-// off - span underflows while off < span).
+// Variable phase of one bit for a column of d edges (any d >= 1).  The sum
+// runs over slots s0 .. d-1, then 0 .. s0-1; inside a warp the lanes' s0
+// differ little, so with lo/hi = the warp's least/greatest s0 the common
+// parts [hi, d) and [0, lo) are summed unconditionally and only [lo, hi)
+// needs a per-lane choice (adding -0.0 leaves a float sum unchanged).
+// The order of additions is each lane's own, so the sum is exact.
 template <bool TORCH>
 __device__ __forceinline__ float qce_var_generic(float *col, int d, int s0,
                                                  float li, bool mv) {
-  const char *cb = reinterpret_cast<const char *>(col);
-  const uint32_t span = (uint32_t)d * (uint32_t)ESLOT;
-  uint32_t off = (uint32_t)(s0 < d ? s0 : 0) * (uint32_t)ESLOT;
+  const int lo = (int)__reduce_min_sync(0xffffffffu, (uint32_t)s0);
+  const int hi = (int)__reduce_max_sync(0xffffffffu, (uint32_t)s0);
   float acc = TORCH ? li : 0.f;
-  int t = 0;
-  for (; t + 4 <= d; t += 4) {
-    float v[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      v[u] = *reinterpret_cast<const float *>(cb + off);
-      off += ESLOT;
-      off = min(off, off - span);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) acc = __fadd_rn(acc, v[u]);
+  for (int i = lo; i < hi; ++i) {                  // own tail, first part
+    const float m = col[i * EZ];
+    acc = __fadd_rn(acc, i >= s0 ? m : -0.f);
   }
-  for (; t < d; ++t) {
-    acc = __fadd_rn(acc, *reinterpret_cast<const float *>(cb + off));
-    off += ESLOT;
-    off = min(off, off - span);
+#pragma unroll 4
+  for (int i = hi; i < d; ++i) acc = __fadd_rn(acc, col[i * EZ]);
+#pragma unroll 4
+  for (int i = 0; i < lo; ++i) acc = __fadd_rn(acc, col[i * EZ]);
+  for (int i = lo; i < hi; ++i) {                  // own head, last part
+    const float m = col[i * EZ];
+    acc = __fadd_rn(acc, i < s0 ? m : -0.f);
   }
   const float tot = TORCH ? acc : __fadd_rn(li, acc);
   if (mv) {
