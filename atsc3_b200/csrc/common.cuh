@@ -103,6 +103,12 @@ __device__ __forceinline__ void dsmem_st_u32(uint32_t a, uint32_t v) {
                : "memory");
 }
 
+// atomic add into (possibly another CTA's) shared memory of the cluster
+__device__ __forceinline__ void dsmem_red_add_u32(uint32_t a, uint32_t v) {
+  asm volatile("red.shared::cluster.add.u32 [%0], %1;" :: "r"(a), "r"(v)
+               : "memory");
+}
+
 template <typename T> __device__ __forceinline__ T dsmem_ld(uint32_t a);
 template <> __device__ __forceinline__ float dsmem_ld<float>(uint32_t a) {
   return dsmem_ld_f32(a);

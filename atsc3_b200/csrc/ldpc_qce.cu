@@ -424,6 +424,13 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
   }
   if (upd) {
     const float inf = __int_as_float(0x7f800000);
+    // min1/min2 with min/max only: the reference's strict-< update
+    // (ldpc_kernel.c:121-126) gives min2 = min(min2, max(min1, mag)),
+    // min1 = min(min1, mag), including ties
+    // Rows of up to 11 edges keep their values to the end and pick each
+    // message by comparing |t| with min1; longer rows track the first
+    // minimum's position instead, so the values can die early (registers).
+    constexpr bool BY_VALUE = D <= 11;
     float min1 = inf, min2 = inf;
     uint32_t first = 0;
     MASK sv = 0;
@@ -437,10 +444,9 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
         ng = ng && on;
       }
       sv |= ng ? ((MASK)1 << j) : (MASK)0;
-      const bool lt = mag < min1;
-      min2 = lt ? min1 : fminf(min2, mag);
-      first = lt ? (uint32_t)j : first;
-      min1 = lt ? mag : min1;
+      if constexpr (!BY_VALUE) first = mag < min1 ? (uint32_t)j : first;
+      min2 = fminf(min2, fmaxf(min1, mag));
+      min1 = fminf(min1, mag);
     }
     constexpr bool WIDE = sizeof(MASK) > 4;
     int par;
@@ -466,9 +472,15 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
     if constexpr (FULL) all = (D >= 8 * (int)sizeof(MASK)) ? ~(MASK)0 : (((MASK)1 << D) - 1);
     else all = live;
     const MASK neg = par ? (sv ^ all) : sv;          // message signs
+    // the edge holding the first minimum gets min2, every other min1; an
+    // edge whose magnitude equals min1 but is not the first one has
+    // min2 == min1, so testing |t| == min1 picks the same value
 #pragma unroll
     for (int j = 0; j < D; ++j) {
-      const uint32_t mg = ((uint32_t)j == first) ? ub : ua;
+      bool take2;
+      if constexpr (BY_VALUE) take2 = fabsf(t[j]) == min1;
+      else take2 = (uint32_t)j == first;
+      const uint32_t mg = take2 ? ub : ua;
       dsmem_st_u32(ad[j], mg | (((uint32_t)(neg >> j) & 1u) << 31));
     }
   }
@@ -484,8 +496,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const int rank = (int)cluster_ctarank();
   const int CL = (int)cluster_nctarank();
   const uint32_t *bm = reinterpret_cast<const uint32_t *>(smem);
+  // syndrome counters (2, alternating iterations); junk word at [40]
   int *part = reinterpret_cast<int *>(smem + a.part_off);
-  int *sbad = part + 32;
   uint2 *rtab = reinterpret_cast<uint2 *>(smem + a.rt_off);
   MASK *rinfo = reinterpret_cast<MASK *>(smem + a.ri_off);
   uint4 *itab = reinterpret_cast<uint4 *>(smem + a.ct_off);
@@ -533,7 +545,10 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
     const int4 v = __ldg(a.itab + i0 + q);
     itab[q] = make_uint4((uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z, (uint32_t)v.w);
   }
-  if (tid == 0) *sbad = 0;
+  if (tid == 0) {
+    part[0] = 0;
+    part[1] = 0;
+  }
   __syncthreads();
 
   // the absent wrap entry (last parity column, bit 359, its wrap slot) is
@@ -561,11 +576,13 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         if (lane < CL) dsmem_st_u32(bm_peer + (iw.w + sub) * 4u, hb);
       }
     }
-    __syncthreads();
-    cluster_sync_all();
+    cluster_sync_all();      // (a cluster barrier also orders this CTA)
 
     for (int it = 0;; ++it) {
       const bool upd = it < a.iters;   // the last pass only needs the syndrome
+      // the count of the previous iteration has been read by every thread
+      // (a barrier ago); its slot is reused two iterations later
+      if (tid == 0 && it > 0) part[(it - 1) & 1] = 0;
       // ---------------- check phase ----------------------------------------
       int mybad = 0;
       for (int w = warp; w < ncitems; w += nwarps) {
@@ -590,17 +607,14 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         }
         mybad += syn;
       }
+      // unsatisfied checks: every warp adds its count into the counter of
+      // every CTA of the cluster, so after the barrier each CTA holds the total
       mybad = __reduce_add_sync(0xffffffffu, mybad);
-      if (lane == 0 && mybad) atomicAdd(sbad, mybad);
-      __syncthreads();
-      if (tid < CL)
-        dsmem_st_u32(dsmem_map(part_sa + (uint32_t)(((it & 1) * 16 + rank) * 4),
-                               (uint32_t)tid),
-                     (uint32_t)*sbad);
+      if (lane < CL && mybad)
+        dsmem_red_add_u32(dsmem_map(part_sa + (uint32_t)((it & 1) * 4), (uint32_t)lane),
+                          (uint32_t)mybad);
       cluster_sync_all();
-      int badct = 0;
-      for (int q = 0; q < CL; ++q) badct += part[(it & 1) * 16 + q];
-      if (tid == 0) *sbad = 0;
+      const int badct = part[it & 1];
       const bool done = (badct == 0) && (!TORCH || it > 0);
       if (done || it >= a.iters) {
         // outputs from this CTA's bitmap replica (complete in every CTA):
@@ -631,9 +645,12 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           a.bad[b] = done ? 0 : badct;
         }
         // every CTA has read its replica before the next codeword's prologue
-        // writes the replicas of the whole cluster
-        __syncthreads();
+        // writes the replicas of the whole cluster; both counters start at 0
         cluster_sync_all();
+        if (tid == 0) {
+          part[0] = 0;
+          part[1] = 0;
+        }
         break;
       }
       // ---------------- variable phase (local) -----------------------------
@@ -697,11 +714,9 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           if (lane < CL) dsmem_st_u32(bm_peer + iw.w * 4u, hb);
         }
       }
-      __syncthreads();
       cluster_sync_all();
     }
   }
-  __syncthreads();
   cluster_sync_all();
 }
 

@@ -480,3 +480,72 @@ def rescue_near_misses(tab, lam, out, near_max=1500, max_blocks=8, iters=100):
         out["conv"][sel] = 1
         out["bad"][sel] = 0
     return near[ok.cpu().numpy()]
+
+
+# ---------------------------------------------------------------------------
+# the alpha ladder
+# ---------------------------------------------------------------------------
+
+ALPHA_LADDER = (1.0, 0.85, 0.75)
+
+
+def ladder_decode(plan, llr, ladder=ALPHA_LADDER, iters=50, semantics="kernel",
+                  want_bits=True, threads=0):
+    """Normalised min-sum with the reference's alpha ladder
+    (``lab/m6_bicm.py:313,341-355`` ``decode_llr``; batched as
+    ``lab/m9_fast.py:843-885`` / ``lab/m44_ldm.py:2497-2526``): every block
+    is decoded at the first alpha; the blocks that did not converge are
+    decoded again at the next one, and so on.  A block keeps the first rung
+    that converges, else the rung with the fewest unsatisfied checks (ties
+    keep the earlier rung).  Returns device tensors bits (if want_bits),
+    hard (packed), conv, its, bad, alpha (the rung kept).  Each rung after the
+    first reads the convergence flags on the host (as the reference does)."""
+    torch = _torch()
+    nb, n = llr.shape
+    dev = llr.device
+    out = {"hard": torch.zeros((nb, (n + 31) // 32 * 4), dtype=torch.uint8, device=dev),
+           "conv": torch.zeros(nb, dtype=torch.uint8, device=dev),
+           "its": torch.zeros(nb, dtype=torch.int32, device=dev),
+           "bad": torch.full((nb,), 1 << 30, dtype=torch.int32, device=dev),
+           "alpha": torch.full((nb,), -1.0, dtype=torch.float32, device=dev)}
+    if want_bits:
+        out["bits"] = torch.zeros((nb, n), dtype=torch.uint8, device=dev)
+    todo = torch.arange(nb, device=dev)
+    for a in ladder:
+        if todo.numel() == 0:
+            break
+        sub = llr if todo.numel() == nb else llr.index_select(0, todo)
+        o = decode_flood(plan, sub, iters=iters, alpha=a, semantics=semantics,
+                         want_bits=want_bits, want_hard=True, threads=threads)
+        c = o["conv"].bool()
+        take = c | (o["bad"] < out["bad"][todo])
+        sel = todo[take]
+        for k in ("hard", "conv", "its", "bad") + (("bits",) if want_bits else ()):
+            out[k][sel] = o[k][take]
+        out["alpha"][sel] = float(a)
+        todo = todo[~c]
+    return out
+
+
+def ldpc_batch(lam2d, rate, n, iters=50, alpha=None, ladder=ALPHA_LADDER,
+               sp_rescue=None):
+    """Host-array form of ``lab/m44_ldm.py:2497`` ``ldpc_batch``: numpy
+    (bits uint8, conv bool, bad int32) of (nblk, n) LLRs decoded with the
+    single ``alpha`` if given, else the alpha ladder; ``sp_rescue`` (a dict
+    of rescue_near_misses arguments) adds the near-miss sum-product, as the
+    reference does when ATSC3_LDM_SP is set."""
+    torch = _torch()
+    plan = plan_for(rate, n)
+    x = torch.from_numpy(np.ascontiguousarray(lam2d, np.float32)).cuda()
+    o = ladder_decode(plan, x, ladder=(alpha,) if alpha else tuple(ladder),
+                      iters=iters, want_bits=True)
+    if sp_rescue:
+        got = rescue_near_misses(sp_tables(C.csr(rate, n), n), x, o, **sp_rescue)
+        if len(got):       # unpack the rescued blocks' packed decisions
+            idx = torch.from_numpy(got.astype(np.int64)).cuda()
+            h = o["hard"].index_select(0, idx)[:, :n // 8]
+            bits = ((h.unsqueeze(-1) >> torch.arange(7, -1, -1, device=h.device)) & 1)
+            o["bits"][idx] = bits.reshape(len(got), -1)[:, :n].to(torch.uint8)
+    torch.cuda.synchronize()
+    return (o["bits"].cpu().numpy(), o["conv"].cpu().numpy().astype(bool),
+            o["bad"].cpu().numpy())

@@ -29,11 +29,14 @@ class FecPipeline:
     rescue: None (off, as the reference's default) or a dict of
     ldpc.rescue_near_misses arguments (near_max, max_blocks, iters): blocks
     min-sum leaves a few checks short get the exact sum-product before BCH
-    (this adds a host read of the flags)."""
+    (this adds a host read of the flags).  ladder: None (the single `alpha`,
+    as the configs pin it) or a tuple of alphas tried in turn on the blocks
+    that did not converge (ldpc.ladder_decode; the reference's default
+    ladder is ldpc.ALPHA_LADDER)."""
 
     def __init__(self, n, mod, rate, iters=50, alpha=0.75, semantics="kernel",
                  cluster=0, threads=0, device="cuda", kind="auto",
-                 rescue=None):
+                 rescue=None, ladder=None):
         torch = _torch()
         self.n, self.mod, self.rate = int(n), mod, rate
         self.nb = C.MOD_BITS[mod]
@@ -47,6 +50,7 @@ class FecPipeline:
         with torch.cuda.device(self.device):
             self.plan = LDPC.plan_for(rate, n, "float32", cluster, kind=kind)
             self.rescue = dict(rescue) if rescue else None
+            self.ladder = tuple(ladder) if ladder else None
             self.sp_tab = (LDPC.sp_tables(C.csr(rate, n), n, self.device)
                            if self.rescue else None)
         self._ws = {}
@@ -85,16 +89,27 @@ class FecPipeline:
             ws.update(out)
         DM.demap(cells, self.mod, self.rate, sigma2=sigma2, n=self.n,
                  deinterleave=True, out=ws["lam"])
-        LDPC.decode_flood(self.plan, ws["lam"], iters=iters or self.iters,
-                          alpha=self.alpha if alpha is None else alpha,
-                          semantics=self.semantics, want_bits=False,
-                          want_hard=True, threads=self.threads, out=ws,
-                          weights=weights)
+        self._ldpc(ws, iters, alpha, weights)
         if self.rescue:
             LDPC.rescue_near_misses(self.sp_tab, ws["lam"], ws, **self.rescue)
         BCH.bch_check(ws["hard"], self.kldpc, self.n, self.kpayload,
                       want_payload=True, out=ws)
         return ws
+
+    def _ldpc(self, ws, iters, alpha, weights):
+        if self.ladder and alpha is None and weights is None:
+            o = LDPC.ladder_decode(self.plan, ws["lam"], ladder=self.ladder,
+                                   iters=iters or self.iters,
+                                   semantics=self.semantics, want_bits=False,
+                                   threads=self.threads)
+            for k in ("hard", "conv", "its", "bad"):
+                ws[k].copy_(o[k])
+            return
+        LDPC.decode_flood(self.plan, ws["lam"], iters=iters or self.iters,
+                          alpha=self.alpha if alpha is None else alpha,
+                          semantics=self.semantics, want_bits=False,
+                          want_hard=True, threads=self.threads, out=ws,
+                          weights=weights)
 
     def decode_stream(self, stream, ti, sigma2, iters=None, alpha=None,
                       out=None, weights=None):
@@ -110,11 +125,9 @@ class FecPipeline:
             ws.update(out)
         TI.demap_deinterleave(stream, ti, self.mod, self.rate, self.n,
                               sigma2=sigma2, out=ws["lam"])
-        LDPC.decode_flood(self.plan, ws["lam"], iters=iters or self.iters,
-                          alpha=self.alpha if alpha is None else alpha,
-                          semantics=self.semantics, want_bits=False,
-                          want_hard=True, threads=self.threads, out=ws,
-                          weights=weights)
+        self._ldpc(ws, iters, alpha, weights)
+        if self.rescue:
+            LDPC.rescue_near_misses(self.sp_tab, ws["lam"], ws, **self.rescue)
         BCH.bch_check(ws["hard"], self.kldpc, self.n, self.kpayload,
                       want_payload=True, out=ws)
         return ws

@@ -614,3 +614,29 @@ def cpe_pool(nsym, per_sym, mods, seed, esn0_db=18.0):
     nz = (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * np.sqrt(n0 / 2)
     pool = x * g[symbol_of] * 1.7 + nz
     return pool, symbol_of, alph, region, dummy
+
+
+def ladder(llr, tables, n, alphas=(1.0, 0.85, 0.75), iters=50):
+    """The alpha ladder of lab/m9_fast.py:843-885 / lab/m44_ldm.py:2497-2526
+    over the oracle's flooding decoder: blocks that did not converge are
+    decoded again at the next alpha; a block keeps the first converged rung,
+    else the rung with the fewest unsatisfied checks.  Returns (bits, conv,
+    its, bad, alpha_kept)."""
+    llr = np.asarray(llr, np.float32)
+    nb = llr.shape[0]
+    bits = np.zeros((nb, n), np.uint8)
+    conv = np.zeros(nb, bool)
+    its = np.zeros(nb, np.int32)
+    bad = np.full(nb, 1 << 30, np.int32)
+    kept = np.full(nb, -1.0, np.float32)
+    todo = np.arange(nb)
+    for a in alphas:
+        if not len(todo):
+            break
+        b, c, it, d = flood(llr[todo], tables, n, iters=iters, alpha=a)
+        take = c | (d < bad[todo])
+        sel = todo[take]
+        bits[sel], conv[sel], its[sel], bad[sel] = b[take], c[take], it[take], d[take]
+        kept[sel] = a
+        todo = todo[~c]
+    return bits, conv, its, bad, kept

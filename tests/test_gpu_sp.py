@@ -63,3 +63,46 @@ def test_rescue_replaces_min_sum_failures():
     for b in got:
         assert np.array_equal(hard[b], np.packbits(sp_bits[b]))
         assert int(o["conv"][b]) == 1 and int(o["bad"][b]) == 0
+
+
+@pytest.mark.parametrize("kind", ["auto", "csr"])
+def test_gpu_ladder_matches_oracle(kind):
+    """The alpha ladder on the GPU keeps, per block, the same rung, bits,
+    convergence, iterations and unsatisfied count as the oracle ladder
+    (which reproduces the reference's, tests/test_ladder_oracle.py)."""
+    import torch
+    from atsc3_b200 import ldpc as LDPC
+    from test_ladder_oracle import golden
+    g = golden()
+    for name, c in sorted(g["cases"].items()):
+        n = c["n"]
+        lam, cw = oracle.near_miss_llr(c["rate"], n, c["nblk"], c["mu"], c["seed"])
+        want = oracle.ladder(lam, C.csr(c["rate"], n), n, alphas=tuple(g["ladder"]),
+                             iters=c["iters"])
+        plan = LDPC.plan_for(c["rate"], n, kind=kind)
+        o = LDPC.ladder_decode(plan, torch.from_numpy(lam).cuda(),
+                               ladder=tuple(g["ladder"]), iters=c["iters"])
+        assert np.array_equal(o["bits"].cpu().numpy(), want[0]), name
+        assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
+        assert o["its"].cpu().numpy().tolist() == want[2].tolist()
+        assert o["bad"].cpu().numpy().tolist() == want[3].tolist()
+        assert np.array_equal(o["alpha"].cpu().numpy(), want[4])
+        assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
+                              np.packbits(want[0], axis=1))
+
+
+def test_pipeline_ladder_and_dropin():
+    """FecPipeline(ladder=...) decodes with the ladder; the host-array
+    ldpc_batch drop-in returns the oracle ladder's (bits, conv, bad)."""
+    import torch
+    from atsc3_b200 import ldpc as LDPC
+    from test_ladder_oracle import golden
+    g = golden()
+    c = g["cases"]["ladder_6_15"]
+    n = c["n"]
+    lam, cw = oracle.near_miss_llr(c["rate"], n, c["nblk"], c["mu"], c["seed"])
+    want = oracle.ladder(lam, C.csr(c["rate"], n), n, alphas=tuple(g["ladder"]),
+                         iters=c["iters"])
+    bits, conv, bad = LDPC.ldpc_batch(lam, c["rate"], n, iters=c["iters"])
+    assert np.array_equal(bits, want[0])
+    assert conv.tolist() == want[1].tolist() and bad.tolist() == want[3].tolist()
