@@ -12,6 +12,9 @@ callers and gates run on the GPU unchanged:
 * ``m3_ldpc._kernel_lib``           -> ``libatsc3_fec.so`` (same C ABI as
   ``lab/ldpc_kernel.c``, bound with the reference's own argtypes,
   ``lab/m3_ldpc.py:439-446``)
+* ``m16_margin.sum_product_decode_batch``
+                                    -> ``atsc3_b200.ldpc`` (float64 on the GPU)
+* ``m6_cells.cpe_correct``          -> ``atsc3_b200.cpe.cpe_correct``
 
 Pass the already-imported reference modules (any subset); nothing here
 imports the receiver.
@@ -41,9 +44,10 @@ def _kernel_lib_factory():
     return lib
 
 
-def install(m9_gpu=None, m16_demap_fast=None, m9_accel=None, m3_ldpc=None):
+def install(m9_gpu=None, m16_demap_fast=None, m9_accel=None, m3_ldpc=None,
+            m16_margin=None, m6_cells=None):
     """Patch the given reference modules; returns the number of bindings."""
-    from . import bch, demap, ldpc
+    from . import bch, cpe, demap, ldpc
 
     def patch(mod, name, value):
         _SAVED.append((mod, name, getattr(mod, name)))
@@ -59,6 +63,10 @@ def install(m9_gpu=None, m16_demap_fast=None, m9_accel=None, m3_ldpc=None):
     if m3_ldpc is not None:
         lib = _kernel_lib_factory()
         patch(m3_ldpc, "_kernel_lib", lambda: lib)
+    if m16_margin is not None:
+        patch(m16_margin, "sum_product_decode_batch", ldpc.sum_product_decode_batch)
+    if m6_cells is not None:
+        patch(m6_cells, "cpe_correct", cpe.cpe_correct)
     return len(_SAVED)
 
 

@@ -136,3 +136,11 @@ def test_install_rebinds_and_restores():
     I.uninstall()
     assert m9_gpu.GpuMinSum == "ref" and m3._kernel_lib == "ref"
     assert m9a.bch_syndrome == "ref" and m16.demap_llr_fast == "ref"
+    from atsc3_b200 import cpe
+    mg = types.SimpleNamespace(sum_product_decode_batch="ref")
+    ce = types.SimpleNamespace(cpe_correct="ref")
+    assert I.install(m16_margin=mg, m6_cells=ce) == 2
+    assert mg.sum_product_decode_batch is ldpc.sum_product_decode_batch
+    assert ce.cpe_correct is cpe.cpe_correct
+    I.uninstall()
+    assert mg.sum_product_decode_batch == "ref" and ce.cpe_correct == "ref"
