@@ -8,15 +8,21 @@ The reference decodes one PLP configuration at a time (``m9_fast`` and
 ``(n, mod, rate)`` blocks and runs
 
     mixed demap + de-interleave  (atsc3_demap_batch, 256-cell chunks)
-    one persistent LDPC launch   (atsc3_ldpc_batch_decode: clusters pull
+    LDPC, concurrently on forked streams:
+      one edge-buffer quasi-cyclic launch per Type B code it accepts
+                                 (atsc3_ldpc_qce_decode over that code's
+                                  blocks, which sit contiguously inside)
+      one persistent CSR launch for every other block
+                                 (atsc3_ldpc_batch_decode: clusters pull
                                   blocks from a device queue, most work first)
     mixed BCH + descramble        (atsc3_bch_batch)
 
-on one stream.  ``capture()`` records the three launches (and the queue
-reset) into a CUDA graph; ``autotune()`` times the graph for each cluster
-size (1..16 CTAs per codeword, as far as every code of the batch fits) and
+``capture()`` records the launches (queue reset, fork and join included)
+into a CUDA graph; ``autotune()`` times the graph for each cluster size of
+the CSR launch (1..16 CTAs per codeword, as far as every CSR code fits) and
 CTA size (512 or 1024 threads) and keeps the fastest; results are cached per
-batch signature.
+batch signature.  Blocks are stored grouped by decoder; ``load`` takes and
+``results`` returns them in the caller's order.
 """
 from __future__ import annotations
 
@@ -61,15 +67,58 @@ def min_cluster(rate, n):
     raise RuntimeError(f"code {n} {rate} does not fit 16 CTAs")
 
 
-class UnevenBatch:
-    """A fixed list of blocks ``specs = [(n, mod, rate), ...]``."""
+_QCE = {}
 
-    def __init__(self, specs, iters=50, alpha=0.75, device="cuda"):
+
+def qce_plan(rate, n):
+    """The edge-buffer quasi-cyclic plan of a code, or None if that decoder
+    does not take it (Type A codes, two circulants in a block)."""
+    key = (rate, n)
+    if key not in _QCE:
+        p = None
+        if C.ldpc_params(rate, n)[0] == "B":
+            try:
+                p = LDPC.QcePlan(rate, n)
+            except N.FecError as e:
+                if e.rc != -4:
+                    raise
+        _QCE[key] = p
+    return _QCE[key]
+
+
+class UnevenBatch:
+    """A fixed list of blocks ``specs = [(n, mod, rate), ...]``.  hybrid:
+    decode the blocks of Type B codes with the edge-buffer quasi-cyclic
+    decoder (one launch per code, concurrent); False puts every block on the
+    CSR persistent launch."""
+
+    def __init__(self, specs, iters=50, alpha=0.75, device="cuda", hybrid=True):
         torch = _torch()
-        self.specs = [tuple(s) for s in specs]
+        user = [tuple(s) for s in specs]
         self.iters, self.alpha = iters, alpha
         self.dev = torch.device(device)
         d = self.dev
+        # internal order: quasi-cyclic groups (by code), then the CSR blocks
+        with torch.cuda.device(d):
+            qp = {(r, n): (qce_plan(r, n) if hybrid else None)
+                  for n, m, r in user}
+        qcodes = sorted({(r, n) for n, m, r in user if qp[(r, n)] is not None},
+                        key=lambda c: (c[1], c[0]))
+        perm = []
+        for code in qcodes:
+            perm += [i for i, (n, m, r) in enumerate(user) if (r, n) == code]
+        rest = [i for i, (n, m, r) in enumerate(user) if qp[(r, n)] is None]
+        perm += rest
+        self.perm = np.array(perm, np.int64)         # internal -> caller index
+        self.specs = [user[i] for i in perm]
+        self.user_specs = user
+        self.groups = []                             # (plan, first, count, n)
+        first = 0
+        for code in qcodes:
+            cnt = sum(1 for n, m, r in user if (r, n) == code)
+            self.groups.append((qp[code], first, cnt, code[1]))
+            first += cnt
+        self.csr_ids = list(range(first, len(user)))
         nb = len(self.specs)
         self.nblk = nb
         ncell = [C.cells_per_block(n, m) for n, m, r in self.specs]
@@ -133,9 +182,14 @@ class UnevenBatch:
             "chunk_blk": T(chunk_blk, np.int32),
             "chunk_start": T(chunk_start, np.int32),
         }
-        # queue order: most edges first
-        edges = [len(C.csr(r, n)[1]) for n, m, r in self.specs]
-        self.a["order"] = T(np.argsort(-np.asarray(edges), kind="stable"), np.int32)
+        # CSR queue: its blocks, most edges first
+        edges = np.array([len(C.csr(r, n)[1]) for n, m, r in self.specs])
+        ids = np.array(self.csr_ids, np.int64)
+        self.a["order"] = T(ids[np.argsort(-edges[ids], kind="stable")]
+                            if len(ids) else np.zeros(1, np.int64), np.int32)
+        self.ncsr = len(ids)
+        self.hb = hb
+        self.side = [torch.cuda.Stream(d) for _ in range(len(self.groups) + 1)]
         # buffers
         self.cells = torch.empty(int(sum(ncell)), dtype=torch.complex64, device=d)
         self.sigma2 = torch.ones(nb, dtype=torch.float32, device=d)
@@ -148,7 +202,11 @@ class UnevenBatch:
         self.syn = torch.empty((nb, 6), dtype=torch.int32, device=d)
         self.ok = torch.empty(nb, dtype=torch.uint8, device=d)
         self.counter = torch.zeros(1, dtype=torch.int32, device=d)
-        self.codes = sorted({(r, n) for n, m, r in self.specs})
+        # CSR plans for the codes of the CSR blocks (one if there are none,
+        # so the launch configuration stays defined)
+        self.codes = sorted({(self.specs[b][2], self.specs[b][0])
+                             for b in self.csr_ids}) or [(self.specs[0][2],
+                                                          self.specs[0][0])]
         self.cl_min = max(min_cluster(r, n) for r, n in self.codes)
         self.graph = None
         self.config = None
@@ -156,19 +214,21 @@ class UnevenBatch:
 
     # -- inputs -----------------------------------------------------------
     def load(self, cells_list, sigma2_list):
-        """Copy per-block cells (complex64 tensors) and scalar sigma2."""
+        """Copy per-block cells (complex64 tensors) and scalar sigma2, in the
+        caller's block order."""
         torch = _torch()
-        for b, (c, s) in enumerate(zip(cells_list, sigma2_list)):
+        for b, u in enumerate(self.perm):
             o = int(self.cell_off[b])
-            self.cells[o:o + self.ncell[b]].copy_(c.reshape(-1))
-        self.sigma2.copy_(torch.as_tensor(np.asarray(sigma2_list, np.float32)))
+            self.cells[o:o + self.ncell[b]].copy_(cells_list[u].reshape(-1))
+        s2 = np.asarray(sigma2_list, np.float32)[self.perm]
+        self.sigma2.copy_(torch.as_tensor(s2))
 
     # -- launch configuration ----------------------------------------------
     def set_config(self, cluster, threads):
         torch = _torch()
         self.plans = [csr_plan(r, n, cluster) for r, n in self.codes]
         idx = {code: i for i, code in enumerate(self.codes)}
-        bplan = [idx[(r, n)] for n, m, r in self.specs]
+        bplan = [idx.get((r, n), 0) for n, m, r in self.specs]   # CSR blocks only
         self.a["bplan"] = torch.tensor(bplan, dtype=torch.int32, device=self.dev)
         nbytes = ctypes.c_int64()
         N.call("atsc3_ldpc_batch_desc_bytes", len(self.plans), ctypes.byref(nbytes))
@@ -189,6 +249,7 @@ class UnevenBatch:
         a = self.a
         zf = torch.view_as_real(self.cells)
         self.counter.zero_()
+        main = torch.cuda.current_stream(self.dev) if stream is None else None
         N.call("atsc3_demap_batch", zf.data_ptr(), a["cell_off"].data_ptr(),
                a["ncell"].data_ptr(), a["nbits"].data_ptr(),
                self.t_pts.data_ptr(), a["pts_off"].data_ptr(),
@@ -196,13 +257,31 @@ class UnevenBatch:
                a["lq_off"].data_ptr(), self.llr.data_ptr(),
                a["llr_off"].data_ptr(), a["chunk_blk"].data_ptr(),
                a["chunk_start"].data_ptr(), self.nchunks, self.max_nbits, st)
-        N.call("atsc3_ldpc_batch_decode", self.desc.data_ptr(), self.cluster,
-               self.smem, a["bplan"].data_ptr(), a["order"].data_ptr(),
-               self.nblk, self.llr.data_ptr(), a["llr_off"].data_ptr(),
-               self.hard.data_ptr(), a["hard_off"].data_ptr(),
-               self.conv.data_ptr(), self.its.data_ptr(), self.bad.data_ptr(),
-               int(self.iters), float(self.alpha), self.counter.data_ptr(),
-               self.threads, 0, st)
+        # fork: one stream per quasi-cyclic group and one for the CSR queue
+        if main is not None and self.groups:
+            for s_ in self.side:
+                s_.wait_stream(main)
+        for gi, (plan, first, cnt, n) in enumerate(self.groups):
+            gst = self.side[gi].cuda_stream if main is not None else st
+            N.call("atsc3_ldpc_qce_decode", plan.handle,
+                   self.llr.data_ptr() + 4 * int(self.llr_off[first]), n, cnt,
+                   int(self.iters), float(self.alpha), 0, None, 0,
+                   self.hard.data_ptr() + int(self.hard_off[first]),
+                   self.hb[first], self.conv.data_ptr() + first,
+                   self.its.data_ptr() + 4 * first, self.bad.data_ptr() + 4 * first,
+                   0, gst)
+        if self.ncsr:
+            cst = self.side[-1].cuda_stream if (main is not None and self.groups) else st
+            N.call("atsc3_ldpc_batch_decode", self.desc.data_ptr(), self.cluster,
+                   self.smem, a["bplan"].data_ptr(), a["order"].data_ptr(),
+                   self.ncsr, self.llr.data_ptr(), a["llr_off"].data_ptr(),
+                   self.hard.data_ptr(), a["hard_off"].data_ptr(),
+                   self.conv.data_ptr(), self.its.data_ptr(), self.bad.data_ptr(),
+                   int(self.iters), float(self.alpha), self.counter.data_ptr(),
+                   self.threads, 0, cst)
+        if main is not None and self.groups:
+            for s_ in self.side:
+                main.wait_stream(s_)
         N.call("atsc3_bch_batch", self.hard.data_ptr(), a["hard_off"].data_ptr(),
                a["kldpc"].data_ptr(), self.t_rt.data_ptr(), a["rt_off"].data_ptr(),
                self.t_scr.data_ptr(), a["kpay"].data_ptr(),
@@ -228,7 +307,7 @@ class UnevenBatch:
         self.graph.replay()
 
     def signature(self):
-        return (tuple(sorted(self.specs)), self.iters)
+        return (tuple(sorted(self.specs)), self.iters, len(self.groups))
 
     def autotune(self, reps=3, clusters=None, threads=(512, 1024)):
         """Time the captured graph for each (cluster, threads) and keep the
@@ -268,12 +347,12 @@ class UnevenBatch:
     def results(self):
         """Per block: payload bytes, conv, its, bad, ok (numpy)."""
         pay = self.payload.cpu().numpy()
-        out = []
+        out = [None] * self.nblk
         conv, its, bad, ok = (t.cpu().numpy() for t in (self.conv, self.its,
                                                         self.bad, self.ok))
         for b in range(self.nblk):
             o = int(self.pay_off[b])
-            out.append({"payload": pay[o:o + self.kpays[b] // 8],
-                        "conv": int(conv[b]), "its": int(its[b]),
-                        "bad": int(bad[b]), "ok": int(ok[b])})
+            out[int(self.perm[b])] = {"payload": pay[o:o + self.kpays[b] // 8],
+                                      "conv": int(conv[b]), "its": int(its[b]),
+                                      "bad": int(bad[b]), "ok": int(ok[b])}
         return out

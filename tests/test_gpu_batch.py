@@ -32,14 +32,18 @@ def _blocks(torch, specs, seed=5):
     return cells, s2s
 
 
-def test_uneven_batch_equals_per_modcod_pipelines():
+@pytest.mark.parametrize("hybrid", [True, False])
+def test_uneven_batch_equals_per_modcod_pipelines(hybrid):
+    """hybrid: Type B blocks on per-code edge-buffer launches beside the CSR
+    queue; False: every block on the CSR queue."""
     import torch
     from atsc3_b200.batch import UnevenBatch
     from atsc3_b200.pipeline import FecPipeline
     rng = np.random.default_rng(2)
     specs = [MIX[i] for i in rng.integers(0, len(MIX), 20)] + MIX
     cells, s2s = _blocks(torch, specs)
-    ub = UnevenBatch(specs, iters=50, alpha=0.75)
+    ub = UnevenBatch(specs, iters=50, alpha=0.75, hybrid=hybrid)
+    assert (len(ub.groups) > 0) == hybrid
     ub.load(cells, s2s)
     ub.launch()
     got = ub.results()
@@ -65,3 +69,23 @@ def test_uneven_batch_equals_per_modcod_pipelines():
     for b in range(len(specs)):
         assert np.array_equal(tuned[b]["payload"], got[b]["payload"])
         assert tuned[b]["its"] == got[b]["its"]
+
+
+def test_uneven_batch_all_quasi_cyclic():
+    """A batch with no CSR block at all (every code Type B)."""
+    import torch
+    from atsc3_b200.batch import UnevenBatch
+    from atsc3_b200.pipeline import FecPipeline
+    specs = [(64800, "256QAM", "10/15"), (16200, "64QAM", "11/15"),
+             (64800, "4096QAM", "12/15"), (64800, "256QAM", "10/15")]
+    cells, s2s = _blocks(torch, specs, seed=9)
+    ub = UnevenBatch(specs, iters=50, alpha=0.75)
+    assert ub.ncsr == 0 and len(ub.groups) == 3
+    ub.load(cells, s2s)
+    ub.capture()
+    ub.run()
+    got = ub.results()
+    for b, (n, m, r) in enumerate(specs):
+        ws = FecPipeline(n, m, r, iters=50, alpha=0.75).decode(cells[b][None], s2s[b])
+        assert np.array_equal(got[b]["payload"], ws["payload"][0].cpu().numpy()), b
+        assert got[b]["its"] == int(ws["its"][0])
