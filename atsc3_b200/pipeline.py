@@ -10,6 +10,8 @@ per-block conv/its/bad), the BCH check (syndrome, ok flag, payload bytes).
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from . import bch as BCH
@@ -21,6 +23,24 @@ from . import ldpc as LDPC
 def _torch():
     import torch
     return torch
+
+
+class _Range:
+    """An NVTX range around a stage when ATSC3_NVTX=1 (for nsys/ncu
+    timelines); nothing otherwise."""
+
+    on = os.environ.get("ATSC3_NVTX", "0") not in ("", "0")
+
+    def __init__(self, name):
+        self.name = name
+
+    def __enter__(self):
+        if self.on:
+            _torch().cuda.nvtx.range_push(self.name)
+
+    def __exit__(self, *exc):
+        if self.on:
+            _torch().cuda.nvtx.range_pop()
 
 
 class FecPipeline:
@@ -87,13 +107,17 @@ class FecPipeline:
         ws = dict(self._buffers(nblk))
         if out:
             ws.update(out)
-        DM.demap(cells, self.mod, self.rate, sigma2=sigma2, n=self.n,
-                 deinterleave=True, out=ws["lam"])
-        self._ldpc(ws, iters, alpha, weights)
+        with _Range("atsc3.demap"):
+            DM.demap(cells, self.mod, self.rate, sigma2=sigma2, n=self.n,
+                     deinterleave=True, out=ws["lam"])
+        with _Range("atsc3.ldpc"):
+            self._ldpc(ws, iters, alpha, weights)
         if self.rescue:
-            LDPC.rescue_near_misses(self.sp_tab, ws["lam"], ws, **self.rescue)
-        BCH.bch_check(ws["hard"], self.kldpc, self.n, self.kpayload,
-                      want_payload=True, out=ws)
+            with _Range("atsc3.sp_rescue"):
+                LDPC.rescue_near_misses(self.sp_tab, ws["lam"], ws, **self.rescue)
+        with _Range("atsc3.bch"):
+            BCH.bch_check(ws["hard"], self.kldpc, self.n, self.kpayload,
+                          want_payload=True, out=ws)
         return ws
 
     def _ldpc(self, ws, iters, alpha, weights):
