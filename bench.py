@@ -9,8 +9,8 @@ noise variance N0/h^2 is passed per cell.  Frame f is at Es/N0 =
 4.0 + 0.5*(f mod 9) dB (the 4..8 dB sweep), normalised min-sum alpha 0.75,
 at most 50 iterations, early stop on a zero syndrome, then BCH + descramble.
 Payload bits are seeded uniform random, encoded by the package's GPU
-transmitter; every step reads a different frame (0.93 GB of distinct frames
-for 64 steps, far above the 126 MB L2).
+transmitter; every step reads a different frame (1.87 GB of distinct frames
+for the default 128 steps, far above the 126 MB L2).
 
 metric = decoded info Mbit/s = 75 * 25728 payload bits per frame / time.
 
@@ -72,7 +72,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -213,8 +213,8 @@ def config(blocks):
             "esn0_db": ESN0, "alpha": ALPHA, "iters_max": ITERS,
             "early_stop": "zero syndrome", "sigma2": "per cell",
             "parallelism": "blocks sharded per GPU (no exchange)",
-            "l2": "inputs larger than L2: a distinct 14.6 MB frame per step, "
-                  "0.93 GB over 64 steps"}
+            "l2": "inputs larger than L2: a distinct 14.6 MB frame per step "
+                  "(1.87 GB over the default 128 steps)"}
 
 
 def decode_frame(pipe, cells, sig, out, stream, weights=None):
@@ -604,7 +604,7 @@ def main(argv=None):
     ap.add_argument("--workload", default="frame", choices=["frame", "uneven"])
     ap.add_argument("--blocks", type=int, default=512)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=128)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=2024)
