@@ -30,6 +30,7 @@ def cpe_correct_device(pool, sym_ptr, region, alphabets, dummy=None, iters=3,
         raise TypeError("pool must be a 1-D CUDA complex128 tensor")
     if not 1 <= len(alphabets) <= 2:
         raise ValueError("one or two alphabets")
+    pool = pool.resolve_conj().contiguous()
     n = pool.numel()
     nsym = sym_ptr.numel() - 1
     dev = pool.device

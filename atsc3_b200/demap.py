@@ -58,9 +58,10 @@ def device_lam_of_q(n, mod, rate, device):
 def _as_float_pairs(cells):
     torch = _torch()
     if cells.dtype == torch.complex64:
-        return torch.view_as_real(cells)
+        # a lazily conjugated tensor (x.conj()) has no real view: resolve it
+        return torch.view_as_real(cells.resolve_conj())
     if cells.dtype == torch.complex128:
-        return torch.view_as_real(cells.to(torch.complex64))
+        return torch.view_as_real(cells.resolve_conj().to(torch.complex64))
     raise TypeError("cells must be complex64 (or complex128)")
 
 

@@ -151,6 +151,7 @@ def demap_deinterleave(stream, ti, mod, rate, n, sigma2=None, out=None,
     if stream.dtype != torch.complex64 or stream.device.type != "cuda" or \
             stream.dim() != 1 or not stream.is_contiguous():
         raise TypeError("stream must be a contiguous 1-D CUDA complex64 tensor")
+    stream = stream.resolve_conj()
     nb = C.MOD_BITS[mod]
     nblk, ncell = ti.nblk, ti.ncell
     if ncell != C.cells_per_block(n, mod):
