@@ -781,8 +781,13 @@ static uint64_t fnv1a(uint64_t h, const void *p, size_t bytes) {
   return h;
 }
 
+// A code's plan for the host-pointer entry point: the edge-buffer
+// quasi-cyclic plan when the tables are an A/322 Type B code that decoder
+// takes (atsc3_ldpc_qc_detect), else the CSR plan.  Both are bit-exact with
+// lab/ldpc_kernel.c.
 struct HostPlanEntry {
   atsc3_ldpc_plan *plan;
+  atsc3_ldpc_qce_plan *qce;
   uint64_t hash;
 };
 static std::mutex g_hp_mu;
@@ -823,21 +828,38 @@ int32_t minsum_f32_host(const float *llr, int32_t nblk, int32_t n, int32_t nc,
   ATSC3_CUDA(cudaGetDevice(&dev));
   const uint64_t h = content_hash(cptr, cidx, vptr, vedge, n, nc, nedges, dev);
   atsc3_ldpc_plan *plan = nullptr;
+  atsc3_ldpc_qce_plan *qce = nullptr;
   {
     std::lock_guard<std::mutex> g(g_hp_mu);
     auto it = g_hp.find(h);
-    if (it != g_hp.end()) plan = it->second.plan;
+    if (it != g_hp.end()) {
+      plan = it->second.plan;
+      qce = it->second.qce;
+    }
   }
-  if (!plan) {
-    int32_t rc = plan_create(cptr, cidx, vptr, vedge, n, nc, nedges, 0, 0, &plan);
-    if (rc) return rc;
+  if (!plan && !qce) {
+    std::vector<int32_t> rowptr((size_t)n / 360 + 1), addr((size_t)nedges + 1);
+    int32_t kq[2] = {0, 0};
+    if (atsc3_ldpc_qc_detect(cptr, cidx, vptr, vedge, n, nc, nedges, kq,
+                             rowptr.data(), addr.data()) == 0) {
+      const int32_t rc = atsc3_ldpc_qce_plan_create(n, kq[0], kq[1], rowptr.data(),
+                                                    addr.data(), 0, &qce);
+      if (rc != 0 && rc != -4) return rc;   // -4: a structure it does not take
+      if (rc) qce = nullptr;
+    }
+    if (!qce) {
+      int32_t rc = plan_create(cptr, cidx, vptr, vedge, n, nc, nedges, 0, 0, &plan);
+      if (rc) return rc;
+    }
     std::lock_guard<std::mutex> g(g_hp_mu);
     auto it = g_hp.find(h);
     if (it != g_hp.end()) {
-      atsc3_ldpc_plan_destroy(plan);
+      if (plan) atsc3_ldpc_plan_destroy(plan);
+      if (qce) atsc3_ldpc_qce_plan_destroy(qce);
       plan = it->second.plan;
+      qce = it->second.qce;
     } else {
-      g_hp[h] = HostPlanEntry{plan, h};
+      g_hp[h] = HostPlanEntry{plan, qce, h};
     }
   }
   if (!t_stream) ATSC3_CUDA(cudaStreamCreateWithFlags(&t_stream, cudaStreamNonBlocking));
@@ -852,10 +874,16 @@ int32_t minsum_f32_host(const float *llr, int32_t nblk, int32_t n, int32_t nc,
   int32_t rc = 0;
   cudaError_t e = cudaMemcpyAsync(buf + o_llr, llr, nl * 4, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
-    rc = flood_launch(plan, buf + o_llr, n, nblk, iters, (double)alpha, 0,
-                      (uint8_t *)(buf + o_bits), n, nullptr, 0,
-                      (uint8_t *)(buf + o_conv), (int32_t *)(buf + o_its),
-                      (int32_t *)(buf + o_bad), 0, st, 0);
+    if (qce)
+      rc = atsc3_ldpc_qce_decode(qce, (const float *)(buf + o_llr), n, nblk, iters,
+                                 alpha, 0, (uint8_t *)(buf + o_bits), n, nullptr, 0,
+                                 (uint8_t *)(buf + o_conv), (int32_t *)(buf + o_its),
+                                 (int32_t *)(buf + o_bad), 0, st);
+    else
+      rc = flood_launch(plan, buf + o_llr, n, nblk, iters, (double)alpha, 0,
+                        (uint8_t *)(buf + o_bits), n, nullptr, 0,
+                        (uint8_t *)(buf + o_conv), (int32_t *)(buf + o_its),
+                        (int32_t *)(buf + o_bad), 0, st, 0);
     if (rc == 0) {
       e = cudaMemcpyAsync(bits, buf + o_bits, nl, cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaMemcpyAsync(conv, buf + o_conv, nblk, cudaMemcpyDeviceToHost, st);

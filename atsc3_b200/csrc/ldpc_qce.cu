@@ -936,6 +936,86 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
   return 0;
 }
 
+// Recognise an A/322 Type B code (360-bit circulants, accumulator parity) in
+// CSR tables laid out as lab/m3_ldpc.py:459-482 builds them, and recover its
+// address table.  The tables are accepted only if they are exactly that
+// code's parity-check matrix in the reference's edge order, so the decoders
+// built from the address table see the same edges in the same order:
+//  * checks ascending, each check's columns strictly ascending;
+//  * vedge = the stable argsort of cidx (each bit's edges by ascending check);
+//  * info bit 360g + mm is on checks (x + mm*Q) mod nc for the checks x of
+//    bit 360g (lab/m3_ldpc.py:166-212 with Q = nc / 360);
+//  * parity bit K + 360j + k is on checks c = j + Q*k and c + 1 (the last
+//    parity bit, c = nc - 1, on c only).
+// Output: kq = {K, Q}, rowptr (K/360 + 1) and addr (the checks of bit 360g,
+// ascending) sized by the caller for n/360 + 1 and nedges entries.  Returns
+// 0, or -4 (not a Type B structure; nothing else is wrong with the tables).
+int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
+                             const int32_t *vptr, const int32_t *vedge,
+                             int32_t n, int32_t nc, int32_t nedges,
+                             int32_t *kq, int32_t *rowptr, int32_t *addr) {
+  using namespace atsc3;
+  ATSC3_ARG(cptr && cidx && vptr && vedge && kq && rowptr && addr, "null argument");
+  ATSC3_ARG(n > 0 && nc > 0 && nedges >= 0, "bad size");
+  auto no = [](const char *why) {
+    set_error(why);
+    return (int32_t)-4;
+  };
+  if (n % EZ || nc % EZ || nc >= n) return no("not a 360-circulant code");
+  const int Q = nc / EZ, K = n - nc, nbi = K / EZ;
+  if (cptr[0] != 0 || cptr[nc] != nedges || vptr[0] != 0 || vptr[n] != nedges)
+    return no("inconsistent CSR");
+  std::vector<int32_t> chk((size_t)nedges);
+  for (int c = 0; c < nc; ++c) {
+    if (cptr[c + 1] < cptr[c]) return no("inconsistent CSR");
+    for (int e = cptr[c]; e < cptr[c + 1]; ++e) {
+      if (cidx[e] < 0 || cidx[e] >= n) return no("column out of range");
+      if (e > cptr[c] && cidx[e] <= cidx[e - 1]) return no("columns not ascending");
+      chk[e] = c;
+    }
+  }
+  std::vector<int32_t> fill((size_t)n, 0);
+  for (int v = 0; v < n; ++v)
+    if (vptr[v + 1] < vptr[v]) return no("inconsistent CSR");
+  for (int e = 0; e < nedges; ++e) {
+    const int v = cidx[e];
+    const int k = vptr[v] + fill[v]++;
+    if (k >= vptr[v + 1] || vedge[k] != e) return no("vedge is not the stable argsort of cidx");
+  }
+  // info bits: the checks of bit 360g, rotated by mm*Q
+  rowptr[0] = 0;
+  for (int g = 0; g < nbi; ++g) {
+    const int v0 = g * EZ, d = vptr[v0 + 1] - vptr[v0];
+    const int32_t *X = addr + rowptr[g];
+    for (int i = 0; i < d; ++i) addr[rowptr[g] + i] = chk[vedge[vptr[v0] + i]];
+    rowptr[g + 1] = rowptr[g] + d;
+    for (int mm = 1; mm < EZ; ++mm) {
+      const int v = v0 + mm;
+      if (vptr[v + 1] - vptr[v] != d) return no("info column degrees differ");
+      const int64_t sh = (int64_t)mm * Q;
+      int s = 0;                               // first x with x + sh >= nc
+      while (s < d && X[s] + sh < nc) ++s;
+      for (int i = 0; i < d; ++i) {
+        const int src = i < d - s ? s + i : i - (d - s);
+        const int64_t want = X[src] + sh - (src >= s ? nc : 0);
+        if (chk[vedge[vptr[v] + i]] != want) return no("info column not a circulant shift");
+      }
+    }
+  }
+  // parity bits: accumulator chain through the column twist
+  for (int j = 0; j < Q; ++j)
+    for (int k = 0; k < EZ; ++k) {
+      const int v = K + EZ * j + k, c = j + Q * k;
+      const int d = vptr[v + 1] - vptr[v];
+      if (d != (c == nc - 1 ? 1 : 2) || chk[vedge[vptr[v]]] != c ||
+          (d == 2 && chk[vedge[vptr[v] + 1]] != c + 1))
+        return no("parity part is not the Type B accumulator");
+    }
+  kq[0] = K;
+  kq[1] = Q;
+  return 0;
+}
+
 int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *h, int32_t threads,
                               int32_t semantics, int32_t *out) {
   using namespace atsc3;

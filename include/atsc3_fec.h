@@ -195,6 +195,21 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
                                    int32_t cluster, atsc3_ldpc_qce_plan **out);
 void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *plan);
 
+/* Host only.  Recognise an A/322 Type B code in CSR tables built as
+ * lab/m3_ldpc.py:459-482 (_kernel_tables) builds them from
+ * lab/m3_ldpc.py:166-212 (parity_check): 360-bit circulants, info bit
+ * 360g+mm on checks (x + mm*Q) mod nc for the checks x of bit 360g,
+ * accumulator parity through the column twist, vedge the stable argsort of
+ * cidx.  On success kq = {K, Q}, rowptr (K/360 + 1 entries) and addr (the
+ * checks of bit 360g, ascending; room for nedges) feed
+ * atsc3_ldpc_qce_plan_create.  Returns 0, or -4 when the tables are not that
+ * structure.  ldpc_minsum_f32 uses it to send Type B codes to the edge-buffer
+ * decoder. */
+int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
+                             const int32_t *vptr, const int32_t *vedge,
+                             int32_t n, int32_t nc, int32_t nedges,
+                             int32_t *kq, int32_t *rowptr, int32_t *addr);
+
 /* info[0]=n [1]=K [2]=Q [3]=cluster [4]=shared bytes per CTA [5]=max
  * block-row degree [6]=max block-column degree [7]=table bytes [8]=most edge
  * slots (360 edges each) held by one CTA [9]=360-bit columns of CTA 0 */
