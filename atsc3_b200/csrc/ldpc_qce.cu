@@ -31,9 +31,10 @@
 // bit mm%32).  The variable phase writes each 32-bit ballot to every CTA of
 // the cluster; the check phase looks up its bits locally.
 //
-// Shared memory per CTA: bitmap (nb*48 B) | syndrome exchange (256 B) | the
-// edge slots of the CTA's columns (1440 B per slot).  For the 64800-bit codes
-// (about 281k edges, 1.1 MB of slots) an 8-CTA cluster holds a codeword.
+// Shared memory per CTA: bitmap (nb*48 B) | syndrome exchange (256 B) |
+// per-launch tables | the edge slots of the CTA's columns (1440 B per slot).
+// For the 64800-bit codes (about 281k edges, 1.1 MB of slots) a 6-CTA
+// cluster holds a codeword (about 215 KB per CTA).
 
 #include <cuda_runtime.h>
 
@@ -162,20 +163,44 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     dcm = std::max(dcm, (int)Cc.size());
     total += (int)Cc.size();
   }
-  // columns assigned to the cluster's CTAs by longest-processing-time
-  // greedy on their slot counts (largest column first, to the CTA holding
-  // the fewest slots): the per-CTA slot totals differ by at most one column
-  std::vector<int> order(nb), load(cluster, 0), who(nb);
-  for (int g = 0; g < nb; ++g) order[g] = g;
+  // Column -> CTA assignment.  Block rows are split into contiguous ranges
+  // (CTA c owns rows [c*per, (c+1)*per)); an edge is local when its column
+  // lives in the CTA that owns its row, and a local edge saves the check
+  // phase a remote load and a remote store.  Parity column j (edges in rows
+  // j and j+1 only) goes to the owner of row j, which makes nearly all parity
+  // edges local.  The information columns follow in decreasing degree
+  // (stable), each to the CTA that owns most of its rows among the CTAs that
+  // stay within the balanced share ceil(edges slots / cluster), ties to the
+  // CTA holding fewer slots; a column no CTA can take within the share goes
+  // to the CTA holding the fewest.
+  const int per = (Q + cluster - 1) / cluster;
+  std::vector<int> order, load(cluster, 0), who(nb), mine(cluster);
+  for (int j = 0; j < Q; ++j) {
+    const int c = std::min(cluster - 1, j / per);
+    who[nbi + j] = c;
+    load[c] += (int)cols[nbi + j].size();
+  }
+  const int share = (total + cluster - 1) / cluster;
+  for (int g = 0; g < nbi; ++g) order.push_back(g);
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
     return cols[x].size() > cols[y].size();
   });
   for (int g : order) {
-    int c = 0;
-    for (int q = 1; q < cluster; ++q)
-      if (load[q] < load[c]) c = q;
+    const int d = (int)cols[g].size();
+    std::fill(mine.begin(), mine.end(), 0);
+    for (auto &sl : cols[g]) ++mine[std::min(cluster - 1, sl.row / per)];
+    int c = -1;
+    for (int q = 0; q < cluster; ++q) {
+      if (load[q] + d > share) continue;
+      if (c < 0 || mine[q] > mine[c] || (mine[q] == mine[c] && load[q] < load[c])) c = q;
+    }
+    if (c < 0) {
+      c = 0;
+      for (int q = 1; q < cluster; ++q)
+        if (load[q] < load[c]) c = q;
+    }
     who[g] = c;
-    load[c] += (int)cols[g].size();
+    load[c] += d;
   }
   t->ccols.clear();
   p->cb[0] = 0;
@@ -185,8 +210,6 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     p->cb[c + 1] = (int)t->ccols.size();
   }
   for (int c = cluster + 1; c <= EMAXCL; ++c) p->cb[c] = nb;
-  (void)total;
-  const int per = (Q + cluster - 1) / cluster;
   for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
   // variable-phase items per CTA: a column of 2..4 edges is cut into six
   // 64-bit items (lane L takes bits 64p + L and 64p + 32 + L), a larger one
