@@ -48,7 +48,7 @@ def test_wms_forward_and_gradients_vs_float64_reference():
     r = ref.detach().numpy()
     close = np.abs(o - r) <= 1e-3 * np.maximum(1.0, np.abs(r))
     assert close.mean() > 0.999, close.mean()
-    assert abs(float(loss) - float(lref)) <= 1e-4 * abs(float(lref))
+    assert abs(float(loss.detach()) - float(lref.detach())) <= 1e-4 * abs(float(lref.detach()))
     for g, gr in ((a.grad, a64.grad), (b.grad, b64.grad)):
         g = g.cpu().double().numpy()
         gr = gr.numpy()
