@@ -400,7 +400,7 @@ def sp_tables(tables, n, device="cuda"):
         d = _SP_TABLES.get(key)
         if d is None:
             d = {"n": int(n), "nc": len(arrs[0]) - 1, "nedges": len(arrs[1]),
-                 "t": [torch.from_numpy(a).to(device) for a in arrs]}
+                 "t": [torch.from_numpy(np.array(a)).to(device) for a in arrs]}
             _SP_TABLES[key] = d
     return d
 

@@ -278,7 +278,7 @@ def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
         with torch.no_grad():
             beta.clamp_(min=0.0)
         if step % log_every == 0 or step == start + steps - 1:
-            hist.append((step, float(loss)))
+            hist.append((step, float(loss.detach())))
     manifest = {"rate": rate, "n": n, "mod": mod, "iters": iters,
                 "buckets": [int(x) for x in code.buckets], "seed": seed,
                 "step": start + steps, "esn0": list(esn0), "channel": channel,

@@ -371,12 +371,15 @@ def run_gpu(args, rank, world, local_rank):
     its_stage = float(np.mean(stage_its)) if stage_its else 0.0
     onchip = {"unit": "GB/s", "bytes_per_launch": 8 * nedges * its_stage,
               "achieved": 8 * nedges * its_stage / (ldpc_ms / 1e3) / 1e9,
-              "what": "distributed-shared-memory exchange, 8 B per edge per "
-                      "iteration (edge-buffer decoder)",
+              "what": "edge-slot exchange of the edge-buffer decoder, 8 B "
+                      "per edge per iteration (a 4-byte load and a 4-byte "
+                      "store); about half is served by the CTA's own shared "
+                      "memory (columns placed with their rows), the rest "
+                      "crosses the cluster's xbar",
               "peak_ncu": 9300.0,
               "peak_note": "xbar-to-L1 distributed shared memory bytes at "
-                           "25.8% of peak = 2.40 TB/s in the committed ncu "
-                           "capture, i.e. about 9.3 TB/s"}
+                           "22.9% of peak = 2.13 TB/s (7.55 GB per launch) "
+                           "in the committed ncu capture, i.e. about 9.3 TB/s"}
     onchip["frac"] = onchip["achieved"] / onchip["peak_ncu"]
     b_ldpc = nblk * (4 * N_INNER + N_INNER // 8 + 9)
     hbm, peak_kind = peaks()
