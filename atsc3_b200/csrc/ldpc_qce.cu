@@ -3,10 +3,11 @@
 // lab/ldpc_kernel.c (kernel semantics) and lab/m9_gpu.py:168-211 (torch
 // semantics), float32.
 //
-// The code structure used is the one of ldpc_qc.cu (360x360 circulants, at
-// most one per block, dual-diagonal parity part, edge order inside a check =
-// block-column order, a bit's summation order = its column's circulant list
-// sorted by (shift, row) and rotated at s0[col*360 + mm]).
+// The code structure used is the one of ldpc_qc.cu (360x360 circulants,
+// dual-diagonal parity part, edge order inside a check = block-column order,
+// a bit's summation order = its column's circulant list sorted by (shift,
+// row) and rotated at s0[col*360 + mm]), except that a block may hold more
+// than one circulant here.
 //
 // What differs is where the decoder state lives.  Every edge of the codeword
 // owns one float32 slot in the distributed shared memory of its cluster, in
@@ -61,7 +62,7 @@ constexpr int EPART = 256;                // syndrome exchange bytes
 // degree; rows with fewer edges mask the rest) (the kernel templates).
 __host__ __device__ constexpr int qce_ns(int dr) {
   return dr <= 8 ? 8 : dr <= 10 ? 10 : dr <= 11 ? 11 : dr <= 14 ? 14
-       : dr <= 17 ? 17 : dr <= 22 ? 22 : dr <= 33 ? 33 : dr <= 56 ? 56 : 0;
+       : dr <= 17 ? 17 : dr <= 22 ? 22 : dr <= 34 ? 34 : dr <= 56 ? 56 : 0;
 }
 
 struct QcePlan {
@@ -124,13 +125,29 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   for (int r = 0; r < Q; ++r) {
     auto &R = rows[r];
     std::sort(R.begin(), R.end(),
-              [](const Slot &a, const Slot &b) { return a.col < b.col; });
-    for (size_t i = 1; i < R.size(); ++i)
-      if (R[i].col == R[i - 1].col) {
-        set_error("unsupported: two circulants share a block (use the CSR "
-                  "decoder)");
-        return -4;
+              [](const Slot &a, const Slot &b) {
+                return a.col != b.col ? a.col < b.col : a.u < b.u;
+              });
+    // Two circulants may share a block (the 16200-bit codes of rates 6/15,
+    // 8/15, 10/15, 12/15 and 13/15 have such blocks): they are two slots of
+    // the same column with different shifts.  Within a check their edges'
+    // order follows the bit index, which depends on the check, while the
+    // slots keep one order; the check update does not depend on the order of
+    // a check's edges (the first minimum matters only through min2, and
+    // min2 == min1 when the minimum is shared), so one slot order serves
+    // every check.  A repeated address cancels in GF(2)
+    // (lab/m3_ldpc.py:199-211): both copies are dropped.
+    {
+      std::vector<Slot> keep;
+      for (size_t i = 0; i < R.size(); ++i) {
+        if (i + 1 < R.size() && R[i + 1].col == R[i].col && R[i + 1].u == R[i].u) {
+          ++i;
+          continue;
+        }
+        keep.push_back(R[i]);
       }
+      R.swap(keep);
+    }
     // dual diagonal: bits K+360(r-1)+k and K+360r+k (r >= 1); K+k and
     // K+360(Q-1)+k-1 (r = 0, absent for k = 0)
     if (r >= 1) {
@@ -158,7 +175,7 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     for (int i = 0; i < (int)Cc.size(); ++i) {
       Cc[i].idx = i;
       for (auto &rs : rows[Cc[i].row])      // back-reference row slot -> idx
-        if (rs.col == g) rs.idx = i;
+        if (rs.col == g && rs.u == Cc[i].u) rs.idx = i;
     }
     dcm = std::max(dcm, (int)Cc.size());
     total += (int)Cc.size();
@@ -767,7 +784,7 @@ static QceFn qce_fn(int semantics, int dr, int threads) {
     case 14: return qce_pick<14>(semantics, big);
     case 17: return qce_pick<17>(semantics, big);
     case 22: return qce_pick<22>(semantics, big);
-    case 33: return qce_pick<33>(semantics, big);
+    case 34: return qce_pick<34>(semantics, big);
     case 56: return qce_pick<56>(semantics, big);
     default: return nullptr;
   }

@@ -65,9 +65,10 @@ def test_every_code_through_the_host_abi(n, torch):
 
 
 def test_concurrent_callers(torch):
-    """Eight threads, mixed codes (edge-buffer, CSR for a Type A code and for
-    a 16200 code whose circulants share blocks), each call checked against
-    the oracle; then the same calls again, all at once."""
+    """Eight threads, mixed codes (the edge-buffer decoder for the Type B
+    codes, the CSR decoder for the Type A ones, 64800 7/15 and 16200 3/15),
+    each call checked against the oracle; then the same calls again, all at
+    once."""
     jobs = []
     for i, (rate, n) in enumerate([("10/15", 64800), ("7/15", 64800), ("6/15", 16200),
                                    ("11/15", 16200), ("8/15", 64800), ("3/15", 16200),

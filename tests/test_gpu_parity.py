@@ -353,11 +353,13 @@ def test_many_codewords_per_cluster_outputs_consistent(kind, torch):
     assert o["its"].cpu().numpy()[sel].tolist() == want[2].tolist()
 
 
-@pytest.mark.parametrize("rate", ["7/15", "9/15", "11/15"])
+@pytest.mark.parametrize("rate", ["6/15", "7/15", "8/15", "9/15", "10/15", "11/15",
+                                  "12/15", "13/15"])
 @pytest.mark.parametrize("cluster", [2, 4])
 def test_qce_16200_codes_vs_oracle(rate, cluster, torch):
-    """Edge-buffer decoder on the 16200-bit Type B codes it accepts, both
-    semantics, packed and unpacked outputs, against the oracle."""
+    """Edge-buffer decoder on every 16200-bit Type B code (6/15, 8/15, 10/15,
+    12/15 and 13/15 put two circulants in some blocks), both semantics,
+    packed and unpacked outputs, against the oracle."""
     from atsc3_b200.ldpc import QcePlan, decode_flood
     n = 16200
     plan = QcePlan(rate, n, cluster=cluster)
