@@ -71,26 +71,25 @@ _QCE = {}
 
 
 def qce_plan(rate, n):
-    """The edge-buffer quasi-cyclic plan of a code, or None if that decoder
-    does not take it (Type A codes, two circulants in a block)."""
+    """The edge-buffer quasi-cyclic plan of a code (every A/322 code), or
+    None if that decoder does not take it."""
     key = (rate, n)
     if key not in _QCE:
         p = None
-        if C.ldpc_params(rate, n)[0] == "B":
-            try:
-                p = LDPC.QcePlan(rate, n)
-            except N.FecError as e:
-                if e.rc != -4:
-                    raise
+        try:
+            p = LDPC.QcePlan(rate, n)
+        except N.FecError as e:
+            if e.rc != -4:
+                raise
         _QCE[key] = p
     return _QCE[key]
 
 
 class UnevenBatch:
     """A fixed list of blocks ``specs = [(n, mod, rate), ...]``.  hybrid:
-    decode the blocks of Type B codes with the edge-buffer quasi-cyclic
-    decoder (one launch per code, concurrent); False puts every block on the
-    CSR persistent launch."""
+    decode the blocks with the edge-buffer quasi-cyclic decoder (one launch
+    per code, concurrent; the CSR persistent launch keeps any code it does
+    not take); False puts every block on the CSR persistent launch."""
 
     def __init__(self, specs, iters=50, alpha=0.75, device="cuda", hybrid=True):
         torch = _torch()

@@ -67,11 +67,14 @@ __host__ __device__ constexpr int qce_ns(int dr) {
 
 struct QcePlan {
   int n = 0, K = 0, Q = 0, nb = 0;
+  int qa = 0, qb = 0;           // accumulator / identity block rows
   int cluster = 1, smem = 0, part_off = 0, rt_off = 0, ri_off = 0, ct_off = 0;
-  int buf_off = 0;
-  int dr_max = 0, dc_max = 0, max_slots = 0, device = 0;
+  int ht_off = 0, buf_off = 0;
+  int dr_max = 0, dr_light = 0, dc_max = 0, max_slots = 0, device = 0;
+  int heavy = 0;                // rows above the compile-time slot count
   int64_t table_bytes = 0;
-  int rb[EMAXCL + 1] = {0};     // block rows of CTA c (check phase)
+  int rb[EMAXCL + 1] = {0};     // block rows CTA c owns (column placement)
+  int ci[EMAXCL + 1] = {0};     // check items (row*12 + chunk) of CTA c
   int ib[EMAXCL + 1] = {0};     // variable-phase items of CTA c in d_itab
   int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
@@ -79,62 +82,81 @@ struct QcePlan {
   int4 *d_itab = nullptr;       // variable-phase items, grouped by CTA
   int32_t *d_rptr = nullptr;    // (Q+1)
   int4 *d_cdesc = nullptr;      // per column
-  uint8_t *d_s0 = nullptr;      // (nb*360) rotation start
+  uint8_t *d_s0 = nullptr;      // (nb*360) rotation start (zone A / only zone)
+  uint8_t *d_s0b = nullptr;     // (nb*360) rotation start in zone B
 };
 
+// Block rows: rows 0 .. qa-1 are the accumulator rows (check r + qa*k, the
+// dual-diagonal parity part), rows qa .. qa+qb-1 the identity rows of a Type A
+// code (check 360*qa + (r - qa) + qb*k, one parity bit each); a Type B code
+// has qb = 0.
 // Row slot (block row r, position j):  x = owner CTA | WRAP << 8 | j << 16,
 // y = byte offset of the edge's circulant slot in the owner's shared memory,
 // z = circulant shift u, w = byte offset of the column's bitmap words.
 // Check (r, k) reads entry (k - u) mod 360 of the slot.
 // Column descriptor (column g): x = slots d, y = byte offset of slot 0 in
 // the owner's shared memory (slots follow at 1440-byte steps, sorted by
-// (u, row)), z = index of the dual-diagonal wrap slot (absent for bit 359)
-// or -1, w = owner CTA.  ccols lists each CTA's columns (cb[c] .. cb[c+1]).
+// (zone, u, row)), z = index of the dual-diagonal wrap slot (absent for bit
+// 359) or -1, w = owner CTA | zone-A slots << 8.  ccols lists each CTA's
+// columns (cb[c] .. cb[c+1]).
 struct QceTables {
   std::vector<int4> rdesc;
   std::vector<int32_t> rptr;
   std::vector<int4> cdesc;
   std::vector<int32_t> ccols;
   std::vector<int4> itab;
-  std::vector<uint8_t> s0;
+  std::vector<uint8_t> s0, s0b;
 };
 
-int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
-              int cluster, QcePlan *p, QceTables *t) {
-  if (n % EZ || K % EZ || Q <= 0 || (n - K) != Q * EZ) {
-    set_error("invalid argument: not a 360-circulant Type B code");
+// variable-phase item modes (bits 25-26 of the item's z word)
+constexpr int VM_PAIR = 0;     // dual-diagonal parity column, 2 slots in check order
+constexpr int VM_EXACT = 1;    // 1..4 slots of one zone, rotated in registers
+constexpr int VM_GEN = 2;      // any slots of one zone, rotated by offsets
+constexpr int VM_GEN2 = 3;     // slots in both zones: two rotated segments
+constexpr uint32_t VNOWRAP = 0xFFu;
+
+int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
+              const int32_t *addr, int cluster, QcePlan *p, QceTables *t) {
+  const int Q = QA + QB;
+  if (n % EZ || K % EZ || QA <= 0 || QB < 0 || (n - K) != Q * EZ) {
+    set_error("invalid argument: not a 360-circulant Type A/B code");
     return -3;
   }
   if (cluster < 1 || cluster > EMAXCL) {
     set_error("invalid argument: cluster must be in 1..16");
     return -3;
   }
-  const int nbi = K / EZ, nb = n / EZ;
+  const int nbi = K / EZ, nb = n / EZ, MA = QA * EZ;
   struct Slot { int col, row, u, pos, wrap, idx; };
   std::vector<std::vector<Slot>> rows(Q), cols(nb);
-  for (int g = 0; g < nbi; ++g)
+  // address-table rows: one per information column group and, for a Type A
+  // code, one per accumulator parity column (its bits feed the identity
+  // rows, A/322 6.1.3.1 step vii); accumulator address x -> (row, shift)
+  const int ntab = nbi + (QB > 0 ? QA : 0);
+  for (int g = 0; g < ntab; ++g)
     for (int e = rowptr[g]; e < rowptr[g + 1]; ++e) {
       const int x = addr[e];
       if (x < 0 || x >= n - K) {
         set_error("invalid argument: address outside the parity range");
         return -3;
       }
-      rows[x % Q].push_back(Slot{g, x % Q, x / Q, 0, 0, 0});
+      if (x < MA) rows[x % QA].push_back(Slot{g, x % QA, x / QA, 0, 0, 0});
+      else rows[QA + (x - MA) % QB].push_back(Slot{g, QA + (x - MA) % QB, (x - MA) / QB, 0, 0, 0});
     }
-  int drm = 0;
+  int drm = 0, drb = 0;
   for (int r = 0; r < Q; ++r) {
     auto &R = rows[r];
     std::sort(R.begin(), R.end(),
               [](const Slot &a, const Slot &b) {
                 return a.col != b.col ? a.col < b.col : a.u < b.u;
               });
-    // Two circulants may share a block (the 16200-bit codes of rates 6/15,
-    // 8/15, 10/15, 12/15 and 13/15 have such blocks): they are two slots of
-    // the same column with different shifts.  Within a check their edges'
-    // order follows the bit index, which depends on the check, while the
-    // slots keep one order; the check update does not depend on the order of
-    // a check's edges (the first minimum matters only through min2, and
-    // min2 == min1 when the minimum is shared), so one slot order serves
+    // Two circulants may share a block (the 16200-bit Type B codes of rates
+    // 6/15, 8/15, 10/15, 12/15 and 13/15 have such blocks): they are two
+    // slots of the same column with different shifts.  Within a check their
+    // edges' order follows the bit index, which depends on the check, while
+    // the slots keep one order; the check update does not depend on the
+    // order of a check's edges (the first minimum matters only through min2,
+    // and min2 == min1 when the minimum is shared), so one slot order serves
     // every check.  A repeated address cancels in GF(2)
     // (lab/m3_ldpc.py:199-211): both copies are dropped.
     {
@@ -148,52 +170,112 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
       }
       R.swap(keep);
     }
-    // dual diagonal: bits K+360(r-1)+k and K+360r+k (r >= 1); K+k and
-    // K+360(Q-1)+k-1 (r = 0, absent for k = 0)
-    if (r >= 1) {
-      R.push_back(Slot{nbi + r - 1, r, 0, 0, 0, 0});
-      R.push_back(Slot{nbi + r, r, 0, 0, 0, 0});
+    if (r < QA) {
+      // dual diagonal: bits K+360(r-1)+k and K+360r+k (r >= 1); K+k and
+      // K+360(QA-1)+k-1 (r = 0, absent for k = 0)
+      if (r >= 1) {
+        R.push_back(Slot{nbi + r - 1, r, 0, 0, 0, 0});
+        R.push_back(Slot{nbi + r, r, 0, 0, 0, 0});
+      } else {
+        R.push_back(Slot{nbi, 0, 0, 0, 0, 0});
+        R.push_back(Slot{nbi + QA - 1, 0, 1, 0, EWRAP, 0});
+      }
     } else {
-      R.push_back(Slot{nbi, 0, 0, 0, 0, 0});
-      R.push_back(Slot{nbi + Q - 1, 0, 1, 0, EWRAP, 0});
+      // identity part of a Type A code: bit K + 360*QA + 360*(r-QA) + k
+      R.push_back(Slot{nbi + r, r, 0, 0, 0, 0});
     }
+    std::stable_sort(R.begin(), R.end(),
+                     [](const Slot &a, const Slot &b) { return a.col < b.col; });
     for (int i = 0; i < (int)R.size(); ++i) R[i].pos = i;
     drm = std::max(drm, (int)R.size());
+    if (r >= QA) drb = std::max(drb, (int)R.size());
   }
-  if (drm > 56) {
+  // compile-time slots per row: the largest row for a Type B code; the
+  // largest identity row for a Type A code, whose few accumulator rows of
+  // higher degree take the kernel's loop path ("heavy" rows)
+  const int dlight = QB > 0 ? drb : drm;
+  const int ns = qce_ns(dlight);
+  if (ns == 0) {
     set_error("unsupported: block-row degree above 56");
+    return -4;
+  }
+  if (QB > 0 && ns != 8) {
+    set_error("unsupported: identity rows of more than 8 edges");
+    return -4;
+  }
+  std::vector<int> rdeg(Q);
+  int heavy = 0;
+  for (int r = 0; r < Q; ++r) {
+    rdeg[r] = (int)rows[r].size();
+    if (rdeg[r] > ns) heavy = 1;
+  }
+  if (drm > 250) {
+    set_error("unsupported: block-row degree above 250");
     return -4;
   }
   for (int r = 0; r < Q; ++r)
     for (auto &sl : rows[r]) cols[sl.col].push_back(sl);
   int dcm = 0, total = 0;
+  std::vector<int> dzA(nb, 0);
   for (int g = 0; g < nb; ++g) {
     auto &Cc = cols[g];
-    std::sort(Cc.begin(), Cc.end(), [](const Slot &a, const Slot &c) {
+    std::sort(Cc.begin(), Cc.end(), [QA](const Slot &a, const Slot &c) {
+      const int za = a.row >= QA, zc = c.row >= QA;
+      if (za != zc) return za < zc;
       return a.u != c.u ? a.u < c.u : a.row < c.row;
     });
     for (int i = 0; i < (int)Cc.size(); ++i) {
       Cc[i].idx = i;
+      if (Cc[i].row < QA) ++dzA[g];
       for (auto &rs : rows[Cc[i].row])      // back-reference row slot -> idx
         if (rs.col == g && rs.u == Cc[i].u) rs.idx = i;
     }
     dcm = std::max(dcm, (int)Cc.size());
     total += (int)Cc.size();
   }
-  // Column -> CTA assignment.  Block rows are split into contiguous ranges
-  // (CTA c owns rows [c*per, (c+1)*per)); an edge is local when its column
-  // lives in the CTA that owns its row, and a local edge saves the check
-  // phase a remote load and a remote store.  Parity column j (edges in rows
-  // j and j+1 only) goes to the owner of row j, which makes nearly all parity
-  // edges local.  The information columns follow in decreasing degree
-  // (stable), each to the CTA that owns most of its rows among the CTAs that
-  // stay within the balanced share ceil(edges slots / cluster), ties to the
-  // CTA holding fewer slots; a column no CTA can take within the share goes
-  // to the CTA holding the fewest.
+  if (dcm > 250) {
+    set_error("unsupported: column degree above 250");
+    return -4;
+  }
+  // Check items (row*12 + chunk) per CTA.  Without heavy rows: contiguous
+  // equal row ranges.  With heavy rows: contiguous item ranges of equal work
+  // (each item costs its row's degree), so the few heavy rows spread over
+  // the cluster.
   const int per = (Q + cluster - 1) / cluster;
+  if (!heavy) {
+    for (int c = 0; c <= cluster; ++c) p->ci[c] = std::min(Q, c * per) * ECHUNK;
+  } else {
+    int64_t work = 0;
+    for (int r = 0; r < Q; ++r) work += (int64_t)(rdeg[r] + 2) * ECHUNK;
+    p->ci[0] = 0;
+    int64_t acc = 0;
+    int c = 1;
+    for (int it = 0; it < Q * ECHUNK && c < cluster; ++it) {
+      acc += rdeg[it / ECHUNK] + 2;
+      while (c < cluster && acc * cluster >= work * c) p->ci[c++] = it + 1;
+    }
+    while (c < cluster) p->ci[c++] = Q * ECHUNK;
+    p->ci[cluster] = Q * ECHUNK;
+  }
+  for (int c = cluster + 1; c <= EMAXCL; ++c) p->ci[c] = Q * ECHUNK;
+  // the row's owner for column placement: the CTA holding its chunk 0
+  std::vector<int> rowown(Q, 0);
+  for (int c = 0; c < cluster; ++c)
+    for (int r = (p->ci[c] + ECHUNK - 1) / ECHUNK; r * ECHUNK < p->ci[c + 1]; ++r)
+      rowown[r] = c;
+  // Column -> CTA assignment.  An edge is local when its column lives in the
+  // CTA that owns its row, and a local edge saves the check phase a remote
+  // load and a remote store.  Parity column j of the accumulator (edges in
+  // rows j and j+1) goes to the owner of row j, an identity parity column to
+  // the owner of its row, which makes nearly all parity edges local.  The
+  // information columns follow in decreasing degree (stable), each to the
+  // CTA that owns most of their rows among the CTAs that stay within the
+  // balanced share ceil(slots / cluster), ties to the CTA holding fewer
+  // slots; a column no CTA can take within the share goes to the CTA holding
+  // the fewest.
   std::vector<int> order, load(cluster, 0), who(nb), mine(cluster);
   for (int j = 0; j < Q; ++j) {
-    const int c = std::min(cluster - 1, j / per);
+    const int c = rowown[j];
     who[nbi + j] = c;
     load[c] += (int)cols[nbi + j].size();
   }
@@ -205,7 +287,7 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   for (int g : order) {
     const int d = (int)cols[g].size();
     std::fill(mine.begin(), mine.end(), 0);
-    for (auto &sl : cols[g]) ++mine[std::min(cluster - 1, sl.row / per)];
+    for (auto &sl : cols[g]) ++mine[rowown[sl.row]];
     int c = -1;
     for (int q = 0; q < cluster; ++q) {
       if (load[q] + d > share) continue;
@@ -227,27 +309,58 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     p->cb[c + 1] = (int)t->ccols.size();
   }
   for (int c = cluster + 1; c <= EMAXCL; ++c) p->cb[c] = nb;
-  for (int c = 0; c <= cluster; ++c) p->rb[c] = std::min(Q, c * per);
-  // variable-phase items per CTA: a column of 2..4 edges is cut into six
-  // 64-bit items (lane L takes bits 64p + L and 64p + 32 + L), a larger one
+  for (int c = 0; c <= cluster; ++c)
+    p->rb[c] = std::min(Q, (p->ci[c] + ECHUNK - 1) / ECHUNK);
+  for (int c = cluster + 1; c <= EMAXCL; ++c) p->rb[c] = Q;
+  // wrap slot and item mode per column
+  std::vector<int> wrapi(nb, -1), vmode(nb, VM_GEN);
+  for (int g = 0; g < nb; ++g) {
+    auto &Cc = cols[g];
+    const int d = (int)Cc.size();
+    for (auto &sl : Cc)
+      if (sl.wrap) wrapi[g] = sl.idx;
+    const bool one_zone = dzA[g] == 0 || dzA[g] == d;
+    const bool acc_parity = g >= nbi && g < nbi + QA;
+    if (acc_parity && d == 2 && (wrapi[g] < 0 || wrapi[g] == 1) && Cc[0].u == 0 &&
+        (Cc[1].u == 0 || wrapi[g] == 1))
+      vmode[g] = VM_PAIR;
+    else if (d <= 4 && one_zone && wrapi[g] < 0)
+      vmode[g] = VM_EXACT;
+    else
+      vmode[g] = one_zone ? VM_GEN : VM_GEN2;
+  }
+  // variable-phase items per CTA: a pair or exact column is cut into six
+  // 64-bit items (lane L takes bits 64p + L and 64p + 32 + L), any other
   // into twelve 32-bit items
-  auto items_of = [&](int g) { const int d = (int)cols[g].size(); return d <= 4 ? 6 : ECHUNK; };
+  auto items_of = [&](int g) { return vmode[g] <= VM_EXACT ? 6 : ECHUNK; };
   int maxitems = 0;
   for (int c = 0; c < cluster; ++c) {
     int ni = 0;
     for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) ni += items_of(t->ccols[q]);
     maxitems = std::max(maxitems, ni);
   }
+  // per CTA: rows touched by its check items (all 12 chunks get row-slot
+  // entries) and heavy-row slot entries
+  int maxrows = 0, maxheavy = 0;
+  for (int c = 0; c < cluster; ++c) {
+    if (p->ci[c + 1] <= p->ci[c]) continue;
+    const int r0 = p->ci[c] / ECHUNK, r1 = (p->ci[c + 1] - 1) / ECHUNK;
+    maxrows = std::max(maxrows, r1 - r0 + 1);
+    int h = 0;
+    for (int r = r0; r <= r1; ++r)
+      if (rdeg[r] > ns) h += rdeg[r];
+    maxheavy = std::max(maxheavy, h);
+  }
   // shared memory: bitmap | syndrome exchange | row-slot table (per row,
-  // chunk and slot, 8 B) | row masks and degree | variable-phase item table
-  // (16 B per item) | slots
-  const int ns = qce_ns(drm);
+  // chunk and slot, 8 B) | row info (3 words per row) | variable-phase item
+  // table (16 B per item) | heavy-row slot table (8 B per slot) | slots
   const int bm_bytes = (nb * ECHUNK * 4 + 15) & ~15;
   const int part_off = bm_bytes;
   const int rt_off = part_off + EPART;
-  const int ri_off = rt_off + per * ECHUNK * ns * 8;
-  const int ct_off = ri_off + ((per * 3 * (ns > 32 ? 8 : 4) + 15) & ~15);
-  const int buf_off = ct_off + maxitems * 16;
+  const int ri_off = rt_off + maxrows * ECHUNK * ns * 8;
+  const int ct_off = ri_off + ((maxrows * 3 * (ns > 32 ? 8 : 4) + 15) & ~15);
+  const int ht_off = ct_off + maxitems * 16;
+  const int buf_off = ht_off + ((maxheavy * 8 + 15) & ~15);
   std::vector<int> owner(nb), base(nb);
   int maxs = 0;
   for (int c = 0; c < cluster; ++c) {
@@ -261,14 +374,18 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
     maxs = std::max(maxs, s);
   }
   p->n = n; p->K = K; p->Q = Q; p->nb = nb;
+  p->qa = QA; p->qb = QB;
   p->cluster = cluster;
   p->dr_max = drm;
+  p->dr_light = dlight;
+  p->heavy = heavy;
   p->dc_max = dcm;
   p->max_slots = maxs;
   p->part_off = part_off;
   p->rt_off = rt_off;
   p->ri_off = ri_off;
   p->ct_off = ct_off;
+  p->ht_off = ht_off;
   p->buf_off = buf_off;
   p->smem = buf_off + maxs * ESLOT;
   t->rptr.assign(Q + 1, 0);
@@ -282,42 +399,48 @@ int qce_build(int n, int K, int Q, const int32_t *rowptr, const int32_t *addr,
   }
   t->cdesc.assign(nb, make_int4(0, 0, -1, 0));
   t->s0.assign((size_t)nb * EZ, 0);
+  t->s0b.assign((size_t)nb * EZ, 0);
   for (int g = 0; g < nb; ++g) {
     auto &Cc = cols[g];
-    int wrap = -1;
-    for (auto &sl : Cc)
-      if (sl.wrap) wrap = sl.idx;
-    // the kernel's parity path expects the wrap edge as slot 1 of a
-    // two-edge column (the last parity column of every Type B code)
-    if (wrap >= 0 && (wrap != 1 || Cc.size() != 2)) {
-      set_error("unsupported: dual-diagonal wrap edge outside a 2-edge column");
-      return -4;
-    }
-    t->cdesc[g] = make_int4((int)Cc.size(), base[g], wrap, owner[g]);
+    t->cdesc[g] = make_int4((int)Cc.size(), base[g], wrapi[g], owner[g] | (dzA[g] << 8));
+    // a bit's checks in ascending index: zone A (index r + QA*k) before zone
+    // B, inside a zone by (k, r) = the slots sorted by (u, row), rotated to
+    // start at the first slot whose k = mm + u wrapped past 359
     for (int mm = 0; mm < EZ; ++mm) {
-      int s = 0;
-      for (auto &sl : Cc) s += (sl.u + mm < EZ) ? 1 : 0;
-      t->s0[(size_t)g * EZ + mm] = (uint8_t)s;
+      int sa = 0, sb = 0;
+      for (auto &sl : Cc) {
+        if (sl.u + mm >= EZ) continue;
+        if (sl.row < QA) ++sa;
+        else ++sb;
+      }
+      // a column of one zone keeps its rotation in s0 (zone B only: the
+      // identity parity columns)
+      t->s0[(size_t)g * EZ + mm] = (uint8_t)(dzA[g] == 0 ? sb : sa);
+      t->s0b[(size_t)g * EZ + mm] = (uint8_t)(dzA[g] == 0 ? 0 : sb);
     }
   }
   // item {byte offset of slot 0's entry of the item's first bit, lam index
   // of that bit, slots | valid lanes of sub-chunk 0 << 8 | of sub-chunk 1
-  // << 16 | absent wrap entry << 24, bitmap word of sub-chunk 0}
+  // << 16 | absent wrap entry << 24 | mode << 25, bitmap word of sub-chunk 0
+  // | zone-A slots << 16 | wrap slot << 24 (0xFF: none)}
   t->itab.clear();
   p->ib[0] = 0;
   for (int c = 0; c < cluster; ++c) {
     for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) {
       const int g = t->ccols[q];
       const int d = (int)cols[g].size();
-      const int wrap = t->cdesc[g].z;
-      const int step = d <= 4 ? 64 : 32;
+      const int wrap = wrapi[g];
+      const int step = items_of(g) == 6 ? 64 : 32;
       for (int mm0 = 0; mm0 < EZ; mm0 += step) {
         const int v0 = std::min(32, EZ - mm0);
         const int v1 = step == 64 ? std::max(0, std::min(32, EZ - mm0 - 32)) : 0;
         const int absent = (wrap >= 0 && mm0 + step >= EZ) ? 1 : 0;
+        const uint32_t w = (uint32_t)(g * ECHUNK + mm0 / 32) | ((uint32_t)dzA[g] << 16) |
+                           ((wrap >= 0 ? (uint32_t)wrap : VNOWRAP) << 24);
         t->itab.push_back(make_int4(base[g] + 4 * mm0, g * EZ + mm0,
-                                    d | (v0 << 8) | (v1 << 16) | (absent << 24),
-                                    g * ECHUNK + mm0 / 32));
+                                    d | (v0 << 8) | (v1 << 16) | (absent << 24) |
+                                        (vmode[g] << 25),
+                                    (int)w));
       }
     }
     p->ib[c + 1] = (int)t->itab.size();
@@ -332,9 +455,10 @@ struct QceArgs {
   int nblk, n, iters;
   float alpha;
   // shared-memory layout (byte offsets): syndrome exchange words, per-chunk
-  // row-slot table, per-row masks, column table; the bitmap sits at 0
-  int part_off, rt_off, ri_off, ct_off;
-  int rb[EMAXCL + 1];
+  // row-slot table, per-row info, variable-phase items, heavy-row slots; the
+  // bitmap sits at 0
+  int part_off, rt_off, ri_off, ct_off, ht_off;
+  int ci[EMAXCL + 1];
   int cb[EMAXCL + 1];
   int ib[EMAXCL + 1];
   const int32_t *ccols;
@@ -343,6 +467,7 @@ struct QceArgs {
   const int32_t *rptr;
   const int4 *cdesc;
   const uint8_t *s0;
+  const uint8_t *s0b;
   // optional learned weights, as ldpc_qc.cu: minima become
   // relu(min*w_a - w_b), (w_a, w_b) = (walpha, wbeta)[min(it, wT-1)][
   // dbucket[check degree]]; null -> (alpha, 0), bit-identical to min*alpha
@@ -387,18 +512,17 @@ __device__ __forceinline__ float qce_var_exact(float *col, int s0, float li,
   return tot;
 }
 
-// Variable phase of one bit for a column of d edges (any d >= 1).  The sum
-// runs over slots s0 .. d-1, then 0 .. s0-1; inside a warp the lanes' s0
-// differ little, so with lo/hi = the warp's least/greatest s0 the common
-// parts [hi, d) and [0, lo) are summed unconditionally and only [lo, hi)
-// needs a per-lane choice (adding -0.0 leaves a float sum unchanged).
-// The order of additions is each lane's own, so the sum is exact.
-template <bool TORCH>
-__device__ __forceinline__ float qce_var_generic(float *col, int d, int s0,
-                                                 float li, bool mv) {
+// Sum of one zone's slots of a column (`col` = its first slot, d slots) in
+// the reference order: slots s0 .. d-1, then 0 .. s0-1.  Inside a warp the
+// lanes' s0 differ little, so with lo/hi = the warp's least/greatest s0 the
+// common parts [hi, d) and [0, lo) are summed unconditionally and only
+// [lo, hi) needs a per-lane choice (adding -0.0 leaves a float sum
+// unchanged).  The order of additions is each lane's own, so the sum is
+// exact.
+__device__ __forceinline__ float qce_seg_sum(float acc, const float *col, int d,
+                                             int s0) {
   const int lo = (int)__reduce_min_sync(0xffffffffu, (uint32_t)s0);
   const int hi = (int)__reduce_max_sync(0xffffffffu, (uint32_t)s0);
-  float acc = TORCH ? li : 0.f;
   for (int i = lo; i < hi; ++i) {                  // own tail, first part
     const float m = col[i * EZ];
     acc = __fadd_rn(acc, i >= s0 ? m : -0.f);
@@ -411,6 +535,20 @@ __device__ __forceinline__ float qce_var_generic(float *col, int d, int s0,
     const float m = col[i * EZ];
     acc = __fadd_rn(acc, i < s0 ? m : -0.f);
   }
+  return acc;
+}
+
+// Variable phase of one bit for a column of d edges (any d >= 1) whose
+// first dA slots lie in the accumulator rows and the rest in the identity
+// rows (dA == d for one zone): the reference order is zone A rotated at s0,
+// then zone B rotated at s0b; every slot is rewritten as tot - m.
+template <bool TORCH>
+__device__ __forceinline__ float qce_var_generic(float *col, int d, int dA,
+                                                 int s0, int s0b, float li,
+                                                 bool mv) {
+  float acc = TORCH ? li : 0.f;
+  acc = qce_seg_sum(acc, col, dA, s0);
+  if (dA < d) acc = qce_seg_sum(acc, col + dA * EZ, d - dA, s0b);
   const float tot = TORCH ? acc : __fadd_rn(li, acc);
   if (mv) {
     int i = 0;
@@ -527,8 +665,77 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
   return (int)(synw & 1u);
 }
 
-// NS: compile-time slots per block row (qce_ns); NT: threads per CTA.
-template <bool TORCH, int NS, int NT>
+// Check item of a heavy row (more edges than the compile-time slot count;
+// the accumulator rows of the Type A codes): 32 consecutive checks of the
+// row, its deg slots walked in a loop.  he[j] = {shared::cluster address of
+// slot j's block, shift u << 16 | bitmap word index}; wrapj = the slot that
+// check (0, 0) lacks, or -1.  Pass 1 loads every edge value, forms the
+// syndrome bit, min1/min2/first (strict <, ldpc_kernel.c:121-126) and the
+// sign parity; pass 2 loads each value again (this lane alone writes it,
+// after reading) and stores the message.  Returns the lane's syndrome bit.
+template <bool TORCH>
+__device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wrapj,
+                                            uint32_t lane, int ch,
+                                            const uint32_t *bm, uint32_t dummy,
+                                            bool upd, const QceArgs &a, int it) {
+  const int k0 = ch * 32 + (int)lane;
+  const bool lv = k0 < EZ;
+  const float inf = __int_as_float(0x7f800000);
+  float min1 = inf, min2 = inf;
+  int first = 0;
+  uint32_t par = 0, synw = 0;
+  for (int j = 0; j < deg; ++j) {
+    const uint2 e = he[j];
+    int bb = ch * 32 - (int)(e.y >> 16);
+    bb += bb < 0 ? EZ : 0;
+    const uint32_t x = (uint32_t)bb + lane;
+    const uint32_t o = min(x, x - (uint32_t)EZ);
+    const bool on = lv && !(k0 == 0 && j == wrapj);
+    const float t = dsmem_ld_f32(on ? e.x + 4u * o : dummy);
+    if (on) {
+      const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
+      synw ^= hw >> (o & 31);
+      const float mag = fabsf(t);
+      par ^= t < 0.f ? 1u : 0u;
+      first = mag < min1 ? j : first;
+      min2 = fminf(min2, fmaxf(min1, mag));
+      min1 = fminf(min1, mag);
+    }
+  }
+  if (upd) {
+    float wa = a.alpha, wb = 0.f;
+    if (a.walpha) {
+      const int nl = deg - ((k0 == 0 && wrapj >= 0) ? 1 : 0);
+      const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+      wa = __ldg(a.walpha + wi);
+      wb = __ldg(a.wbeta + wi);
+    }
+    float A = __fsub_rn(__fmul_rn(min1, wa), wb);
+    float B = __fsub_rn(__fmul_rn(min2, wa), wb);
+    A = A > 0.f ? A : 0.f;
+    B = B > 0.f ? B : 0.f;
+    const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
+    for (int j = 0; j < deg; ++j) {
+      const uint2 e = he[j];
+      int bb = ch * 32 - (int)(e.y >> 16);
+      bb += bb < 0 ? EZ : 0;
+      const uint32_t x = (uint32_t)bb + lane;
+      const uint32_t o = min(x, x - (uint32_t)EZ);
+      const bool on = lv && !(k0 == 0 && j == wrapj);
+      if (on) {
+        const uint32_t ad = e.x + 4u * o;
+        const float t = dsmem_ld_f32(ad);
+        const uint32_t sg = par ^ (t < 0.f ? 1u : 0u);
+        dsmem_st_u32(ad, (j == first ? ub : ua) | (sg << 31));
+      }
+    }
+  }
+  return lv ? (int)(synw & 1u) : 0;
+}
+
+// NS: compile-time slots per block row (qce_ns); NT: threads per CTA; TA:
+// the Type A paths (rows above NS, columns in both zones) are compiled in.
+template <bool TORCH, int NS, int NT, bool TA>
 __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   using MASK = typename std::conditional<(NS > 32), unsigned long long,
                                          uint32_t>::type;
@@ -541,26 +748,59 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   uint2 *rtab = reinterpret_cast<uint2 *>(smem + a.rt_off);
   MASK *rinfo = reinterpret_cast<MASK *>(smem + a.ri_off);
   uint4 *itab = reinterpret_cast<uint4 *>(smem + a.ct_off);
+  uint2 *htab = reinterpret_cast<uint2 *>(smem + a.ht_off);
   const uint32_t sm_sa = smem_u32(smem);
   const uint32_t part_sa = smem_u32(part);
   const uint32_t dummy = part_sa + 40 * 4;   // junk word for masked slots
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  const int r0 = a.rb[rank], nr = a.rb[rank + 1] - r0;
+  // check items g = row*12 + chunk in [c0, c0 + ncitems); rows r0 .. r0+nr-1
+  const int c0 = a.ci[rank], ncitems = a.ci[rank + 1] - c0;
+  const int r0 = c0 / ECHUNK;
+  const int nr = ncitems > 0 ? (c0 + ncitems + ECHUNK - 1) / ECHUNK - r0 : 0;
   const int i0 = a.ib[rank], nvitems = a.ib[rank + 1] - i0;
-  const int ncitems = nr * ECHUNK;
   // this lane's cluster address of CTA `lane`'s bitmap (ballot broadcast)
   const uint32_t bm_peer = lane < CL ? dsmem_map(sm_sa, (uint32_t)lane) : 0u;
 
   // ---- per-launch tables ---------------------------------------------------
   // row slot (rl, chunk, j): {shared::cluster address of the slot block in
   // its owner, (first entry index b = (32*chunk - u) mod 360) << 16 | bitmap
-  // word index of the column}; slots past the row degree repeat the last one
+  // word index of the column}; slots past the row degree repeat the last one.
+  // Heavy rows (degree above NS) get one entry per slot in htab instead and
+  // row info {htab offset, wrap slot + 1 (0: none), degree | 1 << 16}.
+  if (tid == 0) {
+    int off = 0;
+    for (int rl = 0; rl < nr; ++rl) {
+      const int rp = __ldg(a.rptr + r0 + rl);
+      const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
+      if (deg <= NS) continue;
+      int wj = 0;
+      for (int q = 0; q < deg; ++q)
+        if (__ldg(a.rdesc + rp + q).x & EWRAP) wj = q + 1;
+      rinfo[3 * rl] = (MASK)off;
+      rinfo[3 * rl + 1] = (MASK)wj;
+      rinfo[3 * rl + 2] = (MASK)(deg | (1 << 16));
+      off += deg;
+    }
+  }
+  __syncthreads();
+  for (int rl = warp; rl < nr; rl += nwarps) {
+    const int rp = __ldg(a.rptr + r0 + rl);
+    const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
+    if (deg <= NS) continue;
+    const int off = (int)rinfo[3 * rl];
+    for (int j = lane; j < deg; j += 32) {
+      const int4 d = __ldg(a.rdesc + rp + j);
+      htab[off + j] = make_uint2(dsmem_map(sm_sa + (uint32_t)d.y, (uint32_t)(d.x & 0xFF)),
+                                 ((uint32_t)d.z << 16) | ((uint32_t)d.w >> 2));
+    }
+  }
   for (int e = tid; e < nr * NS; e += blockDim.x) {
     const int rl = e / NS;
     const int j = e - rl * NS;
     const int rp = __ldg(a.rptr + r0 + rl);
     const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
+    if (deg > NS) continue;
     const int4 d = __ldg(a.rdesc + rp + min(j, deg - 1));
     const uint32_t base = dsmem_map(sm_sa + (uint32_t)d.y, (uint32_t)(d.x & 0xFF));
     const uint32_t wb = (uint32_t)d.w >> 2;
@@ -603,17 +843,20 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       const uint4 iw = itab[w];
       const int d = (int)(iw.z & 0xFFu);
 #pragma unroll
+      // the absent entry: bit 359 = lane 7 of the item's last sub-chunk
+      const int asub = ((iw.z >> 16) & 0xFFu) ? 1 : 0;
+      const int wrapi = (int)(iw.w >> 24);
       for (int sub = 0; sub < 2; ++sub) {
         const uint32_t nval = (iw.z >> (8 + 8 * sub)) & 0xFFu;
         if (nval == 0) break;                         // 32-bit item
         const bool mv = (uint32_t)lane < nval;
-        const bool absent = sub == 1 && (iw.z >> 24) && lane == ABSENT_LANE;
+        const bool absent = sub == asub && ((iw.z >> 24) & 1u) && lane == ABSENT_LANE;
         const float li = mv ? lam[iw.y + 32 * sub + lane] : 0.f;
         float *col = reinterpret_cast<float *>(smem + iw.x) + 32 * sub + lane;
         if (mv)
-          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == 1) ? -0.f : li;
+          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == wrapi) ? -0.f : li;
         const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < 0.f);
-        if (lane < CL) dsmem_st_u32(bm_peer + (iw.w + sub) * 4u, hb);
+        if (lane < CL) dsmem_st_u32(bm_peer + ((iw.w & 0xFFFFu) + sub) * 4u, hb);
       }
     }
     cluster_sync_all();      // (a cluster barrier also orders this CTA)
@@ -626,14 +869,19 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       // ---------------- check phase ----------------------------------------
       int mybad = 0;
       for (int w = warp; w < ncitems; w += nwarps) {
-        const int rl = w / ECHUNK;
-        const int ch = w - rl * ECHUNK;
+        const int gi = c0 + w;
+        const int row = gi / ECHUNK;
+        const int ch = gi - row * ECHUNK;
+        const int rl = row - r0;
         const MASK wm = rinfo[3 * rl + 1];
         const int deg = (int)rinfo[3 * rl + 2];
         const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
         const bool full = wm == 0 && ch < ECHUNK - 1;
         int syn;
-        if (full && deg == NS) {
+        if (TA && (deg >> 16)) {
+          syn = qce_check_heavy<TORCH>(htab + (int)rinfo[3 * rl], deg & 0xFFFF, (int)wm - 1,
+                                       (uint32_t)lane, ch, bm, dummy, upd, a, it);
+        } else if (full && deg == NS) {
           syn = qce_check_item<TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
         } else if (full && deg == NS - 1) {
           syn = qce_check_item<TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
@@ -697,7 +945,9 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       for (int w = warp; w < nvitems; w += nwarps) {
         const uint4 iw = itab[w];
         const int d = (int)(iw.z & 0xFFu);
-        if (d <= 4) {
+        const int mode = (int)((iw.z >> 25) & 3u);
+        const uint32_t bw = iw.w & 0xFFFFu;            // bitmap word
+        if (mode <= VM_EXACT) {
           // 64-bit item: lane L takes bits y + L and y + 32 + L
           const uint32_t nv0 = (iw.z >> 8) & 0xFFu, nv1 = (iw.z >> 16) & 0xFFu;
           const bool mv0 = (uint32_t)lane < nv0, mv1 = (uint32_t)lane < nv1;
@@ -706,7 +956,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           float *col0 = reinterpret_cast<float *>(smem + iw.x) + l0;
           float *col1 = reinterpret_cast<float *>(smem + iw.x) + l1;
           float t0, t1;
-          if (d == 2) {
+          if (mode == VM_PAIR) {
             // dual-diagonal parity column: slots in check order for every
             // bit (u = 0 twice, or u = 0, 1 for the last column, whose wrap
             // entry of bit 359 is absent and holds -0.0)
@@ -716,7 +966,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
             s1 = __fadd_rn(__fadd_rn(s1, a1), b1);
             t0 = TORCH ? s0 : __fadd_rn(li0, s0);
             t1 = TORCH ? s1 : __fadd_rn(li1, s1);
-            const bool absent = (iw.z >> 24) && lane == ABSENT_LANE;
+            const bool absent = ((iw.z >> 24) & 1u) && lane == ABSENT_LANE;
             if (mv0) {
               col0[0] = __fsub_rn(t0, a0);
               col0[EZ] = __fsub_rn(t0, b0);
@@ -730,28 +980,43 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
             if (d == 3) {
               t0 = qce_var_exact<TORCH, 3>(col0, r0s, li0, mv0);
               t1 = qce_var_exact<TORCH, 3>(col1, r1s, li1, mv1);
-            } else {
+            } else if (d == 4) {
               t0 = qce_var_exact<TORCH, 4>(col0, r0s, li0, mv0);
               t1 = qce_var_exact<TORCH, 4>(col1, r1s, li1, mv1);
+            } else if (d == 2) {
+              t0 = qce_var_exact<TORCH, 2>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<TORCH, 2>(col1, r1s, li1, mv1);
+            } else {
+              t0 = qce_var_exact<TORCH, 1>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<TORCH, 1>(col1, r1s, li1, mv1);
             }
           }
           const uint32_t h0 = __ballot_sync(0xffffffffu, mv0 && t0 < 0.f);
           const uint32_t h1 = __ballot_sync(0xffffffffu, mv1 && t1 < 0.f);
           if (lane < CL) {
-            dsmem_st_u32(bm_peer + iw.w * 4u, h0);
-            if (nv1) dsmem_st_u32(bm_peer + (iw.w + 1) * 4u, h1);
+            dsmem_st_u32(bm_peer + bw * 4u, h0);
+            if (nv1) dsmem_st_u32(bm_peer + (bw + 1) * 4u, h1);
           }
         } else {
-          // 32-bit item of a column with more than four edges
+          // 32-bit item: any degree, one zone or both
           const bool mv = (uint32_t)lane < ((iw.z >> 8) & 0xFFu);
           const int ln = mv ? lane : 0;          // lanes past 359 read bit 0
           const int lamidx = (int)iw.y + ln;
           const float li = lam[lamidx];
           float *col = reinterpret_cast<float *>(smem + iw.x) + ln;
           const int s0 = __ldg(a.s0 + lamidx);
-          const float tot = qce_var_generic<TORCH>(col, d, s0, li, mv);
+          int dA = d, s0b = 0;
+          if (TA && mode == VM_GEN2) {
+            dA = (int)((iw.w >> 16) & 0xFFu);
+            s0b = __ldg(a.s0b + lamidx);
+          }
+          const float tot = qce_var_generic<TORCH>(col, d, dA, s0, s0b, li, mv);
+          // the absent wrap entry (bit 359 = lane 7 of the last item) stays
+          // -0.0
+          if (((iw.z >> 24) & 1u) && lane == ABSENT_LANE)
+            col[(int)(iw.w >> 24) * EZ] = -0.f;
           const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
-          if (lane < CL) dsmem_st_u32(bm_peer + iw.w * 4u, hb);
+          if (lane < CL) dsmem_st_u32(bm_peer + bw * 4u, hb);
         }
       }
       cluster_sync_all();
@@ -764,28 +1029,32 @@ typedef void (*QceFn)(const QceArgs);
 
 // NS <= 17 keeps a check's slot addresses and values in the 64 registers of
 // the 1024-thread build; larger NS run 512 threads (128 registers) only.
-template <int NS>
+template <int NS, bool TA>
 static QceFn qce_pick(int semantics, bool big) {
   if constexpr (NS <= 17) {
     if (big)
-      return semantics ? ldpc_qce_kernel<true, NS, 1024>
-                       : ldpc_qce_kernel<false, NS, 1024>;
+      return semantics ? ldpc_qce_kernel<true, NS, 1024, TA>
+                       : ldpc_qce_kernel<false, NS, 1024, TA>;
   }
-  return semantics ? ldpc_qce_kernel<true, NS, 512>
-                   : ldpc_qce_kernel<false, NS, 512>;
+  return semantics ? ldpc_qce_kernel<true, NS, 512, TA>
+                   : ldpc_qce_kernel<false, NS, 512, TA>;
 }
 
-static QceFn qce_fn(int semantics, int dr, int threads) {
+// ta: the plan has identity rows (a Type A code).  Every Type A code of
+// A/322 has identity rows of at most 7 edges, so only the 8-slot kernels
+// carry the Type A paths; another slot count with ta set is unsupported.
+static QceFn qce_fn(int semantics, int dr, int threads, bool ta) {
   const bool big = threads > 512;
+  if (ta) return qce_ns(dr) == 8 ? qce_pick<8, true>(semantics, big) : nullptr;
   switch (qce_ns(dr)) {
-    case 8: return qce_pick<8>(semantics, big);
-    case 10: return qce_pick<10>(semantics, big);
-    case 11: return qce_pick<11>(semantics, big);
-    case 14: return qce_pick<14>(semantics, big);
-    case 17: return qce_pick<17>(semantics, big);
-    case 22: return qce_pick<22>(semantics, big);
-    case 34: return qce_pick<34>(semantics, big);
-    case 56: return qce_pick<56>(semantics, big);
+    case 8: return qce_pick<8, false>(semantics, big);
+    case 10: return qce_pick<10, false>(semantics, big);
+    case 11: return qce_pick<11, false>(semantics, big);
+    case 14: return qce_pick<14, false>(semantics, big);
+    case 17: return qce_pick<17, false>(semantics, big);
+    case 22: return qce_pick<22, false>(semantics, big);
+    case 34: return qce_pick<34, false>(semantics, big);
+    case 56: return qce_pick<56, false>(semantics, big);
     default: return nullptr;
   }
 }
@@ -857,9 +1126,10 @@ struct atsc3_ldpc_qce_plan {
 
 extern "C" {
 
-int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
-                                   const int32_t *rowptr, const int32_t *addr,
-                                   int32_t cluster, atsc3_ldpc_qce_plan **out) {
+int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
+                                    int32_t qb, const int32_t *rowptr,
+                                    const int32_t *addr, int32_t cluster,
+                                    atsc3_ldpc_qce_plan **out) {
   using namespace atsc3;
   ATSC3_ARG(out && rowptr && addr, "null argument");
   *out = nullptr;
@@ -875,7 +1145,7 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
     // rejection (-3, -4 from the build) ends the search with its message
     bool fits = false;
     for (int cl = 1; cl <= EMAXCL; ++cl) {
-      rc = qce_build(n, kldpc, qldpc, rowptr, addr, cl, &h->p, &t);
+      rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cl, &h->p, &t);
       if (rc) break;
       if (h->p.smem <= smax) {
         fits = true;
@@ -887,7 +1157,7 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
       rc = -4;
     }
   } else {
-    rc = qce_build(n, kldpc, qldpc, rowptr, addr, cluster, &h->p, &t);
+    rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cluster, &h->p, &t);
     if (rc == 0 && h->p.smem > smax) {
       set_error("unsupported: per-CTA shared memory above the device limit");
       rc = -4;
@@ -910,12 +1180,19 @@ int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
   if (e == cudaSuccess) e = up((void **)&h->p.d_ccols, t.ccols.data(), t.ccols.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_itab, t.itab.data(), t.itab.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
+  if (e == cudaSuccess) e = up((void **)&h->p.d_s0b, t.s0b.data(), t.s0b.size());
   if (e != cudaSuccess) {
     atsc3_ldpc_qce_plan_destroy(h);
     return cuda_fail(e, "qce plan upload");
   }
   *out = h;
   return 0;
+}
+
+int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
+                                   const int32_t *rowptr, const int32_t *addr,
+                                   int32_t cluster, atsc3_ldpc_qce_plan **out) {
+  return atsc3_ldpc_qce_plan_create2(n, kldpc, qldpc, 0, rowptr, addr, cluster, out);
 }
 
 void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
@@ -926,6 +1203,7 @@ void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
   cudaFree(h->p.d_ccols);
   cudaFree(h->p.d_itab);
   cudaFree(h->p.d_s0);
+  cudaFree(h->p.d_s0b);
   delete h;
 }
 
@@ -944,17 +1222,18 @@ int32_t atsc3_ldpc_qce_plan_info(const atsc3_ldpc_qce_plan *h, int64_t *info) {
   return 0;
 }
 
-int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
-                                   const int32_t *rowptr, const int32_t *addr,
-                                   int32_t cluster, int32_t *meta,
-                                   int32_t *rdesc, int32_t *rptr,
-                                   int32_t *cdesc, int32_t *ccols,
-                                   uint8_t *s0) {
+int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
+                                    int32_t qb, const int32_t *rowptr,
+                                    const int32_t *addr, int32_t cluster,
+                                    int32_t *meta, int32_t *rdesc,
+                                    int32_t *rptr, int32_t *cdesc,
+                                    int32_t *ccols, uint8_t *s0,
+                                    uint8_t *s0b, int32_t *itab) {
   using namespace atsc3;
   ATSC3_ARG(meta && rowptr && addr, "null argument");
   QcePlan p;
   QceTables t;
-  int rc = qce_build(n, kldpc, qldpc, rowptr, addr, cluster, &p, &t);
+  int rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cluster, &p, &t);
   if (rc) return rc;
   meta[0] = (int32_t)t.rdesc.size();
   meta[1] = p.nb;
@@ -968,12 +1247,33 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
     meta[8 + c] = p.rb[c];
     meta[25 + c] = p.cb[c];
   }
+  for (int c = 0; c <= EMAXCL; ++c) meta[42 + c] = p.ci[c];
+  meta[59] = p.heavy;
+  meta[60] = p.dr_light;
+  meta[61] = (int32_t)t.itab.size();
   if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
   if (ccols) std::memcpy(ccols, t.ccols.data(), t.ccols.size() * 4);
   if (s0) std::memcpy(s0, t.s0.data(), t.s0.size());
+  if (s0b) std::memcpy(s0b, t.s0b.data(), t.s0b.size());
+  if (itab) std::memcpy(itab, t.itab.data(), t.itab.size() * 16);
   return 0;
+}
+
+int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
+                                   const int32_t *rowptr, const int32_t *addr,
+                                   int32_t cluster, int32_t *meta,
+                                   int32_t *rdesc, int32_t *rptr,
+                                   int32_t *cdesc, int32_t *ccols,
+                                   uint8_t *s0) {
+  ATSC3_ARG(meta != nullptr, "null argument");
+  int32_t m[64];
+  const int32_t rc = atsc3_ldpc_qce_tables_host2(n, kldpc, qldpc, 0, rowptr, addr, cluster,
+                                                 m, rdesc, rptr, cdesc, ccols, s0,
+                                                 nullptr, nullptr);
+  if (rc == 0 && meta) std::memcpy(meta, m, 42 * sizeof(int32_t));
+  return rc;
 }
 
 // Recognise an A/322 Type B code (360-bit circulants, accumulator parity) in
@@ -1060,9 +1360,9 @@ int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *h, int32_t threads,
                               int32_t semantics, int32_t *out) {
   using namespace atsc3;
   ATSC3_ARG(h && out, "null argument");
-  if (threads <= 0) threads = qce_default_threads(h->p.dr_max);
-  if (qce_ns(h->p.dr_max) > 17) threads = std::min(threads, 512);
-  QceFn fn = qce_fn(semantics, h->p.dr_max, threads);
+  if (threads <= 0) threads = qce_default_threads(h->p.dr_light);
+  if (qce_ns(h->p.dr_light) > 17) threads = std::min(threads, 512);
+  QceFn fn = qce_fn(semantics, h->p.dr_light, threads, h->p.qb > 0);
   ATSC3_ARG(fn != nullptr, "no kernel for this degree");
   int ncl = 0;
   int32_t rc = qce_max_clusters(fn, h->p.cluster, h->p.smem, threads, h->p.device, &ncl);
@@ -1093,10 +1393,10 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   if (nblk == 0) return 0;
   ATSC3_ARG(conv && its && bad, "null status output");
   ATSC3_ARG(llr != nullptr, "null llr");
-  if (threads <= 0) threads = qce_default_threads(p.dr_max);
+  if (threads <= 0) threads = qce_default_threads(p.dr_light);
   ATSC3_ARG(threads == 512 || threads == 1024, "threads must be 512 or 1024");
-  if (qce_ns(p.dr_max) > 17) threads = 512;   // only the 512-thread build
-  QceFn fn = qce_fn(semantics, p.dr_max, threads);
+  if (qce_ns(p.dr_light) > 17) threads = 512;   // only the 512-thread build
+  QceFn fn = qce_fn(semantics, p.dr_light, threads, p.qb > 0);
   if (!fn) {
     set_error("unsupported: block-row degree too high");
     return -4;
@@ -1121,8 +1421,9 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   a.rt_off = p.rt_off;
   a.ri_off = p.ri_off;
   a.ct_off = p.ct_off;
+  a.ht_off = p.ht_off;
   for (int c = 0; c <= EMAXCL; ++c) {
-    a.rb[c] = p.rb[c];
+    a.ci[c] = p.ci[c];
     a.cb[c] = p.cb[c];
   }
   a.ccols = p.d_ccols;
@@ -1132,6 +1433,7 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   a.rptr = p.d_rptr;
   a.cdesc = p.d_cdesc;
   a.s0 = p.d_s0;
+  a.s0b = p.d_s0b;
   if (walpha) {
     ATSC3_ARG(wbeta && dbucket && wT > 0 && wnb > 0,
               "weights need wbeta, dbucket, wT > 0, wnb > 0");

@@ -121,20 +121,23 @@ class QcPlan:
 class QcePlan(QcPlan):
     """Quasi-cyclic plan with the edge-buffer state layout (csrc/ldpc_qce.cu):
     one float32 slot per edge in the distributed shared memory of the edge's
-    column owner, no per-check records.  Same codes, semantics and outputs
-    as QcPlan; cluster 0 picks the smallest cluster that holds a codeword."""
+    column owner, no per-check records.  Serves every A/322 code (Type A and
+    Type B, where QcPlan takes Type B codes with one circulant per block);
+    same semantics and outputs; cluster 0 picks the smallest cluster that
+    holds a codeword."""
 
     kind = "qce"
 
     def __init__(self, rate, n, cluster=0):
         typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
-        if typ != "B":
-            raise ValueError("the quasi-cyclic decoder serves Type B codes")
+        # accumulator / identity block rows: (Q, 0) for Type B, (Q1, Q2) for
+        # Type A
+        qa, qb = (Q2, 0) if typ == "B" else (Q1, Q2)
         rowptr, addr = C.address_rows(rate, n)
         rowptr = np.ascontiguousarray(rowptr, np.int32)
         addr = np.ascontiguousarray(addr, np.int32)
         h = ctypes.c_void_p()
-        N.call("atsc3_ldpc_qce_plan_create", n, K, Q2, rowptr.ctypes.data,
+        N.call("atsc3_ldpc_qce_plan_create2", n, K, qa, qb, rowptr.ctypes.data,
                addr.ctypes.data, int(cluster), ctypes.byref(h))
         self._h = h
         self.n, self.nc, self.dtype = n, n - K, "float32"
@@ -162,19 +165,21 @@ _PLANS_LOCK = threading.Lock()
 
 
 def plan_for(rate, n, dtype="float32", cluster=0, kind="auto"):
-    """Cached plan of an A/322 code.  kind "auto" picks, for the Type B codes
-    in float32, the edge-buffer quasi-cyclic decoder, then the record-layout
-    one, whichever first accepts the code; else the CSR decoder.  kind "qce"
-    or "qc" asks for that decoder (raising if it rejects a Type B code);
-    codes outside its reach (Type A, float64) get the CSR decoder."""
+    """Cached plan of an A/322 code.  kind "auto" picks, in float32, the
+    edge-buffer quasi-cyclic decoder (every code), then the record-layout one
+    (Type B codes with one circulant per block), whichever first accepts the
+    code; else the CSR decoder.  kind "qce" or "qc" asks for that decoder
+    (raising if it rejects a code in its reach); codes outside its reach
+    (float64; Type A for "qc") get the CSR decoder."""
     torch = _torch()
     key = (rate, n, dtype, cluster, kind, torch.cuda.current_device())
     with _PLANS_LOCK:
         p = _PLANS.get(key)
         if p is None:
-            qc_ok = dtype == "float32" and C.ldpc_params(rate, n)[0] == "B"
-            for k, cls in (("qce", QcePlan), ("qc", QcPlan)):
-                if p is None and kind in ("auto", k) and qc_ok:
+            f32 = dtype == "float32"
+            type_b = C.ldpc_params(rate, n)[0] == "B"
+            for k, cls, ok in (("qce", QcePlan, f32), ("qc", QcPlan, f32 and type_b)):
+                if p is None and kind in ("auto", k) and ok:
                     try:
                         p = cls(rate, n, cluster=cluster)
                     except N.FecError as e:

@@ -290,7 +290,7 @@ def inference_weights(alpha, beta, buckets, device="cuda"):
     """(walpha, wbeta, dbucket) device tensors for the quasi-cyclic decoder:
     dbucket[degree] = bucket index of that check degree."""
     torch = _torch()
-    db = np.zeros(64, np.int8)
+    db = np.zeros(256, np.int8)          # every check degree the decoders take (<= 250)
     for i, d in enumerate(buckets):
         db[int(d)] = i
     return (alpha.detach().float().contiguous().to(device),

@@ -561,7 +561,7 @@ def run_uneven(args):
     ub_csr.load(cells, s2s)
     ub_csr.autotune(reps=2)
     ms_csr = timed(ub_csr)
-    # Type B blocks on per-code edge-buffer launches beside the CSR queue
+    # per-code edge-buffer launches (every A/322 code) beside the CSR queue
     ub = UnevenBatch(specs, iters=ITERS, alpha=ALPHA)
     ub.load(cells, s2s)
     table = ub.autotune(reps=2)

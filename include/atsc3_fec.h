@@ -177,23 +177,36 @@ int32_t atsc3_ldpc_qc_decode_weighted(
     int32_t threads, void *stream);
 
 /* ---- quasi-cyclic decoder, edge-buffer layout ------------------------------
- * Same codes, semantics, arguments and outputs as the atsc3_ldpc_qc_*
- * functions above (they replace the same reference entry points:
+ * Same semantics, arguments and outputs as the atsc3_ldpc_qc_* functions
+ * above (they replace the same reference entry points:
  * lab/ldpc_kernel.c:65 ldpc_minsum_f32 and lab/m9_gpu.py:138-220
- * GpuMinSum.decode for the Type B codes), with a different state layout
+ * GpuMinSum.decode), for every A/322 code: Type B through
+ * atsc3_ldpc_qce_plan_create, blocks holding two circulants included, and
+ * Type A through atsc3_ldpc_qce_plan_create2.  Different state layout
  * (csrc/ldpc_qce.cu): one float32 slot per edge, owned by the edge's column,
  * holding the variable-to-check value after the variable phase and the
  * check-to-variable message after the check phase; hard decisions in a
  * bitmap replicated per CTA; no per-check records.  cluster: any size in
  * 1..16 (not only powers of two); 0 picks the smallest cluster whose per-CTA
- * shared memory fits (6 for the 64800-bit codes, 2 for the 16200-bit
- * ones). */
+ * shared memory fits (6 for most 64800-bit codes, 7 for 64800 5/15 and
+ * 7/15, 2 for the 16200-bit ones). */
 typedef struct atsc3_ldpc_qce_plan atsc3_ldpc_qce_plan;
 
 int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
                                    const int32_t *rowptr, const int32_t *addr,
                                    int32_t cluster, atsc3_ldpc_qce_plan **out);
 void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *plan);
+
+/* As atsc3_ldpc_qce_plan_create for both A/322 code types: qa accumulator
+ * block rows (the dual-diagonal part; Q of a Type B code, Q1 of a Type A
+ * code) and qb identity block rows (0 for Type B, Q2 for Type A, whose
+ * address table then also holds the qa rows of the accumulator parity bits,
+ * lab/m3_ldpc.py:119-159 step vii).  A Type A code's few accumulator rows
+ * above the compile-time slot count take the kernel's loop path. */
+int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
+                                    int32_t qb, const int32_t *rowptr,
+                                    const int32_t *addr, int32_t cluster,
+                                    atsc3_ldpc_qce_plan **out);
 
 /* Host only.  Recognise an A/322 Type B code in CSR tables built as
  * lab/m3_ldpc.py:459-482 (_kernel_tables) builds them from
@@ -234,6 +247,21 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
 
 /* out[0] = clusters resident at once, [1] = CTAs per cluster, [2] = shared
  * bytes per CTA, [3] = threads per CTA (threads 0 = the default). */
+/* atsc3_ldpc_qce_tables_host for both code types (qa, qb as in
+ * atsc3_ldpc_qce_plan_create2).  meta (64 ints): [0..41] as
+ * atsc3_ldpc_qce_tables_host, [42..58] check items (row*12 + chunk) of CTA
+ * c from meta[42+c] to meta[43+c], [59] heavy rows present, [60] degree that
+ * sets the compile-time slot count, [61] variable-phase items.  s0b: (n)
+ * rotation start in the identity rows; itab: int4 per variable-phase item.
+ * Array outputs may be null. */
+int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
+                                    int32_t qb, const int32_t *rowptr,
+                                    const int32_t *addr, int32_t cluster,
+                                    int32_t *meta, int32_t *rdesc,
+                                    int32_t *rptr, int32_t *cdesc,
+                                    int32_t *ccols, uint8_t *s0,
+                                    uint8_t *s0b, int32_t *itab);
+
 int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *plan, int32_t threads,
                               int32_t semantics, int32_t *out);
 

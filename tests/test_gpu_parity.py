@@ -381,6 +381,39 @@ def test_qce_16200_codes_vs_oracle(rate, cluster, torch):
                               np.packbits(bits, axis=1))
 
 
+TYPE_A = [(r, n) for n in (16200, 64800) for r in C.RATES
+          if C.ldpc_params(r, n)[0] == "A"]
+
+
+@pytest.mark.parametrize("rate,n", TYPE_A)
+@pytest.mark.parametrize("bigger", [0, 1])
+def test_qce_type_a_codes_vs_oracle(rate, n, bigger, torch):
+    """Edge-buffer decoder on every Type A code: accumulator rows of high
+    degree take the kernel's loop path, identity rows the register path;
+    both semantics, packed and unpacked outputs, at the smallest cluster that
+    holds a codeword and one CTA more, against the oracle."""
+    from atsc3_b200.ldpc import QcePlan, decode_flood
+    plan = QcePlan(rate, n)
+    if bigger:
+        plan = QcePlan(rate, n, cluster=plan.cluster + 1)
+    rng = np.random.default_rng(n + C.RATES.index(rate) + 100 * bigger)
+    tabs = C.csr(rate, n)
+    llr = (rng.standard_normal((5, n)) * 2.0 + 1.2).astype(np.float32)
+    llr[2] = np.abs(llr[2])                          # clean block: its == 0
+    x = torch.from_numpy(llr).cuda()
+    for sem, code in (("kernel", 0), ("torch", 1)):
+        want = oracle.flood(llr, tabs, n, iters=20, alpha=0.75, semantics=code)
+        o = decode_flood(plan, x, iters=20, alpha=0.75, semantics=sem,
+                         want_hard=True)
+        bits = o["bits"].cpu().numpy()
+        assert np.array_equal(bits, want[0]), (rate, n, sem)
+        assert o["its"].cpu().numpy().tolist() == want[2].tolist(), (rate, n, sem)
+        assert o["bad"].cpu().numpy().tolist() == want[3].tolist(), (rate, n, sem)
+        assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
+        assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
+                              np.packbits(bits, axis=1))
+
+
 def test_qce_iters_zero_and_empty_batch(torch):
     """iters=0 only evaluates the syndrome of the channel LLRs (its 0); an
     empty batch launches nothing."""
