@@ -782,8 +782,8 @@ static uint64_t fnv1a(uint64_t h, const void *p, size_t bytes) {
 }
 
 // A code's plan for the host-pointer entry point: the edge-buffer
-// quasi-cyclic plan when the tables are an A/322 Type B code that decoder
-// takes (atsc3_ldpc_qc_detect), else the CSR plan.  Both are bit-exact with
+// quasi-cyclic plan when the tables are an A/322 code (Type A or B) that
+// decoder takes (atsc3_ldpc_qc_detect2), else the CSR plan.  Both are bit-exact with
 // lab/ldpc_kernel.c.
 struct HostPlanEntry {
   atsc3_ldpc_plan *plan;
@@ -839,11 +839,11 @@ int32_t minsum_f32_host(const float *llr, int32_t nblk, int32_t n, int32_t nc,
   }
   if (!plan && !qce) {
     std::vector<int32_t> rowptr((size_t)n / 360 + 1), addr((size_t)nedges + 1);
-    int32_t kq[2] = {0, 0};
-    if (atsc3_ldpc_qc_detect(cptr, cidx, vptr, vedge, n, nc, nedges, kq,
-                             rowptr.data(), addr.data()) == 0) {
-      const int32_t rc = atsc3_ldpc_qce_plan_create(n, kq[0], kq[1], rowptr.data(),
-                                                    addr.data(), 0, &qce);
+    int32_t kq[3] = {0, 0, 0};
+    if (atsc3_ldpc_qc_detect2(cptr, cidx, vptr, vedge, n, nc, nedges, kq,
+                              rowptr.data(), addr.data()) == 0) {
+      const int32_t rc = atsc3_ldpc_qce_plan_create2(n, kq[0], kq[1], kq[2], rowptr.data(),
+                                                     addr.data(), 0, &qce);
       if (rc != 0 && rc != -4) return rc;   // -4: a structure it does not take
       if (rc) qce = nullptr;
     }

@@ -1276,24 +1276,32 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
   return rc;
 }
 
-// Recognise an A/322 Type B code (360-bit circulants, accumulator parity) in
-// CSR tables laid out as lab/m3_ldpc.py:459-482 builds them, and recover its
-// address table.  The tables are accepted only if they are exactly that
-// code's parity-check matrix in the reference's edge order, so the decoders
-// built from the address table see the same edges in the same order:
+// Recognise an A/322 code (360-bit circulants; Type B: accumulator parity;
+// Type A: accumulator rows plus identity rows) in CSR tables laid out as
+// lab/m3_ldpc.py:459-482 builds them, and recover its address table.  The
+// tables are accepted only if they are exactly that code's parity-check
+// matrix in the reference's edge order, so the decoders built from the
+// address table see the same edges in the same order:
 //  * checks ascending, each check's columns strictly ascending;
 //  * vedge = the stable argsort of cidx (each bit's edges by ascending check);
-//  * info bit 360g + mm is on checks (x + mm*Q) mod nc for the checks x of
-//    bit 360g (lab/m3_ldpc.py:166-212 with Q = nc / 360);
-//  * parity bit K + 360j + k is on checks c = j + Q*k and c + 1 (the last
-//    parity bit, c = nc - 1, on c only).
-// Output: kq = {K, Q}, rowptr (K/360 + 1) and addr (the checks of bit 360g,
-// ascending) sized by the caller for n/360 + 1 and nedges entries.  Returns
-// 0, or -4 (not a Type B structure; nothing else is wrong with the tables).
-int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
-                             const int32_t *vptr, const int32_t *vedge,
-                             int32_t n, int32_t nc, int32_t nedges,
-                             int32_t *kq, int32_t *rowptr, int32_t *addr) {
+//  * qb identity block rows = the trailing degree-1 parity bits / 360 (0 for
+//    Type B, whose last parity bit alone has degree 1); qa = nc/360 - qb;
+//  * a table address x maps bit mm of its group to check (x + mm*qa) mod 360qa
+//    (x < 360qa) or 360qa + (x - 360qa + mm*qb) mod 360qb
+//    (lab/m3_ldpc.py:63-66); info bit 360g + mm is on the checks of bit 360g
+//    mapped that way;
+//  * accumulator parity bit K + 360j + k is on checks c = j + qa*k and c + 1
+//    (c + 1 < 360qa) and, for Type A, on the identity-row checks of bit
+//    K + 360j mapped as above (A/322 step vii); identity parity bit
+//    K + 360qa + 360j + k on check 360qa + j + qb*k.
+// Output: kq = {K, qa, qb}; rowptr (K/360 + 1 rows, + qa for Type A) and
+// addr (each row's addresses, ascending), sized by the caller for n/360 + 1
+// and nedges entries.  Returns 0, or -4 (not such a structure; nothing else
+// is wrong with the tables).
+int32_t atsc3_ldpc_qc_detect2(const int32_t *cptr, const int32_t *cidx,
+                              const int32_t *vptr, const int32_t *vedge,
+                              int32_t n, int32_t nc, int32_t nedges,
+                              int32_t *kq, int32_t *rowptr, int32_t *addr) {
   using namespace atsc3;
   ATSC3_ARG(cptr && cidx && vptr && vedge && kq && rowptr && addr, "null argument");
   ATSC3_ARG(n > 0 && nc > 0 && nedges >= 0, "bad size");
@@ -1302,7 +1310,7 @@ int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
     return (int32_t)-4;
   };
   if (n % EZ || nc % EZ || nc >= n) return no("not a 360-circulant code");
-  const int Q = nc / EZ, K = n - nc, nbi = K / EZ;
+  const int K = n - nc, nbi = K / EZ;
   if (cptr[0] != 0 || cptr[nc] != nedges || vptr[0] != 0 || vptr[n] != nedges)
     return no("inconsistent CSR");
   std::vector<int32_t> chk((size_t)nedges);
@@ -1322,37 +1330,81 @@ int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
     const int k = vptr[v] + fill[v]++;
     if (k >= vptr[v + 1] || vedge[k] != e) return no("vedge is not the stable argsort of cidx");
   }
-  // info bits: the checks of bit 360g, rotated by mm*Q
+  int tail = 0;                                  // trailing degree-1 parity bits
+  while (tail < nc && vptr[n - tail] - vptr[n - tail - 1] == 1) ++tail;
+  const int qb = (tail % EZ == 0 && tail < nc) ? tail / EZ : 0;
+  const int qa = nc / EZ - qb, MA = qa * EZ, MB = qb * EZ;
+  auto map = [&](int64_t x, int64_t mm) -> int64_t {
+    return x < MA ? (x + mm * qa) % MA : MA + (x - MA + mm * qb) % MB;
+  };
+  auto col_is = [&](int v, std::vector<int64_t> &want) {
+    std::sort(want.begin(), want.end());
+    if ((int)want.size() != vptr[v + 1] - vptr[v]) return false;
+    for (size_t i = 0; i < want.size(); ++i)
+      if (chk[vedge[vptr[v] + (int)i]] != want[i]) return false;
+    return true;
+  };
+  std::vector<int64_t> want;
+  // table rows: info groups, then (Type A) the accumulator parity groups'
+  // identity-row checks
   rowptr[0] = 0;
-  for (int g = 0; g < nbi; ++g) {
-    const int v0 = g * EZ, d = vptr[v0 + 1] - vptr[v0];
-    const int32_t *X = addr + rowptr[g];
-    for (int i = 0; i < d; ++i) addr[rowptr[g] + i] = chk[vedge[vptr[v0] + i]];
-    rowptr[g + 1] = rowptr[g] + d;
-    for (int mm = 1; mm < EZ; ++mm) {
-      const int v = v0 + mm;
-      if (vptr[v + 1] - vptr[v] != d) return no("info column degrees differ");
-      const int64_t sh = (int64_t)mm * Q;
-      int s = 0;                               // first x with x + sh >= nc
-      while (s < d && X[s] + sh < nc) ++s;
-      for (int i = 0; i < d; ++i) {
-        const int src = i < d - s ? s + i : i - (d - s);
-        const int64_t want = X[src] + sh - (src >= s ? nc : 0);
-        if (chk[vedge[vptr[v] + i]] != want) return no("info column not a circulant shift");
-      }
+  const int nrows = nbi + (qb > 0 ? qa : 0);
+  for (int g = 0; g < nrows; ++g) {
+    const int v0 = g < nbi ? g * EZ : K + (g - nbi) * EZ;
+    int w = rowptr[g];
+    for (int i = vptr[v0]; i < vptr[v0 + 1]; ++i) {
+      const int c = chk[vedge[i]];
+      if (g >= nbi && c < MA) continue;          // the dual diagonal
+      addr[w++] = c;
     }
+    rowptr[g + 1] = w;
   }
-  // parity bits: accumulator chain through the column twist
-  for (int j = 0; j < Q; ++j)
+  for (int g = 0; g < nbi; ++g)
+    for (int mm = 0; mm < EZ; ++mm) {
+      want.clear();
+      for (int i = rowptr[g]; i < rowptr[g + 1]; ++i) want.push_back(map(addr[i], mm));
+      if (!col_is(g * EZ + mm, want)) return no("info column not a circulant shift");
+    }
+  for (int j = 0; j < qa; ++j)
     for (int k = 0; k < EZ; ++k) {
-      const int v = K + EZ * j + k, c = j + Q * k;
-      const int d = vptr[v + 1] - vptr[v];
-      if (d != (c == nc - 1 ? 1 : 2) || chk[vedge[vptr[v]]] != c ||
-          (d == 2 && chk[vedge[vptr[v] + 1]] != c + 1))
-        return no("parity part is not the Type B accumulator");
+      const int c = j + qa * k;
+      want.clear();
+      want.push_back(c);
+      if (c + 1 < MA) want.push_back(c + 1);
+      if (qb > 0)
+        for (int i = rowptr[nbi + j]; i < rowptr[nbi + j + 1]; ++i)
+          want.push_back(map(addr[i], k));
+      if (!col_is(K + EZ * j + k, want)) return no("parity part is not the accumulator");
+    }
+  for (int j = 0; j < qb; ++j)
+    for (int k = 0; k < EZ; ++k) {
+      want.clear();
+      want.push_back(MA + j + (int64_t)qb * k);
+      if (!col_is(K + MA + EZ * j + k, want)) return no("parity part is not the identity");
     }
   kq[0] = K;
-  kq[1] = Q;
+  kq[1] = qa;
+  kq[2] = qb;
+  return 0;
+}
+
+// Type B only (kq = {K, Q}); a Type A code returns -4.
+int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
+                             const int32_t *vptr, const int32_t *vedge,
+                             int32_t n, int32_t nc, int32_t nedges,
+                             int32_t *kq, int32_t *rowptr, int32_t *addr) {
+  using namespace atsc3;
+  ATSC3_ARG(kq != nullptr, "null argument");
+  int32_t k3[3];
+  const int32_t rc = atsc3_ldpc_qc_detect2(cptr, cidx, vptr, vedge, n, nc, nedges,
+                                           k3, rowptr, addr);
+  if (rc) return rc;
+  if (k3[2] != 0) {
+    set_error("a Type A code (use atsc3_ldpc_qc_detect2)");
+    return -4;
+  }
+  kq[0] = k3[0];
+  kq[1] = k3[1];
   return 0;
 }
 

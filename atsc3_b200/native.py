@@ -66,6 +66,8 @@ SIGNATURES = {
                                            c_vp, c_vp]),
     "atsc3_ldpc_qc_detect": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32,
                                      c_i32, c_vp, c_vp, c_vp]),
+    "atsc3_ldpc_qc_detect2": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32,
+                                      c_i32, c_vp, c_vp, c_vp]),
     "atsc3_ldpc_qce_config": (c_i32, [c_vp, c_i32, c_i32, c_vp]),
     "atsc3_ldpc_qce_decode": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32, c_f32,
                                       c_i32, c_vp, c_i64, c_vp, c_i64, c_vp,

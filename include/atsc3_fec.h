@@ -216,12 +216,22 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
  * cidx.  On success kq = {K, Q}, rowptr (K/360 + 1 entries) and addr (the
  * checks of bit 360g, ascending; room for nedges) feed
  * atsc3_ldpc_qce_plan_create.  Returns 0, or -4 when the tables are not that
- * structure.  ldpc_minsum_f32 uses it to send Type B codes to the edge-buffer
- * decoder. */
+ * structure (a Type A code included: see atsc3_ldpc_qc_detect2). */
 int32_t atsc3_ldpc_qc_detect(const int32_t *cptr, const int32_t *cidx,
                              const int32_t *vptr, const int32_t *vedge,
                              int32_t n, int32_t nc, int32_t nedges,
                              int32_t *kq, int32_t *rowptr, int32_t *addr);
+
+/* As atsc3_ldpc_qc_detect for both code types: kq = {K, qa, qb} (qa
+ * accumulator and qb identity block rows; qb = 0 for Type B), found from the
+ * trailing degree-1 parity bits (the identity part of a Type A code).
+ * rowptr has K/360 + 1 rows, plus qa rows for a Type A code (the identity-row
+ * addresses of the accumulator parity bits, A/322 step vii); the outputs
+ * feed atsc3_ldpc_qce_plan_create2.  ldpc_minsum_f32 uses it. */
+int32_t atsc3_ldpc_qc_detect2(const int32_t *cptr, const int32_t *cidx,
+                              const int32_t *vptr, const int32_t *vedge,
+                              int32_t n, int32_t nc, int32_t nedges,
+                              int32_t *kq, int32_t *rowptr, int32_t *addr);
 
 /* info[0]=n [1]=K [2]=Q [3]=cluster [4]=shared bytes per CTA [5]=max
  * block-row degree [6]=max block-column degree [7]=table bytes [8]=most edge

@@ -3,8 +3,8 @@ lab/ldpc_kernel.c:65) on every A/322 code and under concurrent callers.
 
 The reference calls it from a ThreadPoolExecutor with ctypes releasing the GIL
 (lab/m3_ldpc.py:409-415, lab/m9_fast.py:893-925), so the entry point must be
-thread-safe; Type B codes go to the edge-buffer quasi-cyclic decoder (the
-tables are recognised by atsc3_ldpc_qc_detect), the other codes to the CSR
+thread-safe; A/322 codes go to the edge-buffer quasi-cyclic decoder (the
+tables are recognised by atsc3_ldpc_qc_detect2), any other matrix to the CSR
 decoder.  Either way the outputs equal the oracle's field by field."""
 import ctypes
 from concurrent.futures import ThreadPoolExecutor
@@ -64,12 +64,34 @@ def test_every_code_through_the_host_abi(n, torch):
         assert same(minsum_f32(llr, tabs, n, 6, 0.8), want), (rate, n)
 
 
+def random_code(n=3000, nc=1500, seed=5):
+    """A sparse parity-check matrix with no circulant structure (column
+    degree 3, row degree about 6): the host ABI decodes it with the CSR
+    kernel."""
+    rng = np.random.default_rng(seed)
+    checks = [[] for _ in range(nc)]
+    for v in range(n):
+        for c in rng.choice(nc, 3, replace=False):
+            checks[c].append(v)
+    return C.csr_from_checks([sorted(c) for c in checks], n)
+
+
+def test_non_qc_code_through_the_host_abi(torch):
+    tabs = random_code()
+    llr = case("x", 3000, 9, nblk=4)
+    want = oracle.flood(llr, tabs, 3000, iters=12, alpha=0.75)
+    assert same(minsum_f32(llr, tabs, 3000, 12, 0.75), want)
+
+
 def test_concurrent_callers(torch):
-    """Eight threads, mixed codes (the edge-buffer decoder for the Type B
-    codes, the CSR decoder for the Type A ones, 64800 7/15 and 16200 3/15),
-    each call checked against the oracle; then the same calls again, all at
+    """Eight threads, mixed codes (Type A and Type B on the edge-buffer
+    decoder, a matrix without circulant structure on the CSR decoder), each
+    call checked against the oracle; then the same calls again, all at
     once."""
     jobs = []
+    tabs = random_code()
+    llr = case("x", 3000, 77, nblk=3)
+    jobs.append((llr, tabs, 3000, oracle.flood(llr, tabs, 3000, iters=8, alpha=0.75)))
     for i, (rate, n) in enumerate([("10/15", 64800), ("7/15", 64800), ("6/15", 16200),
                                    ("11/15", 16200), ("8/15", 64800), ("3/15", 16200),
                                    ("13/15", 64800), ("9/15", 16200)]):

@@ -14,16 +14,15 @@ from atsc3_b200 import native as N
 CODES = [(r, n) for n in (16200, 64800) for r in C.RATES]
 
 
-def detect(cptr, cidx, vptr, vedge, n):
+def detect(cptr, cidx, vptr, vedge, n, fn="atsc3_ldpc_qc_detect"):
     nc = len(cptr) - 1
     ne = len(cidx)
-    kq = np.zeros(2, np.int32)
+    kq = np.zeros(3, np.int32)
     rowptr = np.zeros(n // 360 + 1, np.int32)
     addr = np.zeros(max(ne, 1), np.int32)
     arrs = [np.ascontiguousarray(a, np.int32) for a in (cptr, cidx, vptr, vedge)]
-    rc = N.lib().atsc3_ldpc_qc_detect(*[a.ctypes.data for a in arrs], n, nc, ne,
-                                      kq.ctypes.data, rowptr.ctypes.data,
-                                      addr.ctypes.data)
+    rc = getattr(N.lib(), fn)(*[a.ctypes.data for a in arrs], n, nc, ne,
+                              kq.ctypes.data, rowptr.ctypes.data, addr.ctypes.data)
     return rc, kq, rowptr, addr
 
 
@@ -46,7 +45,7 @@ def test_detects_type_b_and_recovers_addresses(rate, n):
         assert rc == -4
         return
     assert rc == 0, N.lib().atsc3_last_error()
-    assert kq.tolist() == [K, Q2]
+    assert kq[:2].tolist() == [K, Q2]
     want = reference_addresses(rate, n)
     assert rowptr[K // 360] == sum(len(w) for w in want)
     got = [addr[rowptr[g]:rowptr[g + 1]].tolist() for g in range(K // 360)]
@@ -96,3 +95,38 @@ def test_refuses_inconsistent_tables_without_reading_past_them():
     vp = vptr.copy()
     vp[-1] += 1
     assert detect(cptr, cidx, vp, vedge, n)[0] == -4
+
+
+@pytest.mark.parametrize("rate,n", CODES)
+def test_detect2_both_types(rate, n):
+    """atsc3_ldpc_qc_detect2 recognises every A/322 code: Type B with qb = 0
+    as above, Type A with qa = Q1, qb = Q2 and the address table's rows for
+    the information groups and the accumulator parity groups."""
+    typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+    rc, kq, rowptr, addr = detect(*C.csr(rate, n), n, fn="atsc3_ldpc_qc_detect2")
+    assert rc == 0, N.lib().atsc3_last_error()
+    nrows = K // 360 + (Q1 if typ == "A" else 0)
+    assert kq.tolist() == ([K, Q2, 0] if typ == "B" else [K, Q1, Q2])
+    want = reference_addresses(rate, n)
+    assert len(want) == nrows
+    got = [addr[rowptr[g]:rowptr[g + 1]].tolist() for g in range(nrows)]
+    assert got == want
+
+
+def test_detect2_refuses_a_broken_type_a_code():
+    n = 16200
+    cptr, cidx, vptr, vedge = C.csr("3/15", n)
+    K = C.kldpc("3/15", n)
+    checks = [list(cidx[cptr[c]:cptr[c + 1]]) for c in range(len(cptr) - 1)]
+    # an identity parity bit moved onto the neighbouring check
+    last = len(checks) - 1
+    bit = [x for x in checks[last] if x >= K][0]
+    checks[last].remove(bit)
+    checks[last - 1] = sorted(checks[last - 1] + [bit])
+    assert detect(*C.csr_from_checks(checks, n), n, fn="atsc3_ldpc_qc_detect2")[0] == -4
+    # one info edge of an accumulator row shifted to the next column
+    checks = [list(cidx[cptr[c]:cptr[c + 1]]) for c in range(len(cptr) - 1)]
+    c0 = checks[3][0]
+    checks[3][0] = c0 + 1 if c0 + 1 not in checks[3] else c0 + 2
+    checks[3].sort()
+    assert detect(*C.csr_from_checks(checks, n), n, fn="atsc3_ldpc_qc_detect2")[0] == -4
