@@ -65,6 +65,12 @@ __host__ __device__ constexpr int qce_ns(int dr) {
        : dr <= 17 ? 17 : dr <= 22 ? 22 : dr <= 34 ? 34 : dr <= 56 ? 56 : 0;
 }
 
+// The same for the identity rows of a Type A code (3 to 7 edges in A/322):
+// 4 and 6 slots keep the short rows unmasked.
+__host__ __device__ constexpr int qce_ns_a(int dr) {
+  return dr <= 4 ? 4 : dr <= 6 ? 6 : dr <= 8 ? 8 : 0;
+}
+
 struct QcePlan {
   int n = 0, K = 0, Q = 0, nb = 0;
   int qa = 0, qb = 0;           // accumulator / identity block rows
@@ -194,13 +200,10 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   // largest identity row for a Type A code, whose few accumulator rows of
   // higher degree take the kernel's loop path ("heavy" rows)
   const int dlight = QB > 0 ? drb : drm;
-  const int ns = qce_ns(dlight);
+  const int ns = QB > 0 ? qce_ns_a(dlight) : qce_ns(dlight);
   if (ns == 0) {
-    set_error("unsupported: block-row degree above 56");
-    return -4;
-  }
-  if (QB > 0 && ns != 8) {
-    set_error("unsupported: identity rows of more than 8 edges");
+    set_error(QB > 0 ? "unsupported: identity rows of more than 8 edges"
+                     : "unsupported: block-row degree above 56");
     return -4;
   }
   std::vector<int> rdeg(Q);
@@ -1040,12 +1043,18 @@ static QceFn qce_pick(int semantics, bool big) {
                    : ldpc_qce_kernel<false, NS, 512, TA>;
 }
 
-// ta: the plan has identity rows (a Type A code).  Every Type A code of
-// A/322 has identity rows of at most 7 edges, so only the 8-slot kernels
-// carry the Type A paths; another slot count with ta set is unsupported.
+// ta: the plan has identity rows (a Type A code); its kernels carry the
+// Type A paths and take 4, 6 or 8 slots (qce_ns_a of the identity rows).
 static QceFn qce_fn(int semantics, int dr, int threads, bool ta) {
   const bool big = threads > 512;
-  if (ta) return qce_ns(dr) == 8 ? qce_pick<8, true>(semantics, big) : nullptr;
+  if (ta) {
+    switch (qce_ns_a(dr)) {
+      case 4: return qce_pick<4, true>(semantics, big);
+      case 6: return qce_pick<6, true>(semantics, big);
+      case 8: return qce_pick<8, true>(semantics, big);
+      default: return nullptr;
+    }
+  }
   switch (qce_ns(dr)) {
     case 8: return qce_pick<8, false>(semantics, big);
     case 10: return qce_pick<10, false>(semantics, big);
