@@ -20,7 +20,9 @@ Contents (reference file:line each restates):
   1096-1115) or the per-row estimate.
 * ``bch_syndrome`` -- lab/m6_bicm.py:269-280 (polynomial remainder).
 * ``flood`` -- ``ldpc_oracle.c`` (lab/ldpc_kernel.c semantics and the
-  float64 / torch semantics); ``flood_ref`` -- the reference kernel itself.
+  float64 / torch semantics); ``flood_ref`` -- the reference kernel itself;
+  ``flood_weighted`` -- the same kernel semantics with per-iteration,
+  per-check-degree scale/offset minima (the learned decoder), numpy.
 """
 from __future__ import annotations
 
@@ -104,6 +106,81 @@ def flood(llr, tables, n, iters=50, alpha=0.75, semantics=0, dtype=np.float32):
     if rc != 0:
         raise RuntimeError(f"oracle decode returned {rc}")
     return bits, conv.astype(bool), its, bad
+
+
+def flood_weighted(llr, tables, n, walpha, wbeta, dbucket, iters=50):
+    """Weighted flooding min-sum, kernel semantics (lab/ldpc_kernel.c:95-142
+    with the check messages of the learned decoder): per iteration t and
+    check of degree d, the minima become relu(min * walpha[min(t, T-1),
+    dbucket[d]] - wbeta[...]) (each float32 op rounded once, no fused
+    multiply-add); first minimum by strict <, sign = parity ^ (v < 0);
+    variable sums from +0 in vedge order, then + llr.  numpy float32,
+    vectorised per check degree and per variable degree.  With walpha = alpha
+    and wbeta = 0 it is ``flood(..., alpha)`` bit for bit (tests pin that).
+    Returns (bits, conv bool, its, bad)."""
+    cptr, cidx, vptr, vedge = [np.asarray(t, np.int64) for t in tables]
+    walpha = np.asarray(walpha, np.float32)
+    wbeta = np.asarray(wbeta, np.float32)
+    dbucket = np.asarray(dbucket, np.int64)
+    T = walpha.shape[0]
+    nc, ne = len(cptr) - 1, len(cidx)
+    cdeg = np.diff(cptr)
+    chk = np.repeat(np.arange(nc), cdeg)
+    vdeg = np.diff(vptr)
+    cgroups = [(d, np.nonzero(cdeg == d)[0]) for d in np.unique(cdeg)]
+    vgroups = [(d, np.nonzero(vdeg == d)[0]) for d in np.unique(vdeg)]
+    nblk = llr.shape[0]
+    bits = np.zeros((nblk, n), np.uint8)
+    conv = np.zeros(nblk, bool)
+    its = np.zeros(nblk, np.int32)
+    bad = np.zeros(nblk, np.int32)
+    f32 = np.float32
+    for b in range(nblk):
+        lam = np.asarray(llr[b], f32)
+        tot = lam.copy()
+        m = np.zeros(ne, f32)
+        for it in range(iters + 1):
+            hard = (tot < 0).astype(np.int64)
+            par = np.bitwise_xor.reduceat(hard[cidx], cptr[:-1]) if ne else np.zeros(nc, np.int64)
+            badct = int(par.sum())
+            if badct == 0:
+                conv[b], its[b], bad[b] = True, it, 0
+                break
+            if it == iters:
+                its[b], bad[b] = iters, badct
+                break
+            v = (tot[cidx] - m).astype(f32)
+            newm = np.empty(ne, f32)
+            ti = min(it, T - 1)
+            for d, cs in cgroups:
+                idx = cptr[cs][:, None] + np.arange(d)[None, :]
+                vv = v[idx]
+                mag = np.abs(vv)
+                first = np.argmin(mag, axis=1)
+                rows = np.arange(len(cs))
+                min1 = mag[rows, first]
+                mag2 = mag.copy()
+                mag2[rows, first] = np.inf
+                min2 = mag2.min(axis=1) if d > 1 else np.full(len(cs), np.inf, f32)
+                wa = walpha[ti, dbucket[d]]
+                wb = wbeta[ti, dbucket[d]]
+                A = np.maximum(f32(min1 * wa) - wb, f32(0)).astype(f32)
+                B = np.maximum(f32(min2 * wa) - wb, f32(0)).astype(f32)
+                ng = vv < 0
+                parity = np.bitwise_xor.reduce(ng.astype(np.int64), axis=1)
+                mg = np.where(np.arange(d)[None, :] == first[:, None], B[:, None], A[:, None])
+                sg = (parity[:, None] ^ ng.astype(np.int64)).astype(bool)
+                newm[idx] = np.where(sg, -mg, mg).astype(f32)
+            m = newm
+            s = np.zeros(n, f32)
+            for d, vs in vgroups:
+                acc = np.zeros(len(vs), f32)
+                for k in range(d):
+                    acc = (acc + m[vedge[vptr[vs] + k]]).astype(f32)
+                s[vs] = acc
+            tot = (lam + s).astype(f32)
+        bits[b] = (tot < 0)
+    return bits, conv, its, bad
 
 
 def flood_ref(llr, tables, n, iters=50, alpha=0.75, threads=1):
