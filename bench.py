@@ -134,7 +134,7 @@ def make_frames(nframes, seed, device):
     return cells, sig, nblk, tx.kp
 
 
-def cpu_reference_decode(cells, sig, threads):
+def cpu_reference_decode(cells, sig, threads, mod=None, rate=None, n=None):
     """The reference's CPU path on host cores: float32 demap (numpy, the
     lab/m44_ldm.py:2431-2494 arithmetic) with per-cell sigma2, de-interleave,
     the reference's compiled lab/ldpc_kernel.c (thread sub-batches, as
@@ -143,20 +143,23 @@ def cpu_reference_decode(cells, sig, threads):
     import oracle
     from concurrent.futures import ThreadPoolExecutor
     from atsc3_b200 import codes as C
-    pts = C.points_for(MOD, RATE)
-    nb = C.MOD_BITS[MOD]
-    lq = C.bicm_map(N_INNER, MOD, RATE)
-    tabs = C.csr(RATE, N_INNER)
-    K = C.kldpc(RATE, N_INNER)
+    mod, rate, n = mod or MOD, rate or RATE, n or N_INNER
+    pts = C.points_for(mod, rate)
+    nb = C.MOD_BITS[mod]
+    lq = C.bicm_map(n, mod, rate)
+    tabs = C.csr(rate, n)
+    K = C.kldpc(rate, n)
     nblk = cells.shape[0]
+    scalar = np.ndim(sig) == 0
     with ThreadPoolExecutor(threads) as ex:
         q = np.concatenate(list(ex.map(
-            lambda b: oracle.demap(cells[b:b + 1], pts, nb, sig[b:b + 1]),
+            lambda b: oracle.demap(cells[b:b + 1], pts, nb,
+                                   sig if scalar else sig[b:b + 1]),
             range(nblk))))
-    lam = oracle.deinterleave(q, lq, N_INNER)
-    bits, conv, its, bad = oracle.flood_ref(lam, tabs, N_INNER, iters=ITERS,
+    lam = oracle.deinterleave(q, lq, n)
+    bits, conv, its, bad = oracle.flood_ref(lam, tabs, n, iters=ITERS,
                                             alpha=ALPHA, threads=threads)
-    syn = oracle.bch_syndrome_fast(bits[:, :K], N_INNER)
+    syn = oracle.bch_syndrome_fast(bits[:, :K], n)
     return sum(1 for s in syn if s == 0), its
 
 
@@ -650,6 +653,58 @@ def run_frame_ti(args):
             "data": "synthetic", "dtype": "f32"}
 
 
+def run_plain(args):
+    """The reference's own CPU-runnable plain case: 32 blocks of 64800-bit
+    rate 10/15 with 256-NUC, AWGN at Es/N0 = 20 dB, the noise variance
+    supplied (scalar), alpha 0.75, at most 50 iterations.  The GPU pipeline
+    (demap -> LDPC -> BCH) on device-resident cells, and the same blocks
+    through the reference's CPU path on the host cores (float32 demap,
+    lab/ldpc_kernel.c over all threads, packed BCH)."""
+    import time
+    import torch
+    from atsc3_b200 import codes as C
+    from atsc3_b200 import synth
+    from atsc3_b200.pipeline import FecPipeline
+    n, mod, rate, nblk = 64800, "256QAM", "10/15", 32
+    tx = synth.Transmitter(n, mod, rate, device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(args.seed)
+    pay = torch.randint(0, 2, (nblk, tx.kp), generator=g, device="cuda", dtype=torch.uint8)
+    x, _ = tx.encode(pay)
+    y, s2 = synth.channel(x, 20.0, "awgn", g)
+    s2 = float(s2)
+    pipe = FecPipeline(n, mod, rate, iters=ITERS, alpha=ALPHA)
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    for _ in range(args.warmup):
+        pipe.decode(y, sigma2=s2)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        o = pipe.decode(y, sigma2=s2)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ok = int(o["ok"].sum())
+    same = bool(torch.equal(o["payload"][:, :tx.kp // 8],
+                            torch.from_numpy(np.packbits(pay.cpu().numpy(), axis=1)).cuda()))
+    its = o["its"].float().mean().item()
+    kp = C.kpayload(rate, n)
+    threads = os.cpu_count() or 1
+    cells = y.cpu().numpy()
+    t0 = time.perf_counter()
+    nok_cpu, its_cpu = cpu_reference_decode(cells, s2, threads, mod=mod, rate=rate, n=n)
+    cpu_s = time.perf_counter() - t0
+    return {"metric": "decoded info Mbit/s, plain case (32 blocks 64800 10/15 256-NUC, 20 dB AWGN)",
+            "value": nblk * kp / (ms / 1e3) / 1e6, "unit": "Mbit/s", "ms_per_step": ms,
+            "steps": args.steps, "warmup": args.warmup, "bch_ok": ok,
+            "payload_equals_sent": same, "mean_iters": its,
+            "cpu_reference": {"value": nblk * kp / cpu_s / 1e6, "unit": "Mbit/s",
+                              "cores": threads, "bch_ok": int(nok_cpu),
+                              "mean_iters": float(np.mean(its_cpu)),
+                              "what": "float32 demap numpy + lab/ldpc_kernel.c over all host threads + packed BCH, same 32 blocks"},
+            "data": "synthetic", "dtype": "f32"}
+
+
 def run_codes(args):
     """Every A/322 code (16200 and 64800, rates 2/15..13/15): the LDPC launch
     alone on 16-NUC blocks at the code's measured threshold + 1 dB (AWGN,
@@ -712,7 +767,7 @@ def run_codes(args):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="frame",
-                    choices=["frame", "uneven", "frame_ti", "codes"])
+                    choices=["frame", "uneven", "frame_ti", "codes", "plain"])
     ap.add_argument("--blocks", type=int, default=512)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=128)
@@ -742,6 +797,10 @@ def main(argv=None):
     if a.workload == "codes":
         if rank == 0:
             print(json.dumps(run_codes(a)), flush=True)
+        return 0
+    if a.workload == "plain":
+        if rank == 0:
+            print(json.dumps(run_plain(a)), flush=True)
         return 0
     if a.impl == "reference":
         line = run_reference(a, rank, world)
