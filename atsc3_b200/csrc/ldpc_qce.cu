@@ -139,6 +139,15 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   // code, one per accumulator parity column (its bits feed the identity
   // rows, A/322 6.1.3.1 step vii); accumulator address x -> (row, shift)
   const int ntab = nbi + (QB > 0 ? QA : 0);
+  if (rowptr[0] != 0) {
+    set_error("invalid argument: rowptr[0] must be 0");
+    return -3;
+  }
+  for (int g = 0; g < ntab; ++g)
+    if (rowptr[g + 1] < rowptr[g]) {
+      set_error("invalid argument: rowptr must not decrease");
+      return -3;
+    }
   for (int g = 0; g < ntab; ++g)
     for (int e = rowptr[g]; e < rowptr[g + 1]; ++e) {
       const int x = addr[e];

@@ -86,3 +86,36 @@ def test_python_wrappers_refuse_bad_inputs():
         T.HybridTI(4, 3, n_virtual=3)
     with pytest.raises(ValueError):
         T.ConvolutionalTI(8, -1)
+
+
+def test_type_a_tables_refused():
+    """The two-zone builder refuses a zone split that does not add up to the
+    parity length, a decreasing rowptr, a nonzero rowptr[0], and an identity
+    address beyond the parity range; atsc3_ldpc_qc_detect2 refuses null
+    outputs."""
+    rate, n = "7/15", 64800
+    typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+    rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows(rate, n)]
+    meta = np.zeros(64, np.int32)
+    f = L.atsc3_ldpc_qce_tables_host2
+
+    def call(qa, qb, rp, ad):
+        return f(n, K, qa, qb, rp.ctypes.data, ad.ctypes.data, 7, meta.ctypes.data,
+                 None, None, None, None, None, None, None)
+
+    assert call(Q1, Q2, rowptr, addr) == 0
+    assert call(Q1 + 1, Q2, rowptr, addr) == -3           # zones do not add up
+    assert call(0, Q2 + Q1, rowptr, addr) == -3           # no accumulator rows
+    rp = rowptr.copy()
+    rp[5] = rp[4] - 1
+    assert call(Q1, Q2, rp, addr) == -3                   # decreasing rowptr
+    rp = rowptr.copy()
+    rp[0] = 1
+    assert call(Q1, Q2, rp, addr) == -3
+    bad = addr.copy()
+    bad[-1] = n - K
+    assert call(Q1, Q2, rowptr, bad) == -3                # past the parity range
+    cptr, cidx, vptr, vedge = [np.ascontiguousarray(t, np.int32) for t in C.csr(rate, n)]
+    assert L.atsc3_ldpc_qc_detect2(cptr.ctypes.data, cidx.ctypes.data, vptr.ctypes.data,
+                                   vedge.ctypes.data, n, len(cptr) - 1, len(cidx),
+                                   None, None, None) == -3
