@@ -80,7 +80,10 @@ struct QcePlan {
   int heavy = 0;                // rows above the compile-time slot count
   int64_t table_bytes = 0;
   int rb[EMAXCL + 1] = {0};     // block rows CTA c owns (column placement)
-  int ci[EMAXCL + 1] = {0};     // check items (row*12 + chunk) of CTA c
+  int ci[EMAXCL + 1] = {0};     // check items (row*12 + chunk) of CTA c; with
+                                // heavy rows: its light items only
+  int hoff[EMAXCL + 1] = {0};   // heavy items of CTA c: hitems[hoff[c] .. hoff[c+1])
+  int nhrows = 0;               // heavy rows (the accumulator rows) or 0
   int ib[EMAXCL + 1] = {0};     // variable-phase items of CTA c in d_itab
   int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
@@ -90,6 +93,7 @@ struct QcePlan {
   int4 *d_cdesc = nullptr;      // per column
   uint8_t *d_s0 = nullptr;      // (nb*360) rotation start (zone A / only zone)
   uint8_t *d_s0b = nullptr;     // (nb*360) rotation start in zone B
+  int16_t *d_hitems = nullptr;  // heavy check items, grouped by CTA
 };
 
 // Block rows: rows 0 .. qa-1 are the accumulator rows (check r + qa*k, the
@@ -112,6 +116,7 @@ struct QceTables {
   std::vector<int32_t> ccols;
   std::vector<int4> itab;
   std::vector<uint8_t> s0, s0b;
+  std::vector<int16_t> hitems;
 };
 
 // variable-phase item modes (bits 25-26 of the item's z word)
@@ -250,31 +255,58 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     return -4;
   }
   // Check items (row*12 + chunk) per CTA.  Without heavy rows: contiguous
-  // equal row ranges.  With heavy rows: contiguous item ranges of equal work
-  // (each item costs its row's degree), so the few heavy rows spread over
-  // the cluster.
+  // equal row ranges.  With heavy rows (the accumulator rows of a Type A
+  // code, all of them): their items are dealt round-robin over the cluster
+  // (a heavy item is long and runs in one warp, so no CTA should hold many),
+  // then each CTA takes a contiguous range of the light items that evens out
+  // the estimated work (a heavy item ~ 35 instructions per edge over two
+  // passes, a light item ~ 25 per compile-time slot + 30).
   const int per = (Q + cluster - 1) / cluster;
+  t->hitems.clear();
+  p->hoff[0] = 0;
+  p->nhrows = 0;
   if (!heavy) {
     for (int c = 0; c <= cluster; ++c) p->ci[c] = std::min(Q, c * per) * ECHUNK;
+    for (int c = 1; c <= EMAXCL; ++c) p->hoff[c] = 0;
   } else {
-    int64_t work = 0;
-    for (int r = 0; r < Q; ++r) work += (int64_t)(rdeg[r] + 2) * ECHUNK;
-    p->ci[0] = 0;
-    int64_t acc = 0;
-    int c = 1;
-    for (int it = 0; it < Q * ECHUNK && c < cluster; ++it) {
-      acc += rdeg[it / ECHUNK] + 2;
-      while (c < cluster && acc * cluster >= work * c) p->ci[c++] = it + 1;
+    for (int r = 0; r < Q; ++r)
+      if ((rdeg[r] > ns) != (r < QA)) {
+        set_error("unsupported: heavy rows other than the accumulator rows");
+        return -4;
+      }
+    p->nhrows = QA;
+    std::vector<int64_t> hc(cluster, 0);
+    std::vector<std::vector<int>> hl(cluster);
+    for (int i = 0; i < QA * ECHUNK; ++i) {
+      hl[i % cluster].push_back(i);
+      hc[i % cluster] += 35 * rdeg[i / ECHUNK];
     }
-    while (c < cluster) p->ci[c++] = Q * ECHUNK;
-    p->ci[cluster] = Q * ECHUNK;
+    for (int c = 0; c < cluster; ++c) {
+      for (int i : hl[c]) t->hitems.push_back((int16_t)i);
+      p->hoff[c + 1] = (int)t->hitems.size();
+    }
+    for (int c = cluster + 1; c <= EMAXCL; ++c) p->hoff[c] = p->hoff[cluster];
+    const int64_t cl = 25 * ns + 30;
+    const int L0 = QA * ECHUNK, L1 = Q * ECHUNK;
+    int64_t total = (int64_t)(L1 - L0) * cl;
+    for (int c = 0; c < cluster; ++c) total += hc[c];
+    const double target = (double)total / cluster;
+    double acc = 0.0;
+    p->ci[0] = L0;
+    for (int c = 0; c < cluster; ++c) {
+      acc += std::max(0.0, target - (double)hc[c]);
+      int b = L0 + (int)(acc / (double)cl + 0.5);
+      p->ci[c + 1] = std::min(L1, std::max(p->ci[c], b));
+    }
+    p->ci[cluster] = L1;
   }
-  for (int c = cluster + 1; c <= EMAXCL; ++c) p->ci[c] = Q * ECHUNK;
+  for (int c = cluster + 1; c <= EMAXCL; ++c) p->ci[c] = p->ci[cluster];
   // the row's owner for column placement: the CTA holding its chunk 0
   std::vector<int> rowown(Q, 0);
   for (int c = 0; c < cluster; ++c)
     for (int r = (p->ci[c] + ECHUNK - 1) / ECHUNK; r * ECHUNK < p->ci[c + 1]; ++r)
       rowown[r] = c;
+  for (int r = 0; r < p->nhrows; ++r) rowown[r] = (r * ECHUNK) % cluster;
   // Column -> CTA assignment.  An edge is local when its column lives in the
   // CTA that owns its row, and a local edge saves the check phase a remote
   // load and a remote store.  Parity column j of the accumulator (edges in
@@ -353,26 +385,25 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   }
   // per CTA: rows touched by its check items (all 12 chunks get row-slot
   // entries) and heavy-row slot entries
-  int maxrows = 0, maxheavy = 0;
+  int maxrows = 0;
   for (int c = 0; c < cluster; ++c) {
     if (p->ci[c + 1] <= p->ci[c]) continue;
     const int r0 = p->ci[c] / ECHUNK, r1 = (p->ci[c + 1] - 1) / ECHUNK;
     maxrows = std::max(maxrows, r1 - r0 + 1);
-    int h = 0;
-    for (int r = r0; r <= r1; ++r)
-      if (rdeg[r] > ns) h += rdeg[r];
-    maxheavy = std::max(maxheavy, h);
   }
+  // every CTA holds all heavy rows: an int4 of row info each, then 8 B per slot
+  int heavy_bytes = 16 * p->nhrows;
+  for (int r = 0; r < p->nhrows; ++r) heavy_bytes += 8 * rdeg[r];
   // shared memory: bitmap | syndrome exchange | row-slot table (per row,
   // chunk and slot, 8 B) | row info (3 words per row) | variable-phase item
-  // table (16 B per item) | heavy-row slot table (8 B per slot) | slots
+  // table (16 B per item) | heavy rows (info + slots) | slots
   const int bm_bytes = (nb * ECHUNK * 4 + 15) & ~15;
   const int part_off = bm_bytes;
   const int rt_off = part_off + EPART;
   const int ri_off = rt_off + maxrows * ECHUNK * ns * 8;
   const int ct_off = ri_off + ((maxrows * 3 * (ns > 32 ? 8 : 4) + 15) & ~15);
   const int ht_off = ct_off + maxitems * 16;
-  const int buf_off = ht_off + ((maxheavy * 8 + 15) & ~15);
+  const int buf_off = ht_off + ((heavy_bytes + 15) & ~15);
   std::vector<int> owner(nb), base(nb);
   int maxs = 0;
   for (int c = 0; c < cluster; ++c) {
@@ -473,6 +504,9 @@ struct QceArgs {
   int ci[EMAXCL + 1];
   int cb[EMAXCL + 1];
   int ib[EMAXCL + 1];
+  int hoff[EMAXCL + 1];         // heavy items of CTA c: hitems[hoff[c] .. hoff[c+1])
+  int nhrows;                   // heavy rows = block rows 0 .. nhrows-1
+  const int16_t *hitems;
   const int32_t *ccols;
   const int4 *itab;
   const int4 *rdesc;
@@ -760,7 +794,6 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   uint2 *rtab = reinterpret_cast<uint2 *>(smem + a.rt_off);
   MASK *rinfo = reinterpret_cast<MASK *>(smem + a.ri_off);
   uint4 *itab = reinterpret_cast<uint4 *>(smem + a.ct_off);
-  uint2 *htab = reinterpret_cast<uint2 *>(smem + a.ht_off);
   const uint32_t sm_sa = smem_u32(smem);
   const uint32_t part_sa = smem_u32(part);
   const uint32_t dummy = part_sa + 40 * 4;   // junk word for masked slots
@@ -771,6 +804,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const int r0 = c0 / ECHUNK;
   const int nr = ncitems > 0 ? (c0 + ncitems + ECHUNK - 1) / ECHUNK - r0 : 0;
   const int i0 = a.ib[rank], nvitems = a.ib[rank + 1] - i0;
+  const int h0 = a.hoff[rank], nhi = TA ? a.hoff[rank + 1] - h0 : 0;
   // this lane's cluster address of CTA `lane`'s bitmap (ballot broadcast)
   const uint32_t bm_peer = lane < CL ? dsmem_map(sm_sa, (uint32_t)lane) : 0u;
 
@@ -778,33 +812,34 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   // row slot (rl, chunk, j): {shared::cluster address of the slot block in
   // its owner, (first entry index b = (32*chunk - u) mod 360) << 16 | bitmap
   // word index of the column}; slots past the row degree repeat the last one.
-  // Heavy rows (degree above NS) get one entry per slot in htab instead and
-  // row info {htab offset, wrap slot + 1 (0: none), degree | 1 << 16}.
-  if (tid == 0) {
-    int off = 0;
-    for (int rl = 0; rl < nr; ++rl) {
-      const int rp = __ldg(a.rptr + r0 + rl);
-      const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
-      if (deg <= NS) continue;
-      int wj = 0;
-      for (int q = 0; q < deg; ++q)
-        if (__ldg(a.rdesc + rp + q).x & EWRAP) wj = q + 1;
-      rinfo[3 * rl] = (MASK)off;
-      rinfo[3 * rl + 1] = (MASK)wj;
-      rinfo[3 * rl + 2] = (MASK)(deg | (1 << 16));
-      off += deg;
+  // Heavy rows (the accumulator rows of a Type A code, above NS edges; every
+  // CTA holds all of them): hinfo[r] = {slot entries' offset in htab, wrap
+  // slot + 1 (0: none), degree}, one htab entry per slot.
+  int4 *hinfo = reinterpret_cast<int4 *>(smem + a.ht_off);
+  uint2 *htab = reinterpret_cast<uint2 *>(smem + a.ht_off + 16 * a.nhrows);
+  if (TA) {
+    if (tid == 0) {
+      int off = 0;
+      for (int r = 0; r < a.nhrows; ++r) {
+        const int rp = __ldg(a.rptr + r);
+        const int deg = __ldg(a.rptr + r + 1) - rp;
+        int wj = 0;
+        for (int q = 0; q < deg; ++q)
+          if (__ldg(a.rdesc + rp + q).x & EWRAP) wj = q + 1;
+        hinfo[r] = make_int4(off, wj, deg, 0);
+        off += deg;
+      }
     }
-  }
-  __syncthreads();
-  for (int rl = warp; rl < nr; rl += nwarps) {
-    const int rp = __ldg(a.rptr + r0 + rl);
-    const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
-    if (deg <= NS) continue;
-    const int off = (int)rinfo[3 * rl];
-    for (int j = lane; j < deg; j += 32) {
-      const int4 d = __ldg(a.rdesc + rp + j);
-      htab[off + j] = make_uint2(dsmem_map(sm_sa + (uint32_t)d.y, (uint32_t)(d.x & 0xFF)),
-                                 ((uint32_t)d.z << 16) | ((uint32_t)d.w >> 2));
+    __syncthreads();
+    for (int r = warp; r < a.nhrows; r += nwarps) {
+      const int rp = __ldg(a.rptr + r);
+      const int deg = __ldg(a.rptr + r + 1) - rp;
+      const int off = hinfo[r].x;
+      for (int j = lane; j < deg; j += 32) {
+        const int4 d = __ldg(a.rdesc + rp + j);
+        htab[off + j] = make_uint2(dsmem_map(sm_sa + (uint32_t)d.y, (uint32_t)(d.x & 0xFF)),
+                                   ((uint32_t)d.z << 16) | ((uint32_t)d.w >> 2));
+      }
     }
   }
   for (int e = tid; e < nr * NS; e += blockDim.x) {
@@ -812,7 +847,6 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
     const int j = e - rl * NS;
     const int rp = __ldg(a.rptr + r0 + rl);
     const int deg = __ldg(a.rptr + r0 + rl + 1) - rp;
-    if (deg > NS) continue;
     const int4 d = __ldg(a.rdesc + rp + min(j, deg - 1));
     const uint32_t base = dsmem_map(sm_sa + (uint32_t)d.y, (uint32_t)(d.x & 0xFF));
     const uint32_t wb = (uint32_t)d.w >> 2;
@@ -880,8 +914,20 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       if (tid == 0 && it > 0) part[(it - 1) & 1] = 0;
       // ---------------- check phase ----------------------------------------
       int mybad = 0;
-      for (int w = warp; w < ncitems; w += nwarps) {
-        const int gi = c0 + w;
+      // this CTA's heavy items first (warps 0.. take one each), then its
+      // range of light items
+      for (int w = warp; w < nhi + ncitems; w += nwarps) {
+        int syn;
+        if (TA && w < nhi) {
+          const int hi = __ldg(a.hitems + h0 + w);
+          const int row = hi / ECHUNK;
+          const int4 hf = hinfo[row];
+          syn = qce_check_heavy<TORCH>(htab + hf.x, hf.z, hf.y - 1, (uint32_t)lane,
+                                       hi - row * ECHUNK, bm, dummy, upd, a, it);
+          mybad += syn;
+          continue;
+        }
+        const int gi = c0 + (w - nhi);
         const int row = gi / ECHUNK;
         const int ch = gi - row * ECHUNK;
         const int rl = row - r0;
@@ -889,11 +935,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         const int deg = (int)rinfo[3 * rl + 2];
         const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
         const bool full = wm == 0 && ch < ECHUNK - 1;
-        int syn;
-        if (TA && (deg >> 16)) {
-          syn = qce_check_heavy<TORCH>(htab + (int)rinfo[3 * rl], deg & 0xFFFF, (int)wm - 1,
-                                       (uint32_t)lane, ch, bm, dummy, upd, a, it);
-        } else if (full && deg == NS) {
+        if (full && deg == NS) {
           syn = qce_check_item<TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
         } else if (full && deg == NS - 1) {
           syn = qce_check_item<TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
@@ -1199,6 +1241,8 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
   if (e == cudaSuccess) e = up((void **)&h->p.d_itab, t.itab.data(), t.itab.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0b, t.s0b.data(), t.s0b.size());
+  if (e == cudaSuccess)
+    e = up((void **)&h->p.d_hitems, t.hitems.data(), t.hitems.size() * sizeof(int16_t));
   if (e != cudaSuccess) {
     atsc3_ldpc_qce_plan_destroy(h);
     return cuda_fail(e, "qce plan upload");
@@ -1222,6 +1266,7 @@ void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
   cudaFree(h->p.d_itab);
   cudaFree(h->p.d_s0);
   cudaFree(h->p.d_s0b);
+  cudaFree(h->p.d_hitems);
   delete h;
 }
 
@@ -1246,7 +1291,8 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
                                     int32_t *meta, int32_t *rdesc,
                                     int32_t *rptr, int32_t *cdesc,
                                     int32_t *ccols, uint8_t *s0,
-                                    uint8_t *s0b, int32_t *itab) {
+                                    uint8_t *s0b, int32_t *itab,
+                                    int32_t *hitems) {
   using namespace atsc3;
   ATSC3_ARG(meta && rowptr && addr, "null argument");
   QcePlan p;
@@ -1269,6 +1315,8 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
   meta[59] = p.heavy;
   meta[60] = p.dr_light;
   meta[61] = (int32_t)t.itab.size();
+  for (int c = 0; c <= EMAXCL; ++c) meta[62 + c] = p.hoff[c];
+  meta[79] = p.nhrows;
   if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
@@ -1276,6 +1324,8 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
   if (s0) std::memcpy(s0, t.s0.data(), t.s0.size());
   if (s0b) std::memcpy(s0b, t.s0b.data(), t.s0b.size());
   if (itab) std::memcpy(itab, t.itab.data(), t.itab.size() * 16);
+  if (hitems)
+    for (size_t i = 0; i < t.hitems.size(); ++i) hitems[i] = t.hitems[i];
   return 0;
 }
 
@@ -1286,10 +1336,10 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
                                    int32_t *cdesc, int32_t *ccols,
                                    uint8_t *s0) {
   ATSC3_ARG(meta != nullptr, "null argument");
-  int32_t m[64];
+  int32_t m[96];
   const int32_t rc = atsc3_ldpc_qce_tables_host2(n, kldpc, qldpc, 0, rowptr, addr, cluster,
                                                  m, rdesc, rptr, cdesc, ccols, s0,
-                                                 nullptr, nullptr);
+                                                 nullptr, nullptr, nullptr);
   if (rc == 0 && meta) std::memcpy(meta, m, 42 * sizeof(int32_t));
   return rc;
 }
@@ -1495,7 +1545,10 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   for (int c = 0; c <= EMAXCL; ++c) {
     a.ci[c] = p.ci[c];
     a.cb[c] = p.cb[c];
+    a.hoff[c] = p.hoff[c];
   }
+  a.nhrows = p.nhrows;
+  a.hitems = p.d_hitems;
   a.ccols = p.d_ccols;
   a.itab = p.d_itab;
   for (int c = 0; c <= EMAXCL; ++c) a.ib[c] = p.ib[c];

@@ -59,7 +59,8 @@ SIGNATURES = {
                                             c_vp, c_i32, c_vp]),
     "atsc3_ldpc_qce_tables_host2": (c_i32, [c_i32, c_i32, c_i32, c_i32, c_vp,
                                             c_vp, c_i32, c_vp, c_vp, c_vp,
-                                            c_vp, c_vp, c_vp, c_vp, c_vp]),
+                                            c_vp, c_vp, c_vp, c_vp, c_vp,
+                                            c_vp]),
     "atsc3_ldpc_qce_plan_info": (c_i32, [c_vp, c_vp]),
     "atsc3_ldpc_qce_tables_host": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp,
                                            c_i32, c_vp, c_vp, c_vp, c_vp,

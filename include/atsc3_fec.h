@@ -258,19 +258,23 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
 /* out[0] = clusters resident at once, [1] = CTAs per cluster, [2] = shared
  * bytes per CTA, [3] = threads per CTA (threads 0 = the default). */
 /* atsc3_ldpc_qce_tables_host for both code types (qa, qb as in
- * atsc3_ldpc_qce_plan_create2).  meta (64 ints): [0..41] as
+ * atsc3_ldpc_qce_plan_create2).  meta (96 ints): [0..41] as
  * atsc3_ldpc_qce_tables_host, [42..58] check items (row*12 + chunk) of CTA
- * c from meta[42+c] to meta[43+c], [59] heavy rows present, [60] degree that
- * sets the compile-time slot count, [61] variable-phase items.  s0b: (n)
- * rotation start in the identity rows; itab: int4 per variable-phase item.
- * Array outputs may be null. */
+ * c from meta[42+c] to meta[43+c] (its light items when heavy rows exist),
+ * [59] heavy rows present, [60] degree that sets the compile-time slot
+ * count, [61] variable-phase items, [62..78] heavy items of CTA c:
+ * hitems[meta[62+c] .. meta[63+c]), [79] heavy rows (block rows 0 ..).
+ * s0b: (n) rotation start in the identity rows; itab: int4 per
+ * variable-phase item; hitems: heavy check items, grouped by CTA.  Array
+ * outputs may be null. */
 int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
                                     int32_t qb, const int32_t *rowptr,
                                     const int32_t *addr, int32_t cluster,
                                     int32_t *meta, int32_t *rdesc,
                                     int32_t *rptr, int32_t *cdesc,
                                     int32_t *ccols, uint8_t *s0,
-                                    uint8_t *s0b, int32_t *itab);
+                                    uint8_t *s0b, int32_t *itab,
+                                    int32_t *hitems);
 
 int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *plan, int32_t threads,
                               int32_t semantics, int32_t *out);

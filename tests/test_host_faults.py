@@ -96,12 +96,12 @@ def test_type_a_tables_refused():
     rate, n = "7/15", 64800
     typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
     rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows(rate, n)]
-    meta = np.zeros(64, np.int32)
+    meta = np.zeros(96, np.int32)
     f = L.atsc3_ldpc_qce_tables_host2
 
     def call(qa, qb, rp, ad):
         return f(n, K, qa, qb, rp.ctypes.data, ad.ctypes.data, 7, meta.ctypes.data,
-                 None, None, None, None, None, None, None)
+                 None, None, None, None, None, None, None, None)
 
     assert call(Q1, Q2, rowptr, addr) == 0
     assert call(Q1 + 1, Q2, rowptr, addr) == -3           # zones do not add up

@@ -25,10 +25,10 @@ def qce_tables(rate, n, cluster):
     K, QA, QB = zones(rate, n)
     Q = QA + QB
     rowptr, addr = [np.ascontiguousarray(a, np.int32) for a in C.address_rows(rate, n)]
-    meta = np.zeros(64, np.int32)
+    meta = np.zeros(96, np.int32)
     args = [n, K, QA, QB, rowptr.ctypes.data, addr.ctypes.data, cluster]
     N.call("atsc3_ldpc_qce_tables_host2", *args, meta.ctypes.data, None, None,
-           None, None, None, None, None)
+           None, None, None, None, None, None)
     nb = n // QZ
     rdesc = np.zeros((meta[0], 4), np.int32)
     rptr = np.zeros(Q + 1, np.int32)
@@ -37,10 +37,12 @@ def qce_tables(rate, n, cluster):
     s0 = np.zeros(nb * QZ, np.uint8)
     s0b = np.zeros(nb * QZ, np.uint8)
     itab = np.zeros((meta[61], 4), np.int32)
+    hitems = np.zeros(max(1, meta[62 + cluster]), np.int32)
     N.call("atsc3_ldpc_qce_tables_host2", *args, meta.ctypes.data,
            rdesc.ctypes.data, rptr.ctypes.data, cdesc.ctypes.data,
-           ccols.ctypes.data, s0.ctypes.data, s0b.ctypes.data, itab.ctypes.data)
-    return K, QA, QB, meta, rdesc, rptr, cdesc, ccols, s0, s0b, itab
+           ccols.ctypes.data, s0.ctypes.data, s0b.ctypes.data, itab.ctypes.data,
+           hitems.ctypes.data)
+    return K, QA, QB, meta, rdesc, rptr, cdesc, ccols, s0, s0b, itab, hitems[:meta[62 + cluster]]
 
 
 def check_index(r, k, QA, QB):
@@ -62,7 +64,7 @@ TYPE_A = [("2/15", 16200, 2), ("3/15", 16200, 3), ("5/15", 16200, 2),
                                             ("10/15", 16200, 2), ("12/15", 16200, 2),
                                             ("13/15", 16200, 2)] + TYPE_A)
 def test_qce_descriptors_reproduce_csr(rate, n, cluster):
-    K, QA, QB, meta, rdesc, rptr, cdesc, ccols, s0, s0b, itab = qce_tables(rate, n, cluster)
+    K, QA, QB, meta, rdesc, rptr, cdesc, ccols, s0, s0b, itab, hitems = qce_tables(rate, n, cluster)
     Q = QA + QB
     ccp, cidx, vptr, vedge = C.csr(rate, n)
     nb = n // QZ
@@ -70,7 +72,19 @@ def test_qce_descriptors_reproduce_csr(rate, n, cluster):
     cb = meta[25:25 + cluster + 1]
     ci = meta[42:42 + cluster + 1]
     assert cb[0] == 0 and cb[-1] == nb and (np.diff(cb) >= 0).all()
-    assert ci[0] == 0 and ci[-1] == Q * 12 and (np.diff(ci) >= 0).all()
+    assert ci[-1] == Q * 12 and (np.diff(ci) >= 0).all()
+    # light ranges + heavy lists: every check item exactly once; heavy items
+    # (the accumulator rows of a Type A code) dealt round-robin
+    hoff = meta[62:62 + cluster + 1]
+    items = [i for c in range(cluster) for i in range(ci[c], ci[c + 1])]
+    items += hitems.tolist()
+    assert sorted(items) == list(range(Q * 12))
+    if meta[79]:
+        assert ci[0] == meta[79] * 12 and meta[79] == QA
+        sizes = np.diff(hoff)
+        assert sizes.max() - sizes.min() <= 1
+    else:
+        assert ci[0] == 0 and len(hitems) == 0
     assert sorted(ccols.tolist()) == list(range(nb))
     buf_off = meta[7]
     assert part_off >= nb * 12 * 4 and buf_off >= part_off + 256
@@ -168,7 +182,7 @@ def test_qce_descriptors_reproduce_csr(rate, n, cluster):
 
 
 def _tables_from(n, K, Q, rowptr, addr, cluster):
-    meta = np.zeros(48, np.int32)
+    meta = np.zeros(96, np.int32)
     nb = n // QZ
     f = N.lib().atsc3_ldpc_qce_tables_host
     rc = f(n, K, Q, rowptr.ctypes.data, addr.ctypes.data, cluster, meta.ctypes.data,
