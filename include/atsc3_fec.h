@@ -188,8 +188,8 @@ int32_t atsc3_ldpc_qc_decode_weighted(
  * check-to-variable message after the check phase; hard decisions in a
  * bitmap replicated per CTA; no per-check records.  cluster: any size in
  * 1..16 (not only powers of two); 0 picks the smallest cluster whose per-CTA
- * shared memory fits (6 for most 64800-bit codes, 7 for 64800 5/15 and
- * 7/15, 2 for the 16200-bit ones). */
+ * shared memory fits (6 for the 64800-bit codes but 7/15, which takes 7;
+ * 2 for the 16200-bit ones, 1 for 16200 2/15). */
 typedef struct atsc3_ldpc_qce_plan atsc3_ldpc_qce_plan;
 
 int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
