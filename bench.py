@@ -384,6 +384,26 @@ def run_gpu(args, rank, world, local_rank):
                            "22.9% of peak = 2.13 TB/s (7.55 GB per launch) "
                            "in the committed ncu capture, i.e. about 9.3 TB/s"}
     onchip["frac"] = onchip["achieved"] / onchip["peak_ncu"]
+    # instruction issue, the decoder's actual bound (ncu: issue active ~60%,
+    # not_selected and math-pipe throttle the leading stalls): warp
+    # instructions per codeword-iteration from the committed capture x the
+    # iterations of the timed launch, against 4 schedulers per occupied SM
+    issue = None
+    if p0.plan.info.get("kind") == "qce" and its_stage:
+        from atsc3_b200 import native as N
+        cfg = np.zeros(4, np.int32)
+        N.call("atsc3_ldpc_qce_config", p0.plan._h, 0, 0, cfg.ctypes.data)
+        sms = int(cfg[0]) * int(cfg[1])
+        mhz = float((clocks or {}).get("sm_mhz") or 1965.0)
+        instr = INSTR_PER_BLOCK_ITER * its_stage
+        ach = instr / (ldpc_ms / 1e3) / 1e9
+        peak = sms * 4 * mhz / 1e3
+        issue = {"unit": "G warp instructions/s", "achieved": ach, "peak": peak,
+                 "frac": ach / peak, "sms": sms, "instructions_per_launch": instr,
+                 "what": "warp instructions per codeword-iteration (1.871 G over "
+                         "75 x 50 in the committed ncu capture) x the launch's "
+                         "iterations / launch time; peak = 4 schedulers x SM "
+                         "clock x the SMs the clusters occupy"}
     b_ldpc = nblk * (4 * N_INNER + N_INNER // 8 + 9)
     hbm, peak_kind = peaks()
     achieved = b_ldpc / (ldpc_ms / 1e3) / 1e9
@@ -413,7 +433,8 @@ def run_gpu(args, rank, world, local_rank):
                              "peak_kind": peak_kind,
                              "bytes_per_launch": b_ldpc,
                              "ms_per_launch": ldpc_ms,
-                             "onchip": onchip},
+                             "onchip": onchip,
+                             "issue": issue},
                 "stage_ms": {"demap": float(stage[:, 0].mean()),
                              "ldpc": ldpc_ms,
                              "bch": float(stage[:, 2].mean())},
@@ -438,6 +459,9 @@ KERNEL_NAMES = {"qce": "ldpc_qce_kernel (quasi-cyclic flooding, edge-buffer layo
 # profiles/ldpc_qce_flood_6_15_frame.md (the record-layout decoder's capture,
 # profiles/ldpc_qc_flood_6_15_frame.md, read 19,553,792 B).
 TRAFFIC_PER_BLOCK = 19_549_184 / 75
+# warp instructions per codeword-iteration of ldpc_qce_kernel<0, 8, 1024, 0> on this
+# workload: 1,870,617,663 over 75 blocks x 50 iterations (profiles/ldpc_qce_flood_6_15_frame.md)
+INSTR_PER_BLOCK_ITER = 1_870_617_663 / 3750
 
 
 def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
@@ -734,8 +758,11 @@ def run_codes(args):
         return e0.elapsed_time(e1) / steps, o
 
     rows = []
+    only = {x.strip() for x in args.only.split(",")} if args.only else None
     for n in (16200, 64800):
         for r in C.RATES:
+            if only and f"{n} {r}" not in only:
+                continue
             qce = LDPC.plan_for(r, n, kind="qce")
             csr = LDPC.plan_for(r, n, kind="csr")
             cfg = np.zeros(4, np.int32)
@@ -780,6 +807,8 @@ def main(argv=None):
     ap.add_argument("--decoder", default="auto", choices=["auto", "qce", "qc", "csr"],
                     help="LDPC decoder (auto = edge-buffer quasi-cyclic)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default="",
+                    help="--workload codes: comma-separated codes, e.g. '64800 7/15'")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         a.warmup = 3
