@@ -84,6 +84,8 @@ struct QcePlan {
                                 // heavy rows: its light items only
   int hoff[EMAXCL + 1] = {0};   // heavy items of CTA c: hitems[hoff[c] .. hoff[c+1])
   int nhrows = 0;               // heavy rows (the accumulator rows) or 0
+  int hsplit = 1;               // parts per heavy item (warps sharing it)
+  int hpb_off = 0;              // shared-memory offset of the heavy partials
   int ib[EMAXCL + 1] = {0};     // variable-phase items of CTA c in d_itab
   int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
@@ -274,7 +276,20 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
         set_error("unsupported: heavy rows other than the accumulator rows");
         return -4;
       }
+    if (ns < 6) {
+      set_error("unsupported: heavy rows with identity rows of at most 4 edges");
+      return -4;
+    }
     p->nhrows = QA;
+    // a heavy item's slots are cut into hsplit contiguous parts of about 24
+    // edges, each pass taken by its own warp (partial minima merged in
+    // shared memory between the two passes)
+    // (only for rows above 64 edges -- 64800 7/15: parts pay an extra CTA
+    // barrier and a partials buffer, which lighter heavy rows do not earn
+    // back; those take one warp per item)
+    int hdmax = 0;
+    for (int r = 0; r < QA; ++r) hdmax = std::max(hdmax, rdeg[r]);
+    p->hsplit = hdmax > 64 ? (hdmax + 23) / 24 : 1;
     std::vector<int64_t> hc(cluster, 0);
     std::vector<std::vector<int>> hl(cluster);
     for (int i = 0; i < QA * ECHUNK; ++i) {
@@ -394,6 +409,11 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   // every CTA holds all heavy rows: an int4 of row info each, then 8 B per slot
   int heavy_bytes = 16 * p->nhrows;
   for (int r = 0; r < p->nhrows; ++r) heavy_bytes += 8 * rdeg[r];
+  heavy_bytes = (heavy_bytes + 15) & ~15;
+  const int hpb_rel = heavy_bytes;        // partials: 16 B per lane per part
+  int maxnh = 0;
+  for (int c = 0; c < cluster; ++c) maxnh = std::max(maxnh, p->hoff[c + 1] - p->hoff[c]);
+  if (p->nhrows && p->hsplit > 1) heavy_bytes += maxnh * p->hsplit * 32 * 16;
   // shared memory: bitmap | syndrome exchange | row-slot table (per row,
   // chunk and slot, 8 B) | row info (3 words per row) | variable-phase item
   // table (16 B per item) | heavy rows (info + slots) | slots
@@ -429,6 +449,7 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   p->ri_off = ri_off;
   p->ct_off = ct_off;
   p->ht_off = ht_off;
+  p->hpb_off = ht_off + hpb_rel;
   p->buf_off = buf_off;
   p->smem = buf_off + maxs * ESLOT;
   t->rptr.assign(Q + 1, 0);
@@ -506,6 +527,7 @@ struct QceArgs {
   int ib[EMAXCL + 1];
   int hoff[EMAXCL + 1];         // heavy items of CTA c: hitems[hoff[c] .. hoff[c+1])
   int nhrows;                   // heavy rows = block rows 0 .. nhrows-1
+  int hsplit, hpb_off;          // parts per heavy item, partials' offset
   const int16_t *hitems;
   const int32_t *ccols;
   const int4 *itab;
@@ -711,6 +733,75 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
   return (int)(synw & 1u);
 }
 
+// Heavy rows (more edges than the compile-time slot count; the accumulator
+// rows of the Type A codes): an item = 32 consecutive checks of the row, its
+// deg slots cut into parts [j0, j1) that different warps walk.  he[j] =
+// {shared::cluster address of slot j's block, shift u << 16 | bitmap word
+// index}; wrapj = the slot that check (0, 0) lacks, or -1.
+struct HeavyPart {               // one lane's partial state over [j0, j1)
+  float min1, min2;
+  int first;                     // absolute slot index of the first minimum
+  uint32_t bits;                 // sign parity | syndrome bit << 1
+};
+
+__device__ __forceinline__ uint32_t heavy_addr(const uint2 &e, int ch, uint32_t lane,
+                                               uint32_t *o) {
+  int bb = ch * 32 - (int)(e.y >> 16);
+  bb += bb < 0 ? EZ : 0;
+  const uint32_t x = (uint32_t)bb + lane;
+  *o = min(x, x - (uint32_t)EZ);
+  return e.x + 4u * *o;
+}
+
+// Pass 1 over [j0, j1): min1/min2/first (strict <, ldpc_kernel.c:121-126),
+// sign parity and syndrome bit of the loaded edge values.
+__device__ __forceinline__ HeavyPart qce_heavy_pass1(const uint2 *he, int j0, int j1,
+                                                     int wrapj, uint32_t lane, int ch,
+                                                     const uint32_t *bm, uint32_t dummy) {
+  const int k0 = ch * 32 + (int)lane;
+  const bool lv = k0 < EZ;
+  const float inf = __int_as_float(0x7f800000);
+  HeavyPart r{inf, inf, j0, 0u};
+  uint32_t synw = 0;
+  for (int j = j0; j < j1; ++j) {
+    const uint2 e = he[j];
+    uint32_t o;
+    const uint32_t ad = heavy_addr(e, ch, lane, &o);
+    const bool on = lv && !(k0 == 0 && j == wrapj);
+    const float t = dsmem_ld_f32(on ? ad : dummy);
+    if (on) {
+      const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
+      synw ^= hw >> (o & 31);
+      const float mag = fabsf(t);
+      r.bits ^= t < 0.f ? 1u : 0u;
+      r.first = mag < r.min1 ? j : r.first;
+      r.min2 = fminf(r.min2, fmaxf(r.min1, mag));
+      r.min1 = fminf(r.min1, mag);
+    }
+  }
+  r.bits |= (synw & 1u) << 1;
+  return r;
+}
+
+// Pass 2 over [j0, j1): reload each value (this lane alone writes it, after
+// reading) and store its message.
+__device__ __forceinline__ void qce_heavy_pass2(const uint2 *he, int j0, int j1, int wrapj,
+                                                uint32_t lane, int ch, uint32_t ua,
+                                                uint32_t ub, int first, uint32_t par) {
+  const int k0 = ch * 32 + (int)lane;
+  const bool lv = k0 < EZ;
+  for (int j = j0; j < j1; ++j) {
+    const uint2 e = he[j];
+    uint32_t o;
+    const uint32_t ad = heavy_addr(e, ch, lane, &o);
+    if (lv && !(k0 == 0 && j == wrapj)) {
+      const float t = dsmem_ld_f32(ad);
+      const uint32_t sg = par ^ (t < 0.f ? 1u : 0u);
+      dsmem_st_u32(ad, (j == first ? ub : ua) | (sg << 31));
+    }
+  }
+}
+
 // Check item of a heavy row (more edges than the compile-time slot count;
 // the accumulator rows of the Type A codes): 32 consecutive checks of the
 // row, its deg slots walked in a loop.  he[j] = {shared::cluster address of
@@ -804,7 +895,10 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const int r0 = c0 / ECHUNK;
   const int nr = ncitems > 0 ? (c0 + ncitems + ECHUNK - 1) / ECHUNK - r0 : 0;
   const int i0 = a.ib[rank], nvitems = a.ib[rank + 1] - i0;
-  const int h0 = a.hoff[rank], nhi = TA ? a.hoff[rank + 1] - h0 : 0;
+  // heavy rows are compiled into the Type A kernels of 6 and 8 slots (the
+  // builder refuses them with 4)
+  constexpr bool HV = TA && NS >= 6;
+  const int h0 = a.hoff[rank], nhi = HV ? a.hoff[rank + 1] - h0 : 0;
   // this lane's cluster address of CTA `lane`'s bitmap (ballot broadcast)
   const uint32_t bm_peer = lane < CL ? dsmem_map(sm_sa, (uint32_t)lane) : 0u;
 
@@ -817,7 +911,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   // slot + 1 (0: none), degree}, one htab entry per slot.
   int4 *hinfo = reinterpret_cast<int4 *>(smem + a.ht_off);
   uint2 *htab = reinterpret_cast<uint2 *>(smem + a.ht_off + 16 * a.nhrows);
-  if (TA) {
+  if (HV) {
     if (tid == 0) {
       int off = 0;
       for (int r = 0; r < a.nhrows; ++r) {
@@ -914,20 +1008,36 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       if (tid == 0 && it > 0) part[(it - 1) & 1] = 0;
       // ---------------- check phase ----------------------------------------
       int mybad = 0;
-      // this CTA's heavy items first (warps 0.. take one each), then its
-      // range of light items
-      for (int w = warp; w < nhi + ncitems; w += nwarps) {
+      // Type A with heavy rows: this CTA's heavy items first, one warp each,
+      // then its light items.  With hsplit > 1 (very heavy rows): phase A =
+      // pass 1 of every heavy item part (one warp each; partials to shared
+      // memory) and the light items; phase B (after a CTA barrier) = merge
+      // each item's partials and pass 2 of every part.
+      const bool split = HV && a.nhrows && a.hsplit > 1;
+      const int nhp = (HV && a.nhrows) ? (split ? nhi * a.hsplit : nhi) : 0;
+      for (int w = warp; w < nhp + ncitems; w += nwarps) {
         int syn;
-        if (TA && w < nhi) {
+        if (HV && w < nhp && !split) {             // one warp per heavy item
           const int hi = __ldg(a.hitems + h0 + w);
           const int row = hi / ECHUNK;
           const int4 hf = hinfo[row];
-          syn = qce_check_heavy<TORCH>(htab + hf.x, hf.z, hf.y - 1, (uint32_t)lane,
-                                       hi - row * ECHUNK, bm, dummy, upd, a, it);
-          mybad += syn;
+          mybad += qce_check_heavy<TORCH>(htab + hf.x, hf.z, hf.y - 1, (uint32_t)lane,
+                                          hi - row * ECHUNK, bm, dummy, upd, a, it);
           continue;
         }
-        const int gi = c0 + (w - nhi);
+        if (HV && w < nhp) {
+          const int i = w / a.hsplit, part = w - i * a.hsplit;
+          const int hi = __ldg(a.hitems + h0 + i);
+          const int row = hi / ECHUNK;
+          const int4 hf = hinfo[row];
+          const int j0 = part * hf.z / a.hsplit, j1 = (part + 1) * hf.z / a.hsplit;
+          const HeavyPart r = qce_heavy_pass1(htab + hf.x, j0, j1, hf.y - 1, (uint32_t)lane,
+                                              hi - row * ECHUNK, bm, dummy);
+          reinterpret_cast<float4 *>(smem + a.hpb_off)[w * 32 + lane] =
+              make_float4(r.min1, r.min2, __int_as_float(r.first), __uint_as_float(r.bits));
+          continue;
+        }
+        const int gi = c0 + (w - nhp);
         const int row = gi / ECHUNK;
         const int ch = gi - row * ECHUNK;
         const int rl = row - r0;
@@ -948,6 +1058,53 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           syn = k0 < EZ ? syn : 0;
         }
         mybad += syn;
+      }
+      if (split) {
+        __syncthreads();
+        const float4 *pb = reinterpret_cast<const float4 *>(smem + a.hpb_off);
+        for (int w = warp; w < nhp; w += nwarps) {
+          const int i = w / a.hsplit, part = w - i * a.hsplit;
+          const int hi = __ldg(a.hitems + h0 + i);
+          const int row = hi / ECHUNK;
+          const int ch = hi - row * ECHUNK;
+          const int4 hf = hinfo[row];
+          const int k0 = ch * 32 + lane;
+          // merge the parts in slot order: the first minimum is the lowest
+          // part's on ties; min2 = the second order statistic
+          const float inf = __int_as_float(0x7f800000);
+          float min1 = inf, min2 = inf;
+          int first = 0;
+          uint32_t bits = 0;
+          for (int q = 0; q < a.hsplit; ++q) {
+            const float4 v = pb[(i * a.hsplit + q) * 32 + lane];
+            if (v.x < min1) {
+              min2 = fminf(min1, v.y);
+              min1 = v.x;
+              first = __float_as_int(v.z);
+            } else {
+              min2 = fminf(min2, v.x);
+            }
+            min2 = fminf(min2, v.y);
+            bits ^= __float_as_uint(v.w);
+          }
+          if (part == 0 && k0 < EZ) mybad += (int)((bits >> 1) & 1u);
+          if (upd) {
+            float wa = a.alpha, wb = 0.f;
+            if (a.walpha) {
+              const int nl = hf.z - ((k0 == 0 && hf.y > 0) ? 1 : 0);
+              const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+              wa = __ldg(a.walpha + wi);
+              wb = __ldg(a.wbeta + wi);
+            }
+            float A = __fsub_rn(__fmul_rn(min1, wa), wb);
+            float B = __fsub_rn(__fmul_rn(min2, wa), wb);
+            A = A > 0.f ? A : 0.f;
+            B = B > 0.f ? B : 0.f;
+            const int j0 = part * hf.z / a.hsplit, j1 = (part + 1) * hf.z / a.hsplit;
+            qce_heavy_pass2(htab + hf.x, j0, j1, hf.y - 1, (uint32_t)lane, ch,
+                            __float_as_uint(A), __float_as_uint(B), first, bits & 1u);
+          }
+        }
       }
       // unsatisfied checks: every warp adds its count into the counter of
       // every CTA of the cluster, so after the barrier each CTA holds the total
@@ -1548,6 +1705,8 @@ int32_t atsc3_ldpc_qce_decode_weighted(
     a.hoff[c] = p.hoff[c];
   }
   a.nhrows = p.nhrows;
+  a.hsplit = p.hsplit;
+  a.hpb_off = p.hpb_off;
   a.hitems = p.d_hitems;
   a.ccols = p.d_ccols;
   a.itab = p.d_itab;
