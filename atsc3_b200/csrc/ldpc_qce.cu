@@ -1,13 +1,16 @@
-// ldpc_qce.cu -- flooding normalised min-sum for the quasi-cyclic A/322 Type
-// B codes with an EDGE-BUFFER layout (sm_100a), bit-exact with
-// lab/ldpc_kernel.c (kernel semantics) and lab/m9_gpu.py:168-211 (torch
-// semantics), float32.
+// ldpc_qce.cu -- flooding normalised min-sum for every quasi-cyclic A/322
+// code (Type B, and Type A with its identity rows) with an EDGE-BUFFER layout
+// (sm_100a), bit-exact with lab/ldpc_kernel.c (kernel semantics) and
+// lab/m9_gpu.py:168-211 (torch semantics), float32.
 //
 // The code structure used is the one of ldpc_qc.cu (360x360 circulants,
 // dual-diagonal parity part, edge order inside a check = block-column order,
 // a bit's summation order = its column's circulant list sorted by (shift,
 // row) and rotated at s0[col*360 + mm]), except that a block may hold more
-// than one circulant here.
+// than one circulant here, and a Type A code adds identity block rows: a
+// bit's checks there come after its accumulator checks, so its sum is two
+// rotated segments (s0, then s0b), and its few accumulator rows of high
+// degree take a loop path ("heavy" rows, see qce_check_heavy).
 //
 // What differs is where the decoder state lives.  Every edge of the codeword
 // owns one float32 slot in the distributed shared memory of its cluster, in
