@@ -103,6 +103,11 @@ __device__ __forceinline__ void dsmem_st_u32(uint32_t a, uint32_t v) {
                : "memory");
 }
 
+__device__ __forceinline__ void dsmem_st_u64(uint32_t a, unsigned long long v) {
+  asm volatile("st.shared::cluster.u64 [%0], %1;" :: "r"(a), "l"(v)
+               : "memory");
+}
+
 // atomic add into (possibly another CTA's) shared memory of the cluster
 __device__ __forceinline__ void dsmem_red_add_u32(uint32_t a, uint32_t v) {
   asm volatile("red.shared::cluster.add.u32 [%0], %1;" :: "r"(a), "r"(v)
@@ -125,5 +130,28 @@ __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, 
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float vabs(float a) { return fabsf(a); }
+__device__ __forceinline__ double vabs(double a) { return fabs(a); }
+__device__ __forceinline__ float vmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double vmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
+template <typename V> __device__ __forceinline__ V vinf();
+template <> __device__ __forceinline__ float vinf<float>() { return __int_as_float(0x7f800000); }
+template <> __device__ __forceinline__ double vinf<double>() {
+  return __longlong_as_double(0x7ff0000000000000ll);
+}
+// the raw bits of a message value and the store of a signed message
+__device__ __forceinline__ uint32_t vbits(float a) { return __float_as_uint(a); }
+__device__ __forceinline__ unsigned long long vbits(double a) {
+  return (unsigned long long)__double_as_longlong(a);
+}
+__device__ __forceinline__ void dsmem_st_msg(uint32_t a, uint32_t mag_bits, uint32_t neg) {
+  dsmem_st_u32(a, mag_bits | (neg << 31));
+}
+__device__ __forceinline__ void dsmem_st_msg(uint32_t a, unsigned long long mag_bits,
+                                             uint32_t neg) {
+  dsmem_st_u64(a, mag_bits | ((unsigned long long)neg << 63));
+}
 
 }  // namespace atsc3

@@ -58,7 +58,7 @@ constexpr int EZ = 360;
 constexpr int ECHUNK = 12;                // ceil(360 / 32) warps per row/column
 constexpr int EMAXCL = 16;
 constexpr int EWRAP = 1 << 8;
-constexpr int ESLOT = EZ * 4;             // bytes of one circulant slot
+constexpr int ESLOT = EZ * 4;             // bytes of one float32 circulant slot
 constexpr int EPART = 256;                // syndrome exchange bytes
 
 // Compile-time slot counts per block row (NS >= the code's largest block-row
@@ -81,6 +81,7 @@ struct QcePlan {
   int ht_off = 0, buf_off = 0;
   int dr_max = 0, dr_light = 0, dc_max = 0, max_slots = 0, device = 0;
   int heavy = 0;                // rows above the compile-time slot count
+  int vb = 4;                   // bytes per slot entry: 4 float32, 8 float64
   int64_t table_bytes = 0;
   int rb[EMAXCL + 1] = {0};     // block rows CTA c owns (column placement)
   int ci[EMAXCL + 1] = {0};     // check items (row*12 + chunk) of CTA c; with
@@ -132,7 +133,10 @@ constexpr int VM_GEN2 = 3;     // slots in both zones: two rotated segments
 constexpr uint32_t VNOWRAP = 0xFFu;
 
 int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
-              const int32_t *addr, int cluster, QcePlan *p, QceTables *t) {
+              const int32_t *addr, int cluster, QcePlan *p, QceTables *t,
+              int vb = 4) {
+  // vb: bytes per slot entry (4: float32 decoder, 8: float64 decoder)
+  const int slotb = EZ * vb;
   const int Q = QA + QB;
   if (n % EZ || K % EZ || QA <= 0 || QB < 0 || (n - K) != Q * EZ) {
     set_error("invalid argument: not a 360-circulant Type A/B code");
@@ -292,7 +296,7 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     // back; those take one warp per item)
     int hdmax = 0;
     for (int r = 0; r < QA; ++r) hdmax = std::max(hdmax, rdeg[r]);
-    p->hsplit = hdmax > 64 ? (hdmax + 23) / 24 : 1;
+    p->hsplit = (hdmax > 64 && vb == 4) ? (hdmax + 23) / 24 : 1;
     std::vector<int64_t> hc(cluster, 0);
     std::vector<std::vector<int>> hl(cluster);
     for (int i = 0; i < QA * ECHUNK; ++i) {
@@ -434,13 +438,14 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) {
       const int g = t->ccols[q];
       owner[g] = c;
-      base[g] = buf_off + s * ESLOT;
+      base[g] = buf_off + s * slotb;
       s += (int)cols[g].size();
     }
     maxs = std::max(maxs, s);
   }
   p->n = n; p->K = K; p->Q = Q; p->nb = nb;
   p->qa = QA; p->qb = QB;
+  p->vb = vb;
   p->cluster = cluster;
   p->dr_max = drm;
   p->dr_light = dlight;
@@ -454,13 +459,13 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   p->ht_off = ht_off;
   p->hpb_off = ht_off + hpb_rel;
   p->buf_off = buf_off;
-  p->smem = buf_off + maxs * ESLOT;
+  p->smem = buf_off + maxs * slotb;
   t->rptr.assign(Q + 1, 0);
   t->rdesc.clear();
   for (int r = 0; r < Q; ++r) {
     for (auto &sl : rows[r])
       t->rdesc.push_back(make_int4(owner[sl.col] | sl.wrap | (sl.pos << 16),
-                                   base[sl.col] + sl.idx * ESLOT, sl.u,
+                                   base[sl.col] + sl.idx * slotb, sl.u,
                                    sl.col * ECHUNK * 4));
     t->rptr[r + 1] = (int)t->rdesc.size();
   }
@@ -504,7 +509,7 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
         const int absent = (wrap >= 0 && mm0 + step >= EZ) ? 1 : 0;
         const uint32_t w = (uint32_t)(g * ECHUNK + mm0 / 32) | ((uint32_t)dzA[g] << 16) |
                            ((wrap >= 0 ? (uint32_t)wrap : VNOWRAP) << 24);
-        t->itab.push_back(make_int4(base[g] + 4 * mm0, g * EZ + mm0,
+        t->itab.push_back(make_int4(base[g] + vb * mm0, g * EZ + mm0,
                                     d | (v0 << 8) | (v1 << 16) | (absent << 24) |
                                         (vmode[g] << 25),
                                     (int)w));
@@ -517,10 +522,11 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
 }
 
 struct QceArgs {
-  const float *llr;
+  const void *llr;              // float or double (the kernel's value type)
   int64_t ld_llr;
   int nblk, n, iters;
   float alpha;
+  double alpha_d;               // the scale of the float64 kernels
   // shared-memory layout (byte offsets): syndrome exchange words, per-chunk
   // row-slot table, per-row info, variable-phase items, heavy-row slots; the
   // bitmap sits at 0
@@ -560,25 +566,24 @@ struct QceArgs {
 // entries are loaded in storage order, the sum is formed in the reference
 // order (slots s0 .. D-1, then 0 .. s0-1) by selecting the rotated value for
 // each position, and every slot is rewritten as tot - m.
-template <bool TORCH, int D>
-__device__ __forceinline__ float qce_var_exact(float *col, int s0, float li,
-                                               bool mv) {
-  float m[D];
+template <typename V, bool TORCH, int D>
+__device__ __forceinline__ V qce_var_exact(V *col, int s0, V li, bool mv) {
+  V m[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) m[i] = col[i * EZ];
   const int s = s0 >= D ? s0 - D : s0;
-  float acc = TORCH ? li : 0.f;
+  V acc = TORCH ? li : V(0);
 #pragma unroll
   for (int t = 0; t < D; ++t) {
-    float v = m[t];
+    V v = m[t];
 #pragma unroll
     for (int c = 1; c < D; ++c) v = (s == c) ? m[(c + t) % D] : v;
-    acc = __fadd_rn(acc, v);
+    acc = add_rn(acc, v);
   }
-  const float tot = TORCH ? acc : __fadd_rn(li, acc);
+  const V tot = TORCH ? acc : add_rn(li, acc);
   if (mv) {
 #pragma unroll
-    for (int i = 0; i < D; ++i) col[i * EZ] = __fsub_rn(tot, m[i]);
+    for (int i = 0; i < D; ++i) col[i * EZ] = sub_rn(tot, m[i]);
   }
   return tot;
 }
@@ -590,21 +595,21 @@ __device__ __forceinline__ float qce_var_exact(float *col, int s0, float li,
 // [lo, hi) needs a per-lane choice (adding -0.0 leaves a float sum
 // unchanged).  The order of additions is each lane's own, so the sum is
 // exact.
-__device__ __forceinline__ float qce_seg_sum(float acc, const float *col, int d,
-                                             int s0) {
+template <typename V>
+__device__ __forceinline__ V qce_seg_sum(V acc, const V *col, int d, int s0) {
   const int lo = (int)__reduce_min_sync(0xffffffffu, (uint32_t)s0);
   const int hi = (int)__reduce_max_sync(0xffffffffu, (uint32_t)s0);
   for (int i = lo; i < hi; ++i) {                  // own tail, first part
-    const float m = col[i * EZ];
-    acc = __fadd_rn(acc, i >= s0 ? m : -0.f);
+    const V m = col[i * EZ];
+    acc = add_rn(acc, i >= s0 ? m : V(-0.0));
   }
 #pragma unroll 4
-  for (int i = hi; i < d; ++i) acc = __fadd_rn(acc, col[i * EZ]);
+  for (int i = hi; i < d; ++i) acc = add_rn(acc, col[i * EZ]);
 #pragma unroll 4
-  for (int i = 0; i < lo; ++i) acc = __fadd_rn(acc, col[i * EZ]);
+  for (int i = 0; i < lo; ++i) acc = add_rn(acc, col[i * EZ]);
   for (int i = lo; i < hi; ++i) {                  // own head, last part
-    const float m = col[i * EZ];
-    acc = __fadd_rn(acc, i < s0 ? m : -0.f);
+    const V m = col[i * EZ];
+    acc = add_rn(acc, i < s0 ? m : V(-0.0));
   }
   return acc;
 }
@@ -613,24 +618,23 @@ __device__ __forceinline__ float qce_seg_sum(float acc, const float *col, int d,
 // first dA slots lie in the accumulator rows and the rest in the identity
 // rows (dA == d for one zone): the reference order is zone A rotated at s0,
 // then zone B rotated at s0b; every slot is rewritten as tot - m.
-template <bool TORCH>
-__device__ __forceinline__ float qce_var_generic(float *col, int d, int dA,
-                                                 int s0, int s0b, float li,
-                                                 bool mv) {
-  float acc = TORCH ? li : 0.f;
+template <typename V, bool TORCH>
+__device__ __forceinline__ V qce_var_generic(V *col, int d, int dA, int s0,
+                                             int s0b, V li, bool mv) {
+  V acc = TORCH ? li : V(0);
   acc = qce_seg_sum(acc, col, dA, s0);
   if (dA < d) acc = qce_seg_sum(acc, col + dA * EZ, d - dA, s0b);
-  const float tot = TORCH ? acc : __fadd_rn(li, acc);
+  const V tot = TORCH ? acc : add_rn(li, acc);
   if (mv) {
     int i = 0;
     for (; i + 4 <= d; i += 4) {
-      float v[4];
+      V v[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) v[u] = col[(i + u) * EZ];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) col[(i + u) * EZ] = __fsub_rn(tot, v[u]);
+      for (int u = 0; u < 4; ++u) col[(i + u) * EZ] = sub_rn(tot, v[u]);
     }
-    for (; i < d; ++i) col[i * EZ] = __fsub_rn(tot, col[i * EZ]);
+    for (; i < d; ++i) col[i * EZ] = sub_rn(tot, col[i * EZ]);
   }
   return tot;
 }
@@ -640,7 +644,7 @@ __device__ __forceinline__ float qce_var_generic(float *col, int d, int dA,
 // checks (no masking at all); otherwise `live` masks absent slots (rows of
 // lower degree, the missing wrap edge of check (0, 0), lanes past 359), whose
 // loads and stores go to a junk word.  Returns the lane's syndrome bit.
-template <bool TORCH, int D, bool FULL, typename MASK>
+template <typename V, bool TORCH, int D, bool FULL, typename MASK>
 __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
                                               uint32_t lane,
                                               const uint32_t *bm,
@@ -649,8 +653,9 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
   // per slot: address, remote load (its value is first used by the update
   // below, so the syndrome lookup overlaps its latency), syndrome bit; the
   // syndrome-only final pass loads too (valid addresses, values unused)
+  constexpr uint32_t VB = sizeof(V);
   uint32_t ad[D];
-  float t[D];
+  V t[D];
   uint32_t synw = 0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
@@ -658,12 +663,12 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
     const uint32_t x = (e.y >> 16) + lane;
     const uint32_t o = min(x, x - (uint32_t)EZ);    // (b + lane) mod 360
     if constexpr (FULL) {
-      ad[j] = e.x + 4u * o;
+      ad[j] = e.x + VB * o;
     } else {
       const uint32_t on = (uint32_t)(live >> j) & 1u;
-      ad[j] = on ? e.x + 4u * o : dummy;
+      ad[j] = on ? e.x + VB * o : dummy;
     }
-    t[j] = dsmem_ld_f32(ad[j]);
+    t[j] = dsmem_ld<V>(ad[j]);
     const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
     if constexpr (FULL) {
       synw ^= hw >> (o & 31);
@@ -672,7 +677,7 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
     }
   }
   if (upd) {
-    const float inf = __int_as_float(0x7f800000);
+    const V inf = vinf<V>();
     // min1/min2 with min/max only: the reference's strict-< update
     // (ldpc_kernel.c:121-126) gives min2 = min(min2, max(min1, mag)),
     // min1 = min(min1, mag), including ties
@@ -680,13 +685,13 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
     // message by comparing |t| with min1; longer rows track the first
     // minimum's position instead, so the values can die early (registers).
     constexpr bool BY_VALUE = D <= 11;
-    float min1 = inf, min2 = inf;
+    V min1 = inf, min2 = inf;
     uint32_t first = 0;
     MASK sv = 0;
 #pragma unroll
     for (int j = 0; j < D; ++j) {
-      float mag = fabsf(t[j]);
-      bool ng = t[j] < 0.f;
+      V mag = vabs(t[j]);
+      bool ng = t[j] < V(0);
       if constexpr (!FULL) {
         const bool on = (live >> j) & 1;
         mag = on ? mag : inf;
@@ -694,15 +699,19 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
       }
       sv |= ng ? ((MASK)1 << j) : (MASK)0;
       if constexpr (!BY_VALUE) first = mag < min1 ? (uint32_t)j : first;
-      min2 = fminf(min2, fmaxf(min1, mag));
-      min1 = fminf(min1, mag);
+      min2 = vmin(min2, vmax(min1, mag));
+      min1 = vmin(min1, mag);
     }
     constexpr bool WIDE = sizeof(MASK) > 4;
     int par;
     if constexpr (WIDE) par = __popcll((unsigned long long)sv) & 1;
     else par = __popc((uint32_t)sv) & 1;
-    float wa = a.alpha, wb = 0.f;
-    if (a.walpha) {
+    // float32: scale a.alpha or the learned (scale, offset); float64: the
+    // scale a.alpha_d (no learned weights)
+    V wa, wb = V(0);
+    if constexpr (sizeof(V) == 8) wa = a.alpha_d;
+    else wa = a.alpha;
+    if (sizeof(V) == 4 && a.walpha) {
       int nl = D;
       if constexpr (!FULL) {
         if constexpr (WIDE) nl = __popcll((unsigned long long)live);
@@ -712,11 +721,11 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
       wa = __ldg(a.walpha + wi);
       wb = __ldg(a.wbeta + wi);
     }
-    float A = __fsub_rn(__fmul_rn(min1, wa), wb);
-    float B = __fsub_rn(__fmul_rn(min2, wa), wb);
-    A = A > 0.f ? A : 0.f;
-    B = B > 0.f ? B : 0.f;
-    const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
+    V A = sub_rn(mul_rn(min1, wa), wb);
+    V B = sub_rn(mul_rn(min2, wa), wb);
+    A = A > V(0) ? A : V(0);
+    B = B > V(0) ? B : V(0);
+    const auto ua = vbits(A), ub = vbits(B);
     MASK all;
     if constexpr (FULL) all = (D >= 8 * (int)sizeof(MASK)) ? ~(MASK)0 : (((MASK)1 << D) - 1);
     else all = live;
@@ -727,10 +736,9 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
 #pragma unroll
     for (int j = 0; j < D; ++j) {
       bool take2;
-      if constexpr (BY_VALUE) take2 = fabsf(t[j]) == min1;
+      if constexpr (BY_VALUE) take2 = vabs(t[j]) == min1;
       else take2 = (uint32_t)j == first;
-      const uint32_t mg = take2 ? ub : ua;
-      dsmem_st_u32(ad[j], mg | (((uint32_t)(neg >> j) & 1u) << 31));
+      dsmem_st_msg(ad[j], take2 ? ub : ua, (uint32_t)(neg >> j) & 1u);
     }
   }
   return (int)(synw & 1u);
@@ -813,15 +821,16 @@ __device__ __forceinline__ void qce_heavy_pass2(const uint2 *he, int j0, int j1,
 // syndrome bit, min1/min2/first (strict <, ldpc_kernel.c:121-126) and the
 // sign parity; pass 2 loads each value again (this lane alone writes it,
 // after reading) and stores the message.  Returns the lane's syndrome bit.
-template <bool TORCH>
+template <typename V, bool TORCH>
 __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wrapj,
                                             uint32_t lane, int ch,
                                             const uint32_t *bm, uint32_t dummy,
                                             bool upd, const QceArgs &a, int it) {
   const int k0 = ch * 32 + (int)lane;
   const bool lv = k0 < EZ;
-  const float inf = __int_as_float(0x7f800000);
-  float min1 = inf, min2 = inf;
+  constexpr uint32_t VB = sizeof(V);
+  const V inf = vinf<V>();
+  V min1 = inf, min2 = inf;
   int first = 0;
   uint32_t par = 0, synw = 0;
   for (int j = 0; j < deg; ++j) {
@@ -831,30 +840,32 @@ __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wra
     const uint32_t x = (uint32_t)bb + lane;
     const uint32_t o = min(x, x - (uint32_t)EZ);
     const bool on = lv && !(k0 == 0 && j == wrapj);
-    const float t = dsmem_ld_f32(on ? e.x + 4u * o : dummy);
+    const V t = dsmem_ld<V>(on ? e.x + VB * o : dummy);
     if (on) {
       const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
       synw ^= hw >> (o & 31);
-      const float mag = fabsf(t);
-      par ^= t < 0.f ? 1u : 0u;
+      const V mag = vabs(t);
+      par ^= t < V(0) ? 1u : 0u;
       first = mag < min1 ? j : first;
-      min2 = fminf(min2, fmaxf(min1, mag));
-      min1 = fminf(min1, mag);
+      min2 = vmin(min2, vmax(min1, mag));
+      min1 = vmin(min1, mag);
     }
   }
   if (upd) {
-    float wa = a.alpha, wb = 0.f;
-    if (a.walpha) {
+    V wa, wb = V(0);
+    if constexpr (sizeof(V) == 8) wa = a.alpha_d;
+    else wa = a.alpha;
+    if (sizeof(V) == 4 && a.walpha) {
       const int nl = deg - ((k0 == 0 && wrapj >= 0) ? 1 : 0);
       const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
       wa = __ldg(a.walpha + wi);
       wb = __ldg(a.wbeta + wi);
     }
-    float A = __fsub_rn(__fmul_rn(min1, wa), wb);
-    float B = __fsub_rn(__fmul_rn(min2, wa), wb);
-    A = A > 0.f ? A : 0.f;
-    B = B > 0.f ? B : 0.f;
-    const uint32_t ua = __float_as_uint(A), ub = __float_as_uint(B);
+    V A = sub_rn(mul_rn(min1, wa), wb);
+    V B = sub_rn(mul_rn(min2, wa), wb);
+    A = A > V(0) ? A : V(0);
+    B = B > V(0) ? B : V(0);
+    const auto ua = vbits(A), ub = vbits(B);
     for (int j = 0; j < deg; ++j) {
       const uint2 e = he[j];
       int bb = ch * 32 - (int)(e.y >> 16);
@@ -863,10 +874,9 @@ __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wra
       const uint32_t o = min(x, x - (uint32_t)EZ);
       const bool on = lv && !(k0 == 0 && j == wrapj);
       if (on) {
-        const uint32_t ad = e.x + 4u * o;
-        const float t = dsmem_ld_f32(ad);
-        const uint32_t sg = par ^ (t < 0.f ? 1u : 0u);
-        dsmem_st_u32(ad, (j == first ? ub : ua) | (sg << 31));
+        const uint32_t ad = e.x + VB * o;
+        const V t = dsmem_ld<V>(ad);
+        dsmem_st_msg(ad, j == first ? ub : ua, par ^ (t < V(0) ? 1u : 0u));
       }
     }
   }
@@ -875,7 +885,7 @@ __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wra
 
 // NS: compile-time slots per block row (qce_ns); NT: threads per CTA; TA:
 // the Type A paths (rows above NS, columns in both zones) are compiled in.
-template <bool TORCH, int NS, int NT, bool TA>
+template <typename V, bool TORCH, int NS, int NT, bool TA>
 __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   using MASK = typename std::conditional<(NS > 32), unsigned long long,
                                          uint32_t>::type;
@@ -979,7 +989,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   constexpr int ABSENT_LANE = EZ - 32 * (ECHUNK - 1) - 1;
 
   for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
-    const float *lam = a.llr + (size_t)b * a.ld_llr;
+    const V *lam = reinterpret_cast<const V *>(a.llr) + (size_t)b * a.ld_llr;
     // ---- prologue: q = lam - 0 = lam on every slot, hard bits of lam; the
     // absent entry holds -0.0 (adding it is exact) ---------------------------
     for (int w = warp; w < nvitems; w += nwarps) {
@@ -994,11 +1004,11 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         if (nval == 0) break;                         // 32-bit item
         const bool mv = (uint32_t)lane < nval;
         const bool absent = sub == asub && ((iw.z >> 24) & 1u) && lane == ABSENT_LANE;
-        const float li = mv ? lam[iw.y + 32 * sub + lane] : 0.f;
-        float *col = reinterpret_cast<float *>(smem + iw.x) + 32 * sub + lane;
+        const V li = mv ? lam[iw.y + 32 * sub + lane] : V(0);
+        V *col = reinterpret_cast<V *>(smem + iw.x) + 32 * sub + lane;
         if (mv)
-          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == wrapi) ? -0.f : li;
-        const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < 0.f);
+          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == wrapi) ? V(-0.0) : li;
+        const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < V(0));
         if (lane < CL) dsmem_st_u32(bm_peer + ((iw.w & 0xFFFFu) + sub) * 4u, hb);
       }
     }
@@ -1016,7 +1026,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       // pass 1 of every heavy item part (one warp each; partials to shared
       // memory) and the light items; phase B (after a CTA barrier) = merge
       // each item's partials and pass 2 of every part.
-      const bool split = HV && a.nhrows && a.hsplit > 1;
+      // (the parts path is float32 only; float64 plans keep one warp per item)
+      const bool split = HV && sizeof(V) == 4 && a.nhrows && a.hsplit > 1;
       const int nhp = (HV && a.nhrows) ? (split ? nhi * a.hsplit : nhi) : 0;
       for (int w = warp; w < nhp + ncitems; w += nwarps) {
         int syn;
@@ -1024,7 +1035,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           const int hi = __ldg(a.hitems + h0 + w);
           const int row = hi / ECHUNK;
           const int4 hf = hinfo[row];
-          mybad += qce_check_heavy<TORCH>(htab + hf.x, hf.z, hf.y - 1, (uint32_t)lane,
+          mybad += qce_check_heavy<V, TORCH>(htab + hf.x, hf.z, hf.y - 1, (uint32_t)lane,
                                           hi - row * ECHUNK, bm, dummy, upd, a, it);
           continue;
         }
@@ -1049,15 +1060,15 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
         const bool full = wm == 0 && ch < ECHUNK - 1;
         if (full && deg == NS) {
-          syn = qce_check_item<TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
+          syn = qce_check_item<V, TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
         } else if (full && deg == NS - 1) {
-          syn = qce_check_item<TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
+          syn = qce_check_item<V, TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
         } else {
           const int k0 = ch * 32 + lane;
           MASK live = rinfo[3 * rl];
           if (k0 == 0) live &= ~wm;                  // check (0, 0): no wrap edge
           if (k0 >= EZ) live = 0;                    // lanes past the circulant
-          syn = qce_check_item<TORCH, NS, false, MASK>(te, live, lane, bm, dummy, upd, a, it);
+          syn = qce_check_item<V, TORCH, NS, false, MASK>(te, live, lane, bm, dummy, upd, a, it);
           syn = k0 < EZ ? syn : 0;
         }
         mybad += syn;
@@ -1166,47 +1177,47 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           const uint32_t nv0 = (iw.z >> 8) & 0xFFu, nv1 = (iw.z >> 16) & 0xFFu;
           const bool mv0 = (uint32_t)lane < nv0, mv1 = (uint32_t)lane < nv1;
           const int l0 = mv0 ? lane : 0, l1 = mv1 ? 32 + lane : 0;
-          const float li0 = lam[iw.y + l0], li1 = lam[iw.y + l1];
-          float *col0 = reinterpret_cast<float *>(smem + iw.x) + l0;
-          float *col1 = reinterpret_cast<float *>(smem + iw.x) + l1;
-          float t0, t1;
+          const V li0 = lam[iw.y + l0], li1 = lam[iw.y + l1];
+          V *col0 = reinterpret_cast<V *>(smem + iw.x) + l0;
+          V *col1 = reinterpret_cast<V *>(smem + iw.x) + l1;
+          V t0, t1;
           if (mode == VM_PAIR) {
             // dual-diagonal parity column: slots in check order for every
             // bit (u = 0 twice, or u = 0, 1 for the last column, whose wrap
             // entry of bit 359 is absent and holds -0.0)
-            const float a0 = col0[0], b0 = col0[EZ], a1 = col1[0], b1 = col1[EZ];
-            float s0 = TORCH ? li0 : 0.f, s1 = TORCH ? li1 : 0.f;
-            s0 = __fadd_rn(__fadd_rn(s0, a0), b0);
-            s1 = __fadd_rn(__fadd_rn(s1, a1), b1);
-            t0 = TORCH ? s0 : __fadd_rn(li0, s0);
-            t1 = TORCH ? s1 : __fadd_rn(li1, s1);
+            const V a0 = col0[0], b0 = col0[EZ], a1 = col1[0], b1 = col1[EZ];
+            V s0 = TORCH ? li0 : V(0), s1 = TORCH ? li1 : V(0);
+            s0 = add_rn(add_rn(s0, a0), b0);
+            s1 = add_rn(add_rn(s1, a1), b1);
+            t0 = TORCH ? s0 : add_rn(li0, s0);
+            t1 = TORCH ? s1 : add_rn(li1, s1);
             const bool absent = ((iw.z >> 24) & 1u) && lane == ABSENT_LANE;
             if (mv0) {
-              col0[0] = __fsub_rn(t0, a0);
-              col0[EZ] = __fsub_rn(t0, b0);
+              col0[0] = sub_rn(t0, a0);
+              col0[EZ] = sub_rn(t0, b0);
             }
             if (mv1) {
-              col1[0] = __fsub_rn(t1, a1);
-              col1[EZ] = absent ? -0.f : __fsub_rn(t1, b1);
+              col1[0] = sub_rn(t1, a1);
+              col1[EZ] = absent ? V(-0.0) : sub_rn(t1, b1);
             }
           } else {
             const int r0s = __ldg(a.s0 + iw.y + l0), r1s = __ldg(a.s0 + iw.y + l1);
             if (d == 3) {
-              t0 = qce_var_exact<TORCH, 3>(col0, r0s, li0, mv0);
-              t1 = qce_var_exact<TORCH, 3>(col1, r1s, li1, mv1);
+              t0 = qce_var_exact<V, TORCH, 3>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<V, TORCH, 3>(col1, r1s, li1, mv1);
             } else if (d == 4) {
-              t0 = qce_var_exact<TORCH, 4>(col0, r0s, li0, mv0);
-              t1 = qce_var_exact<TORCH, 4>(col1, r1s, li1, mv1);
+              t0 = qce_var_exact<V, TORCH, 4>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<V, TORCH, 4>(col1, r1s, li1, mv1);
             } else if (d == 2) {
-              t0 = qce_var_exact<TORCH, 2>(col0, r0s, li0, mv0);
-              t1 = qce_var_exact<TORCH, 2>(col1, r1s, li1, mv1);
+              t0 = qce_var_exact<V, TORCH, 2>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<V, TORCH, 2>(col1, r1s, li1, mv1);
             } else {
-              t0 = qce_var_exact<TORCH, 1>(col0, r0s, li0, mv0);
-              t1 = qce_var_exact<TORCH, 1>(col1, r1s, li1, mv1);
+              t0 = qce_var_exact<V, TORCH, 1>(col0, r0s, li0, mv0);
+              t1 = qce_var_exact<V, TORCH, 1>(col1, r1s, li1, mv1);
             }
           }
-          const uint32_t h0 = __ballot_sync(0xffffffffu, mv0 && t0 < 0.f);
-          const uint32_t h1 = __ballot_sync(0xffffffffu, mv1 && t1 < 0.f);
+          const uint32_t h0 = __ballot_sync(0xffffffffu, mv0 && t0 < V(0));
+          const uint32_t h1 = __ballot_sync(0xffffffffu, mv1 && t1 < V(0));
           if (lane < CL) {
             dsmem_st_u32(bm_peer + bw * 4u, h0);
             if (nv1) dsmem_st_u32(bm_peer + (bw + 1) * 4u, h1);
@@ -1216,20 +1227,20 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           const bool mv = (uint32_t)lane < ((iw.z >> 8) & 0xFFu);
           const int ln = mv ? lane : 0;          // lanes past 359 read bit 0
           const int lamidx = (int)iw.y + ln;
-          const float li = lam[lamidx];
-          float *col = reinterpret_cast<float *>(smem + iw.x) + ln;
+          const V li = lam[lamidx];
+          V *col = reinterpret_cast<V *>(smem + iw.x) + ln;
           const int s0 = __ldg(a.s0 + lamidx);
           int dA = d, s0b = 0;
           if (TA && mode == VM_GEN2) {
             dA = (int)((iw.w >> 16) & 0xFFu);
             s0b = __ldg(a.s0b + lamidx);
           }
-          const float tot = qce_var_generic<TORCH>(col, d, dA, s0, s0b, li, mv);
+          const V tot = qce_var_generic<V, TORCH>(col, d, dA, s0, s0b, li, mv);
           // the absent wrap entry (bit 359 = lane 7 of the last item) stays
           // -0.0
           if (((iw.z >> 24) & 1u) && lane == ABSENT_LANE)
-            col[(int)(iw.w >> 24) * EZ] = -0.f;
-          const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < 0.f);
+            col[(int)(iw.w >> 24) * EZ] = V(-0.0);
+          const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < V(0));
           if (lane < CL) dsmem_st_u32(bm_peer + bw * 4u, hb);
         }
       }
@@ -1244,37 +1255,41 @@ typedef void (*QceFn)(const QceArgs);
 // NS <= 17 keeps a check's slot addresses and values in the 64 registers of
 // the 1024-thread build; larger NS run 512 threads (128 registers) only.
 template <int NS, bool TA>
-static QceFn qce_pick(int semantics, bool big) {
+static QceFn qce_pick(int semantics, bool big, bool f64) {
+  if (f64)       // float64 slots and values: 512 threads (128 registers)
+    return semantics ? ldpc_qce_kernel<double, true, NS, 512, TA>
+                     : ldpc_qce_kernel<double, false, NS, 512, TA>;
   if constexpr (NS <= 17) {
     if (big)
-      return semantics ? ldpc_qce_kernel<true, NS, 1024, TA>
-                       : ldpc_qce_kernel<false, NS, 1024, TA>;
+      return semantics ? ldpc_qce_kernel<float, true, NS, 1024, TA>
+                       : ldpc_qce_kernel<float, false, NS, 1024, TA>;
   }
-  return semantics ? ldpc_qce_kernel<true, NS, 512, TA>
-                   : ldpc_qce_kernel<false, NS, 512, TA>;
+  return semantics ? ldpc_qce_kernel<float, true, NS, 512, TA>
+                   : ldpc_qce_kernel<float, false, NS, 512, TA>;
 }
 
 // ta: the plan has identity rows (a Type A code); its kernels carry the
 // Type A paths and take 4, 6 or 8 slots (qce_ns_a of the identity rows).
-static QceFn qce_fn(int semantics, int dr, int threads, bool ta) {
-  const bool big = threads > 512;
+// f64: the float64 build (the plan's slots hold doubles).
+static QceFn qce_fn(int semantics, int dr, int threads, bool ta, bool f64 = false) {
+  const bool big = threads > 512 && !f64;
   if (ta) {
     switch (qce_ns_a(dr)) {
-      case 4: return qce_pick<4, true>(semantics, big);
-      case 6: return qce_pick<6, true>(semantics, big);
-      case 8: return qce_pick<8, true>(semantics, big);
+      case 4: return qce_pick<4, true>(semantics, big, f64);
+      case 6: return qce_pick<6, true>(semantics, big, f64);
+      case 8: return qce_pick<8, true>(semantics, big, f64);
       default: return nullptr;
     }
   }
   switch (qce_ns(dr)) {
-    case 8: return qce_pick<8, false>(semantics, big);
-    case 10: return qce_pick<10, false>(semantics, big);
-    case 11: return qce_pick<11, false>(semantics, big);
-    case 14: return qce_pick<14, false>(semantics, big);
-    case 17: return qce_pick<17, false>(semantics, big);
-    case 22: return qce_pick<22, false>(semantics, big);
-    case 34: return qce_pick<34, false>(semantics, big);
-    case 56: return qce_pick<56, false>(semantics, big);
+    case 8: return qce_pick<8, false>(semantics, big, f64);
+    case 10: return qce_pick<10, false>(semantics, big, f64);
+    case 11: return qce_pick<11, false>(semantics, big, f64);
+    case 14: return qce_pick<14, false>(semantics, big, f64);
+    case 17: return qce_pick<17, false>(semantics, big, f64);
+    case 22: return qce_pick<22, false>(semantics, big, f64);
+    case 34: return qce_pick<34, false>(semantics, big, f64);
+    case 56: return f64 ? nullptr : qce_pick<56, false>(semantics, big, false);
     default: return nullptr;
   }
 }
@@ -1346,10 +1361,9 @@ struct atsc3_ldpc_qce_plan {
 
 extern "C" {
 
-int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
-                                    int32_t qb, const int32_t *rowptr,
-                                    const int32_t *addr, int32_t cluster,
-                                    atsc3_ldpc_qce_plan **out) {
+static int32_t qce_plan_create_vb(int32_t n, int32_t kldpc, int32_t qa, int32_t qb,
+                                  const int32_t *rowptr, const int32_t *addr,
+                                  int32_t cluster, int vb, atsc3_ldpc_qce_plan **out) {
   using namespace atsc3;
   ATSC3_ARG(out && rowptr && addr, "null argument");
   *out = nullptr;
@@ -1365,7 +1379,7 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
     // rejection (-3, -4 from the build) ends the search with its message
     bool fits = false;
     for (int cl = 1; cl <= EMAXCL; ++cl) {
-      rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cl, &h->p, &t);
+      rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cl, &h->p, &t, vb);
       if (rc) break;
       if (h->p.smem <= smax) {
         fits = true;
@@ -1377,7 +1391,7 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
       rc = -4;
     }
   } else {
-    rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cluster, &h->p, &t);
+    rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cluster, &h->p, &t, vb);
     if (rc == 0 && h->p.smem > smax) {
       set_error("unsupported: per-CTA shared memory above the device limit");
       rc = -4;
@@ -1409,6 +1423,20 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
   }
   *out = h;
   return 0;
+}
+
+int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
+                                    int32_t qb, const int32_t *rowptr,
+                                    const int32_t *addr, int32_t cluster,
+                                    atsc3_ldpc_qce_plan **out) {
+  return qce_plan_create_vb(n, kldpc, qa, qb, rowptr, addr, cluster, 4, out);
+}
+
+int32_t atsc3_ldpc_qce_plan_create_f64(int32_t n, int32_t kldpc, int32_t qa,
+                                       int32_t qb, const int32_t *rowptr,
+                                       const int32_t *addr, int32_t cluster,
+                                       atsc3_ldpc_qce_plan **out) {
+  return qce_plan_create_vb(n, kldpc, qa, qb, rowptr, addr, cluster, 8, out);
 }
 
 int32_t atsc3_ldpc_qce_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
@@ -1641,8 +1669,8 @@ int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *h, int32_t threads,
   using namespace atsc3;
   ATSC3_ARG(h && out, "null argument");
   if (threads <= 0) threads = qce_default_threads(h->p.dr_light);
-  if (qce_ns(h->p.dr_light) > 17) threads = std::min(threads, 512);
-  QceFn fn = qce_fn(semantics, h->p.dr_light, threads, h->p.qb > 0);
+  if (qce_ns(h->p.dr_light) > 17 || h->p.vb == 8) threads = std::min(threads, 512);
+  QceFn fn = qce_fn(semantics, h->p.dr_light, threads, h->p.qb > 0, h->p.vb == 8);
   ATSC3_ARG(fn != nullptr, "no kernel for this degree");
   int ncl = 0;
   int32_t rc = qce_max_clusters(fn, h->p.cluster, h->p.smem, threads, h->p.device, &ncl);
@@ -1654,16 +1682,20 @@ int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *h, int32_t threads,
   return 0;
 }
 
-int32_t atsc3_ldpc_qce_decode_weighted(
-    const atsc3_ldpc_qce_plan *h, const float *llr, int64_t ld_llr,
-    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+static int32_t qce_decode_impl(
+    const atsc3_ldpc_qce_plan *h, const void *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, double alpha, int32_t semantics,
     const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
     const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
     int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
-    int32_t threads, void *stream) {
+    int32_t threads, void *stream, bool f64) {
   using namespace atsc3;
   ATSC3_ARG(h != nullptr, "null plan");
   const QcePlan &p = h->p;
+  ATSC3_ARG(p.vb == (f64 ? 8 : 4),
+            f64 ? "not a float64 plan (atsc3_ldpc_qce_plan_create_f64)"
+                : "a float64 plan needs atsc3_ldpc_qce_decode_f64");
+  ATSC3_ARG(!(f64 && walpha), "learned weights are float32 only");
   ATSC3_ARG(nblk >= 0 && iters >= 0, "negative size");
   ATSC3_ARG(semantics == 0 || semantics == 1, "semantics must be 0 or 1");
   ATSC3_ARG(!(semantics == 1 && iters == 0), "semantics 1 needs iters >= 1");
@@ -1675,8 +1707,8 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   ATSC3_ARG(llr != nullptr, "null llr");
   if (threads <= 0) threads = qce_default_threads(p.dr_light);
   ATSC3_ARG(threads == 512 || threads == 1024, "threads must be 512 or 1024");
-  if (qce_ns(p.dr_light) > 17) threads = 512;   // only the 512-thread build
-  QceFn fn = qce_fn(semantics, p.dr_light, threads, p.qb > 0);
+  if (qce_ns(p.dr_light) > 17 || f64) threads = 512;   // only the 512-thread build
+  QceFn fn = qce_fn(semantics, p.dr_light, threads, p.qb > 0, f64);
   if (!fn) {
     set_error("unsupported: block-row degree too high");
     return -4;
@@ -1696,7 +1728,8 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   a.nblk = nblk;
   a.n = p.n;
   a.iters = iters;
-  a.alpha = alpha;
+  a.alpha = (float)alpha;
+  a.alpha_d = alpha;
   a.part_off = p.part_off;
   a.rt_off = p.rt_off;
   a.ri_off = p.ri_off;
@@ -1749,6 +1782,29 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   cfg.numAttrs = 1;
   ATSC3_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
   return 0;
+}
+
+int32_t atsc3_ldpc_qce_decode_weighted(
+    const atsc3_ldpc_qce_plan *h, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream) {
+  return qce_decode_impl(h, llr, ld_llr, nblk, iters, alpha, semantics, walpha, wbeta,
+                         wT, wnb, dbucket, bits, ld_bits, hard, ld_hard, conv, its, bad,
+                         threads, stream, false);
+}
+
+int32_t atsc3_ldpc_qce_decode_f64(const atsc3_ldpc_qce_plan *h, const double *llr,
+                                  int64_t ld_llr, int32_t nblk, int32_t iters,
+                                  double alpha, int32_t semantics, uint8_t *bits,
+                                  int64_t ld_bits, uint8_t *hard, int64_t ld_hard,
+                                  uint8_t *conv, int32_t *its, int32_t *bad,
+                                  int32_t threads, void *stream) {
+  return qce_decode_impl(h, llr, ld_llr, nblk, iters, alpha, semantics, nullptr, nullptr,
+                         0, 0, nullptr, bits, ld_bits, hard, ld_hard, conv, its, bad,
+                         threads, stream, true);
 }
 
 int32_t atsc3_ldpc_qce_decode(const atsc3_ldpc_qce_plan *h, const float *llr,

@@ -128,19 +128,30 @@ class QcePlan(QcPlan):
 
     kind = "qce"
 
-    def __init__(self, rate, n, cluster=0):
-        typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
-        # accumulator / identity block rows: (Q, 0) for Type B, (Q1, Q2) for
-        # Type A
-        qa, qb = (Q2, 0) if typ == "B" else (Q1, Q2)
-        rowptr, addr = C.address_rows(rate, n)
+    def __init__(self, rate=None, n=None, cluster=0, dtype="float32", tables=None):
+        """rate, n: an A/322 code; or tables = (n, K, qa, qb, rowptr, addr)
+        as atsc3_ldpc_qc_detect2 recovers them from CSR tables.  dtype
+        float32 or float64 (the float64 build: 8-byte slots, float64
+        arithmetic, no learned weights)."""
+        if dtype not in ("float32", "float64"):
+            raise ValueError("dtype must be float32 or float64")
+        if tables is None:
+            typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+            # accumulator / identity block rows: (Q, 0) for Type B, (Q1, Q2)
+            # for Type A
+            qa, qb = (Q2, 0) if typ == "B" else (Q1, Q2)
+            rowptr, addr = C.address_rows(rate, n)
+        else:
+            n, K, qa, qb, rowptr, addr = tables
         rowptr = np.ascontiguousarray(rowptr, np.int32)
         addr = np.ascontiguousarray(addr, np.int32)
         h = ctypes.c_void_p()
-        N.call("atsc3_ldpc_qce_plan_create2", n, K, qa, qb, rowptr.ctypes.data,
-               addr.ctypes.data, int(cluster), ctypes.byref(h))
+        fn = ("atsc3_ldpc_qce_plan_create_f64" if dtype == "float64"
+              else "atsc3_ldpc_qce_plan_create2")
+        N.call(fn, n, K, qa, qb, rowptr.ctypes.data, addr.ctypes.data, int(cluster),
+               ctypes.byref(h))
         self._h = h
-        self.n, self.nc, self.dtype = n, n - K, "float32"
+        self.n, self.nc, self.dtype = n, n - K, dtype
         info = np.zeros(10, np.int64)
         N.call("atsc3_ldpc_qce_plan_info", h, info.ctypes.data)
         self.info = dict(zip(("n", "K", "Q", "cluster", "smem_bytes",
@@ -165,12 +176,13 @@ _PLANS_LOCK = threading.Lock()
 
 
 def plan_for(rate, n, dtype="float32", cluster=0, kind="auto"):
-    """Cached plan of an A/322 code.  kind "auto" picks, in float32, the
-    edge-buffer quasi-cyclic decoder (every code), then the record-layout one
-    (Type B codes with one circulant per block), whichever first accepts the
-    code; else the CSR decoder.  kind "qce" or "qc" asks for that decoder
-    (raising if it rejects a code in its reach); codes outside its reach
-    (float64; Type A for "qc") get the CSR decoder."""
+    """Cached plan of an A/322 code.  kind "auto" picks the edge-buffer
+    quasi-cyclic decoder (every code, float32 or float64), then in float32
+    the record-layout one (Type B codes with one circulant per block),
+    whichever first accepts the code; else the CSR decoder.  kind "qce" or
+    "qc" asks for that decoder (raising if it rejects a code in its reach);
+    codes outside its reach (float64 or Type A for "qc") get the CSR
+    decoder."""
     torch = _torch()
     key = (rate, n, dtype, cluster, kind, torch.cuda.current_device())
     with _PLANS_LOCK:
@@ -178,10 +190,11 @@ def plan_for(rate, n, dtype="float32", cluster=0, kind="auto"):
         if p is None:
             f32 = dtype == "float32"
             type_b = C.ldpc_params(rate, n)[0] == "B"
-            for k, cls, ok in (("qce", QcePlan, f32), ("qc", QcPlan, f32 and type_b)):
+            for k, cls, ok in (("qce", QcePlan, True), ("qc", QcPlan, f32 and type_b)):
                 if p is None and kind in ("auto", k) and ok:
                     try:
-                        p = cls(rate, n, cluster=cluster)
+                        p = (cls(rate, n, cluster=cluster, dtype=dtype) if k == "qce"
+                             else cls(rate, n, cluster=cluster))
                     except N.FecError as e:
                         if kind == k or e.rc != -4:
                             raise
@@ -222,6 +235,15 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     kind = getattr(plan, "kind", "csr")
     if weights is not None and kind not in ("qc", "qce"):
         raise ValueError("learned weights run on the quasi-cyclic decoders")
+    if kind == "qce" and plan.dtype == "float64":
+        if weights is not None:
+            raise ValueError("learned weights run on the float32 decoders")
+        N.call("atsc3_ldpc_qce_decode_f64", plan.handle, llr.data_ptr(),
+               llr.stride(0), nblk, int(iters), float(alpha), SEMANTICS[semantics],
+               N.ptr(bits), bits.stride(0) if bits is not None else 0, N.ptr(hard),
+               hard.stride(0) if hard is not None else 0, o["conv"].data_ptr(),
+               o["its"].data_ptr(), o["bad"].data_ptr(), int(threads), st)
+        return o
     if kind in ("qc", "qce"):
         wa = wb = db = None
         wT = wnb = 0
@@ -246,6 +268,34 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
            hard.stride(0) if hard is not None else 0, o["conv"].data_ptr(),
            o["its"].data_ptr(), o["bad"].data_ptr(), int(threads), st)
     return o
+
+
+def qce_plan_from_csr(tables, n, dtype="float32", cluster=0):
+    """The edge-buffer plan of the A/322 code whose CSR tables these are
+    (atsc3_ldpc_qc_detect2: circulant structure, accumulator and identity
+    parity, reference edge order), or None for any other matrix or a code
+    the decoder does not take."""
+    cptr, cidx, vptr, vedge = [np.ascontiguousarray(t, np.int32) for t in tables]
+    nc, ne = len(cptr) - 1, len(cidx)
+    kq = np.zeros(3, np.int32)
+    rowptr = np.zeros(n // 360 + 1, np.int32)
+    addr = np.zeros(max(ne, 1), np.int32)
+    rc = N.lib().atsc3_ldpc_qc_detect2(cptr.ctypes.data, cidx.ctypes.data,
+                                       vptr.ctypes.data, vedge.ctypes.data, n, nc, ne,
+                                       kq.ctypes.data, rowptr.ctypes.data,
+                                       addr.ctypes.data)
+    if rc == -4:
+        return None
+    N.check("atsc3_ldpc_qc_detect2", rc)
+    K, qa, qb = (int(x) for x in kq)
+    nrows = K // 360 + (qa if qb else 0)
+    try:
+        return QcePlan(dtype=dtype, cluster=cluster,
+                       tables=(n, K, qa, qb, rowptr[:nrows + 1], addr[:rowptr[nrows]]))
+    except N.FecError as e:
+        if e.rc != -4:
+            raise
+        return None
 
 
 class GpuMinSum:
@@ -273,8 +323,12 @@ class GpuMinSum:
         self.dtype_name = dtype
         self.semantics = semantics
         with torch.cuda.device(self.dev):
-            self.plan = Plan(*C.csr_from_checks(checks, n), n, dtype=dtype,
-                             cluster=cluster)
+            tabs = C.csr_from_checks(checks, n)
+            # an A/322 code (recognised from its CSR tables) takes the
+            # edge-buffer decoder, any other matrix the CSR decoder
+            self.plan = qce_plan_from_csr(tabs, n, dtype=dtype, cluster=cluster)
+            if self.plan is None:
+                self.plan = Plan(*tabs, n, dtype=dtype, cluster=cluster)
         self.nc = self.plan.nc
         self.stats = dict(calls=0, iters=0, blocks=0)
 

@@ -208,6 +208,24 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
                                     const int32_t *addr, int32_t cluster,
                                     atsc3_ldpc_qce_plan **out);
 
+/* The float64 edge-buffer decoder (8-byte slots, float64 messages and
+ * posteriors, 512 threads per CTA): the arithmetic of the float64 paths of
+ * lab/m9_gpu.py:168-211 (torch semantics, GpuMinSum's default dtype) and
+ * lab/m3_ldpc.py:560-630, bit for bit; semantics 0 (lab/ldpc_kernel.c
+ * order) in float64 too.  A 64800-bit codeword needs about 12 CTAs.  Plans
+ * from atsc3_ldpc_qce_plan_create_f64 decode only with
+ * atsc3_ldpc_qce_decode_f64 (no learned weights); alpha is a double. */
+int32_t atsc3_ldpc_qce_plan_create_f64(int32_t n, int32_t kldpc, int32_t qa,
+                                       int32_t qb, const int32_t *rowptr,
+                                       const int32_t *addr, int32_t cluster,
+                                       atsc3_ldpc_qce_plan **out);
+int32_t atsc3_ldpc_qce_decode_f64(const atsc3_ldpc_qce_plan *plan, const double *llr,
+                                  int64_t ld_llr, int32_t nblk, int32_t iters,
+                                  double alpha, int32_t semantics, uint8_t *bits,
+                                  int64_t ld_bits, uint8_t *hard, int64_t ld_hard,
+                                  uint8_t *conv, int32_t *its, int32_t *bad,
+                                  int32_t threads, void *stream);
+
 /* Host only.  Recognise an A/322 Type B code in CSR tables built as
  * lab/m3_ldpc.py:459-482 (_kernel_tables) builds them from
  * lab/m3_ldpc.py:166-212 (parity_check): 360-bit circulants, info bit

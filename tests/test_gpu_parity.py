@@ -430,3 +430,48 @@ def test_qce_iters_zero_and_empty_batch(torch):
     assert o["bad"].cpu().numpy().tolist() == want[3].tolist()
     e = decode_flood(plan, torch.zeros((0, n), dtype=torch.float32, device="cuda"))
     assert e["its"].numel() == 0
+
+
+@pytest.mark.parametrize("rate,n", [("10/15", 64800), ("7/15", 64800), ("11/15", 16200),
+                                    ("8/15", 16200), ("3/15", 16200)])
+def test_qce_float64_vs_oracle(rate, n, torch):
+    """The float64 edge-buffer decoder (8-byte slots, float64 arithmetic)
+    against the float64 C oracle, both semantics: Type B, Type A (with heavy
+    accumulator rows) and a 16200 code with two circulants in some blocks."""
+    from atsc3_b200.ldpc import QcePlan, decode_flood
+    plan = QcePlan(rate, n, dtype="float64")
+    rng = np.random.default_rng(n + C.RATES.index(rate))
+    tabs = C.csr(rate, n)
+    llr = rng.standard_normal((4, n)) * 2.0 + 1.4
+    llr[3] = np.abs(llr[3])
+    x = torch.from_numpy(llr).cuda()
+    for sem, code in (("kernel", 0), ("torch", 1)):
+        want = oracle.flood(llr, tabs, n, iters=18, alpha=0.8, semantics=code,
+                            dtype=np.float64)
+        o = decode_flood(plan, x, iters=18, alpha=0.8, semantics=sem, want_hard=True)
+        bits = o["bits"].cpu().numpy()
+        assert np.array_equal(bits, want[0]), (rate, n, sem)
+        assert o["its"].cpu().numpy().tolist() == want[2].tolist(), (rate, n, sem)
+        assert o["bad"].cpu().numpy().tolist() == want[3].tolist(), (rate, n, sem)
+        assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
+        assert np.array_equal(o["hard"].cpu().numpy()[:, :n // 8],
+                              np.packbits(bits, axis=1))
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_gpuminsum_routes_a322_codes_to_the_edge_buffer_decoder(dtype, torch):
+    """GpuMinSum is built from check lists; an A/322 code is recognised and
+    decoded by the edge-buffer plan, with the CSR decoder's outputs."""
+    from atsc3_b200.ldpc import GpuMinSum, Plan, decode_flood
+    rate, n = "9/15", 16200
+    g = GpuMinSum(C.parity_check(rate, n), n, dtype=dtype)
+    assert g.plan.kind == "qce" and g.plan.dtype == dtype
+    rng = np.random.default_rng(4)
+    llr = (rng.standard_normal((5, n)) * 2.0 + 1.8).astype(dtype)
+    got = g.decode(llr)
+    csr = Plan(*C.csr(rate, n), n, dtype=dtype)
+    want = decode_flood(csr, torch.from_numpy(llr).cuda(), iters=50, alpha=0.75,
+                        semantics="torch")
+    assert np.array_equal(got[0], want["bits"].cpu().numpy())
+    assert got[2].tolist() == want["its"].cpu().numpy().tolist()
+    assert got[3].tolist() == want["bad"].cpu().numpy().tolist()
