@@ -212,7 +212,8 @@ int32_t atsc3_ldpc_qce_plan_create2(int32_t n, int32_t kldpc, int32_t qa,
  * posteriors, 512 threads per CTA): the arithmetic of the float64 paths of
  * lab/m9_gpu.py:168-211 (torch semantics, GpuMinSum's default dtype) and
  * lab/m3_ldpc.py:560-630, bit for bit; semantics 0 (lab/ldpc_kernel.c
- * order) in float64 too.  A 64800-bit codeword needs about 12 CTAs.  Plans
+ * order) in float64 too.  A 64800-bit codeword needs at least 11 CTAs;
+ * cluster 0 picks the size that occupies the most SMs (16 on B200).  Plans
  * from atsc3_ldpc_qce_plan_create_f64 decode only with
  * atsc3_ldpc_qce_decode_f64 (no learned weights); alpha is a double. */
 int32_t atsc3_ldpc_qce_plan_create_f64(int32_t n, int32_t kldpc, int32_t qa,
