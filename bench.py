@@ -634,8 +634,9 @@ def run_frame_ti(args):
     blocks of 25 FEC Blocks, A/322 7.1.5.4 twisted block interleaver): each
     step decodes one PLP cell stream with the de-interleave fused into the
     demapper's load (FecPipeline.decode_stream), against the same frames
-    decoded from de-interleaved rows (FecPipeline.decode); per-stage device
-    times of the gather demap and the row demap."""
+    decoded from de-interleaved rows (FecPipeline.decode), frames alternating
+    over --streams streams as in the frame bench (one-stream figures beside);
+    per-stage device times of the gather demap and the row demap."""
     import torch
     from atsc3_b200 import demap as DM
     from atsc3_b200 import timeint as TI
@@ -660,9 +661,35 @@ def run_frame_ti(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / K
 
+    # frames alternate over S streams with a pipeline (workspace) each, as in
+    # the frame bench: one LDPC launch's last round overlaps the next frame
+    S = max(1, args.streams)
+    pipes = [p] + [FecPipeline(N_INNER, MOD, RATE, iters=ITERS, alpha=ALPHA, device=dev)
+                   for _ in range(S - 1)]
+    sts = [torch.cuda.Stream(device=dev) for _ in range(S)]
+
+    def timed_s(fn):
+        main = torch.cuda.current_stream(dev)
+        for f in range(W):
+            fn(f, pipes[f % S])
+        torch.cuda.synchronize()
+        e0.record(main)
+        for st in sts:
+            st.wait_stream(main)
+        for k in range(K):
+            with torch.cuda.stream(sts[k % S]):
+                fn(W + k, pipes[k % S])
+        for st in sts:
+            main.wait_stream(st)
+        e1.record(main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / K
+
     ok = []
-    ms_ti = timed(lambda f: ok.append(p.decode_stream(streams[f], ti, sstreams[f])["ok"].sum()))
-    ms_rows = timed(lambda f: p.decode(cells[f], sig[f]))
+    ms_ti = timed_s(lambda f, q: ok.append(q.decode_stream(streams[f], ti, sstreams[f])["ok"].sum()))
+    ms_rows = timed_s(lambda f, q: q.decode(cells[f], sig[f]))
+    ms_ti1 = timed(lambda f: p.decode_stream(streams[f], ti, sstreams[f]))
+    ms_rows1 = timed(lambda f: p.decode(cells[f], sig[f]))
     dg = timed(lambda f: TI.demap_deinterleave(streams[f], ti, MOD, RATE, N_INNER,
                                                sigma2=sstreams[f]))
     dr = timed(lambda f: DM.demap(cells[f], MOD, RATE, sigma2=sig[f], n=N_INNER))
@@ -670,7 +697,9 @@ def run_frame_ti(args):
                       "(hybrid TI de-interleave fused into the demap load)",
             "value": nblk * kp / (ms_ti / 1e3) / 1e6, "unit": "Mbit/s",
             "ms_per_step": ms_ti, "steps": K, "warmup": W,
-            "rows_mbit_s": nblk * kp / (ms_rows / 1e3) / 1e6,
+            "rows_mbit_s": nblk * kp / (ms_rows / 1e3) / 1e6, "streams": S,
+            "one_stream_mbit_s": nblk * kp / (ms_ti1 / 1e3) / 1e6,
+            "one_stream_rows_mbit_s": nblk * kp / (ms_rows1 / 1e3) / 1e6,
             "gather_demap_ms": dg, "row_demap_ms": dr,
             "ti": {"nrows": ti.nrows, "ncols": ti.ncols, "nti": ti.nti},
             "bch_ok_blocks": int(sum(int(x) for x in ok[W:])),
