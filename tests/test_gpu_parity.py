@@ -475,3 +475,21 @@ def test_gpuminsum_routes_a322_codes_to_the_edge_buffer_decoder(dtype, torch):
     assert np.array_equal(got[0], want["bits"].cpu().numpy())
     assert got[2].tolist() == want["its"].cpu().numpy().tolist()
     assert got[3].tolist() == want["bad"].cpu().numpy().tolist()
+
+
+@pytest.mark.parametrize("n", [16200, 64800])
+def test_all_codes_float64_edge_buffer_equals_csr(n, torch):
+    """Every A/322 code in float64 (torch semantics, GpuMinSum's default):
+    the edge-buffer decoder equals the float64 CSR decoder field by field."""
+    from atsc3_b200.ldpc import Plan, QcePlan, decode_flood
+    rng = np.random.default_rng(n + 64)
+    for rate in C.RATES:
+        llr = rng.standard_normal((3, n)) * 2.2 + 1.4
+        llr[2] = np.abs(llr[2])
+        x = torch.from_numpy(llr).cuda()
+        a = decode_flood(QcePlan(rate, n, dtype="float64"), x, iters=10, alpha=0.75,
+                         semantics="torch")
+        b = decode_flood(Plan(*C.csr(rate, n), n, dtype="float64"), x, iters=10,
+                         alpha=0.75, semantics="torch")
+        for k in ("bits", "conv", "its", "bad"):
+            assert torch.equal(a[k], b[k]), (rate, n, k)
