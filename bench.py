@@ -762,8 +762,9 @@ def run_codes(args):
     """Every A/322 code (16200 and 64800, rates 2/15..13/15): the LDPC launch
     alone on 16-NUC blocks at the code's measured threshold + 1 dB (AWGN,
     atsc3_b200/data/thresholds.json), three blocks per resident cluster, on
-    the edge-buffer decoder and on the CSR decoder; kernel semantics, at
-    most 50 iterations, alpha 0.75.  Outputs of the two decoders must agree."""
+    the edge-buffer decoder and on the CSR decoder; kernel semantics in
+    float32, torch semantics in float64 (--dtype), at most 50 iterations,
+    alpha 0.75.  Outputs of the two decoders must agree."""
     import torch
     from atsc3_b200 import codes as C
     from atsc3_b200 import demap as DM
@@ -775,13 +776,16 @@ def run_codes(args):
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
     steps = max(1, min(args.steps, 8))
 
+    f64 = args.dtype == "float64"
+    sem = "torch" if f64 else "kernel"   # the float64 decoders run torch semantics
+
     def timed(plan, lam):
         for _ in range(args.warmup):
-            LDPC.decode_flood(plan, lam, iters=ITERS, alpha=ALPHA)
+            LDPC.decode_flood(plan, lam, iters=ITERS, alpha=ALPHA, semantics=sem)
         torch.cuda.synchronize()
         e0.record()
         for _ in range(steps):
-            o = LDPC.decode_flood(plan, lam, iters=ITERS, alpha=ALPHA)
+            o = LDPC.decode_flood(plan, lam, iters=ITERS, alpha=ALPHA, semantics=sem)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps, o
@@ -792,8 +796,8 @@ def run_codes(args):
         for r in C.RATES:
             if only and f"{n} {r}" not in only:
                 continue
-            qce = LDPC.plan_for(r, n, kind="qce")
-            csr = LDPC.plan_for(r, n, kind="csr")
+            qce = LDPC.plan_for(r, n, kind="qce", dtype=args.dtype)
+            csr = LDPC.plan_for(r, n, kind="csr", dtype=args.dtype)
             cfg = np.zeros(4, np.int32)
             N.call("atsc3_ldpc_qce_config", qce._h, 0, 0, cfg.ctypes.data)
             nblk = 3 * int(cfg[0])
@@ -804,6 +808,8 @@ def run_codes(args):
             esn0 = thresholds.lookup(n, "16QAM", r) + 1.0
             y, s2 = synth.channel(x, esn0, "awgn", g)
             lam = DM.demap(y, "16QAM", r, sigma2=float(s2), n=n)
+            if f64:
+                lam = lam.double()
             ms_q, oq = timed(qce, lam)
             ms_c, oc = timed(csr, lam)
             same = all(torch.equal(oq[k], oc[k]) for k in ("bits", "conv", "its", "bad"))
@@ -817,7 +823,8 @@ def run_codes(args):
                          "outputs_equal": bool(same)})
     return {"metric": "per-code LDPC decoded info Mbit/s (edge-buffer vs CSR decoder)",
             "unit": "Mbit/s", "steps": steps, "warmup": args.warmup,
-            "data": "synthetic", "dtype": "f32", "codes": rows}
+            "data": "synthetic", "dtype": "f64" if f64 else "f32",
+            "semantics": sem, "codes": rows}
 
 
 def main(argv=None):
@@ -836,6 +843,8 @@ def main(argv=None):
     ap.add_argument("--decoder", default="auto", choices=["auto", "qce", "qc", "csr"],
                     help="LDPC decoder (auto = edge-buffer quasi-cyclic)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dtype", default="float32", choices=["float32", "float64"],
+                    help="--workload codes: decoder arithmetic")
     ap.add_argument("--only", default="",
                     help="--workload codes: comma-separated codes, e.g. '64800 7/15'")
     a = ap.parse_args(argv)
