@@ -1,6 +1,6 @@
 """GPU parity: every CUDA path against the oracle / reference golden vectors.
 
-Bar (BASELINE north_star): hard decisions, iteration counts and BCH outcomes
+Bar: hard decisions, iteration counts and BCH outcomes
 bit-exact with float32 messages; demapper LLRs bit-exact with a supplied
 sigma2 (within 1e-5 relative with the estimated sigma2).
 """
