@@ -22,9 +22,9 @@
 //  * all calls share the one scratch: calls that overlap on the GPU (other
 //    streams, other threads) race and corrupt each other -- serialise them;
 //  * every call writes all the scratch it reads, so nothing needs clearing;
-//  * the LDPC plan is created beforehand (atsc3_ldpc_qc_plan_create or
-//    atsc3_ldpc_plan_create, at set-up); this entry point itself calls no
-//    allocator.
+//  * the LDPC plan is created beforehand (atsc3_ldpc_qce_plan_create /
+//    _create2, atsc3_ldpc_qc_plan_create or atsc3_ldpc_plan_create, at
+//    set-up; float32 plans); this entry point itself calls no allocator.
 
 #include <cuda_runtime.h>
 
@@ -102,7 +102,8 @@ extern "C" int32_t atsc3_fec_decode_noalloc(
     int32_t *bad, uint32_t *syn, uint8_t *ok, void *stream) {
   using namespace atsc3;
   ATSC3_ARG(plan != nullptr, "null plan");
-  ATSC3_ARG(plan_kind == 0 || plan_kind == 1, "plan_kind must be 0 (CSR) or 1 (QC)");
+  ATSC3_ARG(plan_kind >= 0 && plan_kind <= 2,
+            "plan_kind must be 0 (CSR), 1 (QC record layout) or 2 (QC edge buffer)");
   ATSC3_ARG(nblk >= 0 && ncell > 0 && nbits > 0, "bad size");
   const int64_t n = (int64_t)ncell * nbits;
   if (nblk > ATSC3_NOALLOC_MAX_BLOCKS || n > ATSC3_NOALLOC_MAX_N) {
@@ -113,9 +114,11 @@ extern "C" int32_t atsc3_fec_decode_noalloc(
   }
   if (nblk == 0) return 0;
   ATSC3_ARG(lam_of_q != nullptr, "lam_of_q required (codeword order)");
-  if (plan_kind == 1) {
+  if (plan_kind == 1 || plan_kind == 2) {
     int64_t info[10];
-    int32_t rc0 = atsc3_ldpc_qc_plan_info((const atsc3_ldpc_qc_plan *)plan, info);
+    int32_t rc0 = plan_kind == 1
+        ? atsc3_ldpc_qc_plan_info((const atsc3_ldpc_qc_plan *)plan, info)
+        : atsc3_ldpc_qce_plan_info((const atsc3_ldpc_qce_plan *)plan, info);
     if (rc0) return rc0;
     ATSC3_ARG(info[0] == n, "ncell*nbits differs from the plan's codeword length");
   } else {
@@ -130,7 +133,12 @@ extern "C" int32_t atsc3_fec_decode_noalloc(
   rc = demap_launch(cells, ld_cells, nblk, ncell, pts, nbits, sigma_mode,
                     sigma2, ld_sigma, sigma2_scalar, lam_of_q, llr, n, st);
   if (rc) return rc;
-  if (plan_kind == 1) {
+  if (plan_kind == 2) {
+    // a float64 plan is refused here (-3): the scratch holds float32 LLRs
+    rc = atsc3_ldpc_qce_decode((const atsc3_ldpc_qce_plan *)plan, llr, n, nblk,
+                               iters, alpha, 0, nullptr, 0, hard,
+                               ATSC3_NOALLOC_HARD_LD, conv, its, bad, 0, stream);
+  } else if (plan_kind == 1) {
     rc = atsc3_ldpc_qc_decode((const atsc3_ldpc_qc_plan *)plan, llr, n, nblk,
                               iters, alpha, 0, nullptr, 0, hard,
                               ATSC3_NOALLOC_HARD_LD, conv, its, bad, 0, stream);

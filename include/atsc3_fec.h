@@ -534,11 +534,11 @@ int32_t atsc3_bch_batch(const uint8_t *hard, const int64_t *hard_off,
  * torch).  For callers that must not allocate device memory on their decode
  * path -- a real-time loop with a fixed memory budget, or a host that only
  * lends the GPU pre-reserved buffers: the demap -> LDPC -> BCH chain of
- * atsc3_demap / atsc3_ldpc_qc_decode (plan_kind 1) or
- * atsc3_ldpc_decode_flood (plan_kind 0) / atsc3_bch_check in one call, with
- * its LLR and hard-decision intermediates in a fixed file-scope device
- * scratch (about 4.3 MB on every GPU that loads the library) instead of
- * caller buffers.  Limit: at most 16 codewords of at most 64800 bits per
+ * atsc3_demap / atsc3_ldpc_qce_decode (plan_kind 2), atsc3_ldpc_qc_decode
+ * (plan_kind 1) or atsc3_ldpc_decode_flood (plan_kind 0) / atsc3_bch_check
+ * in one call, with its LLR and hard-decision intermediates in a fixed
+ * file-scope device scratch (about 4.3 MB on every GPU that loads the
+ * library) instead of caller buffers.  Limit: at most 16 codewords of at most 64800 bits per
  * call (-3 otherwise).  The first call on a device looks up the scratch
  * address: make it before any stream capture.  Calls that overlap on the GPU
  * share the scratch and race.  Arguments mean what they mean for the three

@@ -35,8 +35,9 @@ def _noalloc(torch, p, cells, s2):
            "bad": torch.empty(nblk, dtype=torch.int32, device=dev),
            "syn": torch.empty((nblk, 6), dtype=torch.int32, device=dev),
            "ok": torch.empty(nblk, dtype=torch.uint8, device=dev)}
-    # the entry point takes CSR (0) and record-layout quasi-cyclic (1) plans
-    kinds = {"csr": 0, "qc": 1}
+    # the entry point takes CSR (0), record-layout quasi-cyclic (1) and
+    # edge-buffer quasi-cyclic (2) plans
+    kinds = {"csr": 0, "qc": 1, "qce": 2}
     plan_kind = getattr(p.plan, "kind", "csr")
     assert plan_kind in kinds, f"no-alloc entry point has no {plan_kind} plans"
     kind = kinds[plan_kind]
@@ -61,15 +62,18 @@ def _kind(c):
     return "qc" if C.ldpc_params(c["rate"], c["n"])[0] == "B" else "csr"
 
 
-def test_noalloc_matches_regular_path_twice():
+@pytest.mark.parametrize("kinds", ["qc_csr", "qce"])
+def test_noalloc_matches_regular_path_twice(kinds):
     import torch
     from atsc3_b200.pipeline import FecPipeline
-    # two different codes (quasi-cyclic and CSR decoders) in a row: the
-    # second call reuses the scratch the first one left behind
+    # two different codes (Type B and Type A) in a row: the second call
+    # reuses the scratch the first one left behind
     for name in ("c64_16qam_6_15_ray", "c64_64qam_7_15", "c64_16qam_6_15_ray"):
         c, pay, cw, cells, s2, q, lam = oracle_case(name)
+        kind = _kind(c) if kinds == "qc_csr" else "qce"
         p = FecPipeline(c["n"], c["mod"], c["rate"], iters=50, alpha=0.75,
-                        kind=_kind(c))
+                        kind=kind)
+        assert p.plan.kind == kind
         s2d = float(s2) if np.ndim(s2) == 0 else \
             torch.from_numpy(np.ascontiguousarray(s2, np.float32)).cuda()
         ws = p.decode(torch.from_numpy(cells).cuda(), s2d)
@@ -90,3 +94,16 @@ def test_noalloc_rejects_oversize_batch():
     with pytest.raises(N.FecError) as e:
         _noalloc(torch, p, cells, 1.0)
     assert e.value.rc == -3 and "at most 16" in str(e.value)
+
+
+def test_noalloc_rejects_float64_edge_buffer_plan():
+    import torch
+    from atsc3_b200 import ldpc as LDPC
+    from atsc3_b200 import native as N
+    from atsc3_b200.pipeline import FecPipeline
+    p = FecPipeline(16200, "QPSK", "6/15", kind="qce")
+    p.plan = LDPC.QcePlan("6/15", 16200, dtype="float64")
+    cells = np.zeros((2, p.ncell), np.complex64)
+    with pytest.raises(N.FecError) as e:
+        _noalloc(torch, p, cells, 1.0)
+    assert e.value.rc == -3 and "float64" in str(e.value)
