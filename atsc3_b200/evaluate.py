@@ -2,6 +2,7 @@
 iteration sweeps (all on the GPU, BCH as the arbiter).
 
     python -m atsc3_b200.evaluate [--steps 2000] [--batch 256] [--blocks 100000]
+    python -m atsc3_b200.evaluate --compare 6/15 16QAM 8.25 --blocks 11111
 
 For each MODCOD (64800-bit rate 6/15 with 16-NUC, 8/15 with 64-NUC, 10/15
 with 256-NUC):
@@ -35,6 +36,7 @@ from . import codes as C
 from . import demap as DM
 from . import ldpc as LDPC
 from . import learned as LR
+from . import native as N
 from . import synth
 
 MODCODS = (("6/15", "16QAM"), ("8/15", "64QAM"), ("10/15", "256QAM"))
@@ -179,6 +181,71 @@ def summary(rows, target=1e-4):
     return None
 
 
+def compare_decoders(rate, mod, esn0, nblk, weights_path=None, n=64800,
+                     seed=99, chunk=2000, iters=50, alpha=0.75):
+    """Mean iterations of four decoders on the same held-out seeded AWGN
+    blocks at one Es/N0 (the blocks ``sweep`` draws at that point): the plain
+    flooding min-sum, the learned flooding min-sum, the layered min-sum
+    (Type B codes) and the float64 log-tanh sum-product flooding decoder
+    (the exact message update a scale/offset min-sum approximates).
+    Iterations count message updates up to the zero syndrome (the
+    sum-product count is the update after which its syndrome vanished, the
+    same count).  A block error is a wrong information bit or no zero
+    syndrome within ``iters``."""
+    torch = _torch()
+    tx = synth.Transmitter(n, mod, rate, device="cuda")
+    plan = LDPC.plan_for(rate, n)
+    K = C.kldpc(rate, n)
+    if weights_path is None:
+        weights_path = os.path.join(
+            HERE, "data", f"weights_fast_{rate.replace('/', '_')}_{mod}.pt")
+    al, be, _ = LR.load_weights(weights_path)
+    w = LR.inference_weights(al, be, LR.WmsCode(rate, n).buckets)
+    try:
+        lplan = LDPC.LayeredPlan(rate, n)
+    except (ValueError, N.FecError):
+        lplan = None
+    sptab = LDPC.sp_tables(C.csr(rate, n), n)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed + int(round(esn0 * 10)))
+    acc = {}
+
+    def add(name, o, cw, ms):
+        wrong = (o["bits"][:, :K] != cw[:, :K]).any(dim=1) | (o["conv"] == 0)
+        a = acc.setdefault(name, [0, 0, 0.0])
+        a[0] += int(wrong.sum())
+        a[1] += int(o["its"].sum())
+        a[2] += ms
+
+    for lo in range(0, nblk, chunk):
+        lam, cw = blocks(tx, gen, min(chunk, nblk - lo), esn0)
+        runs = [("plain flooding min-sum",
+                 lambda: LDPC.decode_flood(plan, lam, iters=iters, alpha=alpha)),
+                ("learned flooding min-sum",
+                 lambda: LDPC.decode_flood(plan, lam, iters=iters, alpha=alpha,
+                                           weights=w)),
+                ("float64 sum-product flooding",
+                 lambda: LDPC.sp_decode(sptab, lam.double(), iters=iters))]
+        if lplan is not None:
+            runs.append(("plain layered min-sum",
+                         lambda: LDPC.decode_layered(lplan, lam, iters=iters,
+                                                     alpha=alpha)))
+        for name, fn in runs:
+            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            e0.record()
+            o = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            add(name, o, cw, e0.elapsed_time(e1))
+        if lplan is not None:
+            LDPC.check_layered_error(lplan)
+    return {"rate": rate, "mod": mod, "n": n, "esn0_db": esn0, "blocks": nblk,
+            "channel": "awgn", "weights": os.path.basename(weights_path),
+            "decoders": {k: {"block_errors": er, "mean_iters": it / nblk,
+                             "gpu_ms": round(ms, 1)}
+                         for k, (er, it, ms) in acc.items()}}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
@@ -193,7 +260,18 @@ def main(argv=None):
     ap.add_argument("--tag", default="", help="weights file infix")
     ap.add_argument("--depths", type=int, nargs="*", default=None,
                     help="average the output BCE over these unrolled depths")
+    ap.add_argument("--compare", nargs=3, metavar=("RATE", "MOD", "ESN0"),
+                    default=None,
+                    help="only compare the mean iterations of the plain, learned, "
+                         "layered and sum-product decoders at one Es/N0 on "
+                         "--blocks held-out blocks")
+    ap.add_argument("--weights", default=None, help="weights file for --compare")
     a = ap.parse_args(argv)
+    if a.compare:
+        rate, mod, e = a.compare
+        print(json.dumps(compare_decoders(rate, mod, float(e), a.blocks,
+                                          weights_path=a.weights)), flush=True)
+        return
     print(json.dumps(run(a.steps, a.batch, a.blocks, a.points, a.out,
                          iters=a.iters, window=tuple(a.window), tag=a.tag,
                          depths=a.depths)),
