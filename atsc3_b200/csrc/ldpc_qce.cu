@@ -907,6 +907,17 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const int c0 = a.ci[rank], ncitems = a.ci[rank + 1] - c0;
   const int r0 = c0 / ECHUNK;
   const int nr = ncitems > 0 ? (c0 + ncitems + ECHUNK - 1) / ECHUNK - r0 : 0;
+  // the check items run as: chunks 0 .. ECHUNK-2 of these rows in row order
+  // (nlead of them, from chunk coff of row r0), then the rows' last chunks
+  // (TAILW checks each; the rows whose last chunk is this CTA's) packed
+  // TAILG to a warp, lane group g taking tail t = TAILG * item + g
+  constexpr int TAILW = EZ - 32 * (ECHUNK - 1);
+  constexpr int TAILG = 32 / TAILW;
+  static_assert(TAILW > 0 && 32 % TAILW == 0, "tail chunk must divide a warp");
+  const int coff = c0 - r0 * ECHUNK;
+  const int ntail = max(0, min(nr, (c0 + ncitems) / ECHUNK - r0));
+  const int nlead = ncitems - ntail;
+  const int ncpk = nlead + (ntail + TAILG - 1) / TAILG;
   const int i0 = a.ib[rank], nvitems = a.ib[rank + 1] - i0;
   // heavy rows are compiled into the Type A kernels of 6 and 8 slots (the
   // builder refuses them with 4)
@@ -1029,7 +1040,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       // (the parts path is float32 only; float64 plans keep one warp per item)
       const bool split = HV && sizeof(V) == 4 && a.nhrows && a.hsplit > 1;
       const int nhp = (HV && a.nhrows) ? (split ? nhi * a.hsplit : nhi) : 0;
-      for (int w = warp; w < nhp + ncitems; w += nwarps) {
+      for (int w = warp; w < nhp + ncpk; w += nwarps) {
         int syn;
         if (HV && w < nhp && !split) {             // one warp per heavy item
           const int hi = __ldg(a.hitems + h0 + w);
@@ -1051,27 +1062,41 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
               make_float4(r.min1, r.min2, __int_as_float(r.first), __uint_as_float(r.bits));
           continue;
         }
-        const int gi = c0 + (w - nhp);
-        const int row = gi / ECHUNK;
-        const int ch = gi - row * ECHUNK;
-        const int rl = row - r0;
-        const MASK wm = rinfo[3 * rl + 1];
-        const int deg = (int)rinfo[3 * rl + 2];
-        const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
-        const bool full = wm == 0 && ch < ECHUNK - 1;
-        if (full && deg == NS) {
-          syn = qce_check_item<V, TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
-        } else if (full && deg == NS - 1) {
-          syn = qce_check_item<V, TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy, upd, a, it);
-        } else {
-          const int k0 = ch * 32 + lane;
-          MASK live = rinfo[3 * rl];
-          if (k0 == 0) live &= ~wm;                  // check (0, 0): no wrap edge
-          if (k0 >= EZ) live = 0;                    // lanes past the circulant
-          syn = qce_check_item<V, TORCH, NS, false, MASK>(te, live, lane, bm, dummy, upd, a, it);
-          syn = k0 < EZ ? syn : 0;
+        const int wl = w - nhp;
+        const uint2 *te;
+        MASK live;
+        uint32_t el;                               // the lane's check within its chunk
+        bool valid = true;
+        if (wl < nlead) {                          // chunks 0 .. ECHUNK-2 of a row
+          const int u = wl + coff;
+          const int rl = u / (ECHUNK - 1);
+          const int ch = u - rl * (ECHUNK - 1);
+          const MASK wm = rinfo[3 * rl + 1];
+          const int deg = (int)rinfo[3 * rl + 2];
+          te = rtab + (rl * ECHUNK + ch) * NS;
+          if (wm == 0 && deg == NS) {
+            mybad += qce_check_item<V, TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy,
+                                                              upd, a, it);
+            continue;
+          }
+          if (wm == 0 && deg == NS - 1) {
+            mybad += qce_check_item<V, TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy,
+                                                                  upd, a, it);
+            continue;
+          }
+          live = rinfo[3 * rl];
+          if (ch == 0 && lane == 0) live &= ~wm;     // check (0, 0): no wrap edge
+          el = (uint32_t)lane;
+        } else {                                   // last chunks, TAILG rows a warp
+          const int t = (wl - nlead) * TAILG + lane / TAILW;
+          valid = t < ntail;
+          const int rl = valid ? t : 0;
+          te = rtab + (rl * ECHUNK + ECHUNK - 1) * NS;
+          live = valid ? rinfo[3 * rl] : (MASK)0;
+          el = (uint32_t)(lane % TAILW);
         }
-        mybad += syn;
+        syn = qce_check_item<V, TORCH, NS, false, MASK>(te, live, el, bm, dummy, upd, a, it);
+        mybad += valid ? syn : 0;
       }
       if (split) {
         __syncthreads();

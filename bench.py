@@ -379,10 +379,10 @@ def run_gpu(args, rank, world, local_rank):
                       "store); about half is served by the CTA's own shared "
                       "memory (columns placed with their rows), the rest "
                       "crosses the cluster's xbar",
-              "peak_ncu": 9300.0,
+              "peak_ncu": 9350.0,
               "peak_note": "xbar-to-L1 distributed shared memory bytes at "
-                           "22.9% of peak = 2.13 TB/s (7.55 GB per launch) "
-                           "in the committed ncu capture, i.e. about 9.3 TB/s"}
+                           "23.7% of peak = 2.22 TB/s (7.55 GB per launch) "
+                           "in the committed ncu capture, i.e. about 9.35 TB/s"}
     onchip["frac"] = onchip["achieved"] / onchip["peak_ncu"]
     # instruction issue, the decoder's actual bound (ncu: issue active ~60%,
     # not_selected and math-pipe throttle the leading stalls): warp
@@ -400,7 +400,7 @@ def run_gpu(args, rank, world, local_rank):
         peak = sms * 4 * mhz / 1e3
         issue = {"unit": "G warp instructions/s", "achieved": ach, "peak": peak,
                  "frac": ach / peak, "sms": sms, "instructions_per_launch": instr,
-                 "what": "warp instructions per codeword-iteration (1.871 G over "
+                 "what": "warp instructions per codeword-iteration (1.805 G over "
                          "75 x 50 in the committed ncu capture) x the launch's "
                          "iterations / launch time; peak = 4 schedulers x SM "
                          "clock x the SMs the clusters occupy"}
@@ -455,13 +455,13 @@ KERNEL_NAMES = {"qce": "ldpc_qce_kernel (quasi-cyclic flooding, edge-buffer layo
 
 # DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch:
 # dram__bytes_read.sum + dram__bytes_write.sum of one captured 75-block launch
-# of the edge-buffer decoder (19,549,184 + 0 B) / 75, from
+# of the edge-buffer decoder (19,542,528 + 0 B) / 75, from
 # profiles/ldpc_qce_flood_6_15_frame.md (the record-layout decoder's capture,
 # profiles/ldpc_qc_flood_6_15_frame.md, read 19,553,792 B).
-TRAFFIC_PER_BLOCK = 19_549_184 / 75
+TRAFFIC_PER_BLOCK = 19_542_528 / 75
 # warp instructions per codeword-iteration of ldpc_qce_kernel<0, 8, 1024, 0> on this
-# workload: 1,870,617,663 over 75 blocks x 50 iterations (profiles/ldpc_qce_flood_6_15_frame.md)
-INSTR_PER_BLOCK_ITER = 1_870_617_663 / 3750
+# workload: 1,805,381,535 over 75 blocks x 50 iterations (profiles/ldpc_qce_flood_6_15_frame.md)
+INSTR_PER_BLOCK_ITER = 1_805_381_535 / 3750
 
 
 def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
