@@ -1,7 +1,9 @@
 // ldpc_qce.cu -- flooding normalised min-sum for every quasi-cyclic A/322
 // code (Type B, and Type A with its identity rows) with an EDGE-BUFFER layout
 // (sm_100a), bit-exact with lab/ldpc_kernel.c (kernel semantics) and
-// lab/m9_gpu.py:168-211 (torch semantics), float32.
+// lab/m9_gpu.py:168-211 (torch semantics), float32; the same source, templated on
+// the value type, also builds a float64 decoder (8-byte slots, no learned
+// weights).
 //
 // The code structure used is the one of ldpc_qc.cu (360x360 circulants,
 // dual-diagonal parity part, edge order inside a check = block-column order,
@@ -25,7 +27,9 @@
 // The check phase therefore reads each edge's q with one 4-byte remote load
 // (32 consecutive checks of a block row read 32 consecutive entries of a
 // circulant slot), forms min1/min2/first/signs in registers, and writes the
-// messages back into the same slots with posted remote stores.  The variable
+// messages back into the same slots with posted remote stores.  A row's 360
+// checks are 11 such warp items and an 8-check last chunk; a CTA's last
+// chunks run four rows to a warp (8 lanes per row).  The variable
 // phase is local: it sums its slots in the reference order, forms tot, and
 // rewrites every slot as tot - m.  No per-check records are kept.
 //
@@ -36,7 +40,8 @@
 // the cluster; the check phase looks up its bits locally.
 //
 // Shared memory per CTA: bitmap (nb*48 B) | syndrome exchange (256 B) |
-// per-launch tables | the edge slots of the CTA's columns (1440 B per slot).
+// per-launch tables | the edge slots of the CTA's columns (1440 B per slot;
+// 2880 B in the float64 build).
 // For the 64800-bit codes (about 281k edges, 1.1 MB of slots) a 6-CTA
 // cluster holds a codeword (about 215 KB per CTA).
 
