@@ -1089,6 +1089,13 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
                                                                   upd, a, it);
             continue;
           }
+          if constexpr (NS >= 10) {                // rows two short of the template
+            if (wm == 0 && deg == NS - 2) {
+              mybad += qce_check_item<V, TORCH, NS - 2, true, MASK>(te, (MASK)0, lane, bm,
+                                                                    dummy, upd, a, it);
+              continue;
+            }
+          }
           live = rinfo[3 * rl];
           if (ch == 0 && lane == 0) live &= ~wm;     // check (0, 0): no wrap edge
           el = (uint32_t)lane;
