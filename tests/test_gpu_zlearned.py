@@ -25,3 +25,22 @@ def test_training_lowers_loss_and_iterations():
     # fewer iterations at no worse block error rate
     assert l["mean_iters"] < p["mean_iters"]
     assert l["block_errors"] <= p["block_errors"] + 2
+
+
+def test_compare_decoders_same_blocks():
+    """The four-decoder comparison at the 6/15 16-NUC operating point on a
+    small held-out set: the learned and the exact sum-product flooding
+    decoders need fewer iterations than plain min-sum, the layered schedule
+    fewer still, and the learned and sum-product decoders leave no block
+    without a zero syndrome."""
+    from atsc3_b200 import evaluate as EV
+    r = EV.compare_decoders("6/15", "16QAM", 8.25, 200, chunk=200)
+    d = r["decoders"]
+    assert set(d) == {"plain flooding min-sum", "learned flooding min-sum",
+                      "float64 sum-product flooding", "plain layered min-sum"}
+    plain = d["plain flooding min-sum"]["mean_iters"]
+    assert d["learned flooding min-sum"]["mean_iters"] < plain
+    assert d["float64 sum-product flooding"]["mean_iters"] < plain
+    assert d["plain layered min-sum"]["mean_iters"] < d["learned flooding min-sum"]["mean_iters"]
+    assert d["learned flooding min-sum"]["block_errors"] == 0
+    assert d["float64 sum-product flooding"]["block_errors"] == 0
