@@ -344,6 +344,9 @@ def run_gpu(args, rank, world, local_rank):
     if w is not None:
         louts = [new_out() for _ in range(K)]
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+            torch.cuda.synchronize()
         e0.record(main)
         for st in streams:
             st.wait_event(e0)
@@ -357,6 +360,8 @@ def run_gpu(args, rank, world, local_rank):
         e1.record(main)
         torch.cuda.synchronize()
         lms = e0.elapsed_time(e1)
+        if world > 1:
+            lms = shard.max_over_ranks(lms, device=dev)
         lits = torch.stack([o["its"] for o in louts]).cpu().numpy()
         lok = torch.stack([o["ok"] for o in louts]).cpu().numpy()
         learned = {"value": world * K * nblk * kp / (lms / 1e3) / 1e6,
@@ -500,6 +505,10 @@ def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
     for s in range(2 * S):   # warm the pinned path
         step(s % K)
     torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     ends = [torch.cuda.Event() for _ in range(S)]
@@ -514,6 +523,9 @@ def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
     e1.record(main)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    if world > 1:                      # the slowest rank's time, as for `value`
+        from atsc3_b200 import shard
+        ms = shard.max_over_ranks(ms, device=dev)
     h2d = nblk * pipes[0].ncell * (8 + 4)
     d2h = nblk * (kp // 8) + 4 * nblk * 4
     return {"value": world * K * nblk * kp / (ms / 1e3) / 1e6, "unit": "Mbit/s",
