@@ -94,6 +94,106 @@ __global__ void __launch_bounds__(256) row_sigma_kernel(
   }
 }
 
+// ---- float64: the drop-in for the reference's default float64
+// demap_llr_fast (lab/m16_demap_fast.py:80-119; m = |p|^2 - 2 Re(y p*), the
+// per-bit minima, / sigma2).  Same work split, double arithmetic, cells as
+// double2 (complex128), output in q order or through lam_of_q.
+template <int NB>
+__global__ void __launch_bounds__(256) demap_f64_kernel(
+    const double2 *__restrict__ cells, int64_t ld_cells, int nblk, int ncell,
+    const double *__restrict__ pts, int sigma_mode,
+    const double *__restrict__ sigma2, int64_t ld_sigma, double s2scalar,
+    const int32_t *__restrict__ lam_of_q, double *__restrict__ out,
+    int64_t ld_out) {
+  using A = DemapArith<double>;
+  constexpr int M = 1 << NB;
+  extern __shared__ double spd[];
+  double *spr = spd, *spi = spd + M, *sp2 = spd + 2 * M;
+  for (int k = threadIdx.x; k < 3 * M; k += blockDim.x) spd[k] = pts[k];
+  __syncthreads();
+  const int64_t total = (int64_t)nblk * ncell;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int b = (int)(g / ncell);
+    const int s = (int)(g - (int64_t)b * ncell);
+    const double2 z = cells[(size_t)b * ld_cells + s];
+    double mn[NB][2];
+    cell_minima<NB, double>(z.x, z.y, spr, spi, sp2, mn, nullptr);
+    double s2 = s2scalar;
+    if (sigma_mode == 1) s2 = sigma2[(size_t)b * ld_sigma + s];
+    else if (sigma_mode == 2) s2 = sigma2[b];
+    double *o = out + (size_t)b * ld_out;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      const double d = A::div(A::sub(mn[i][1], mn[i][0]), s2);
+      const int q = s * NB + i;
+      o[lam_of_q ? __ldg(lam_of_q + q) : q] = d;
+    }
+  }
+}
+
+// sigma2[b] = max(mean_s(|z|^2 + min_k q_k), 1e-9) in float64 (the estimate
+// of lab/m16_demap_fast.py:104-106).
+template <int NB>
+__global__ void __launch_bounds__(256) row_sigma_f64_kernel(
+    const double2 *__restrict__ cells, int64_t ld_cells, int ncell,
+    const double *__restrict__ pts, double *__restrict__ sigma2) {
+  using A = DemapArith<double>;
+  constexpr int M = 1 << NB;
+  extern __shared__ double spd[];
+  __shared__ double red[32];
+  double *spr = spd, *spi = spd + M, *sp2 = spd + 2 * M;
+  for (int k = threadIdx.x; k < 3 * M; k += blockDim.x) spd[k] = pts[k];
+  __syncthreads();
+  const int b = blockIdx.x;
+  double acc = 0.0;
+  for (int s = threadIdx.x; s < ncell; s += blockDim.x) {
+    const double2 z = cells[(size_t)b * ld_cells + s];
+    double mn[NB][2], qmin;
+    cell_minima<NB, double>(z.x, z.y, spr, spi, sp2, mn, &qmin);
+    const double z2 = A::add(A::mul(z.x, z.x), A::mul(z.y, z.y));
+    acc += A::add(z2, qmin);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    sigma2[b] = fmax(t / (double)ncell, 1e-9);
+  }
+}
+
+typedef void (*DemapF64Fn)(const double2 *, int64_t, int, int, const double *,
+                           int, const double *, int64_t, double,
+                           const int32_t *, double *, int64_t);
+typedef void (*SigmaF64Fn)(const double2 *, int64_t, int, const double *,
+                           double *);
+
+static DemapF64Fn demap_f64_fn(int nb) {
+  switch (nb) {
+    case 2: return demap_f64_kernel<2>;
+    case 4: return demap_f64_kernel<4>;
+    case 6: return demap_f64_kernel<6>;
+    case 8: return demap_f64_kernel<8>;
+    case 10: return demap_f64_kernel<10>;
+    case 12: return demap_f64_kernel<12>;
+  }
+  return nullptr;
+}
+
+static SigmaF64Fn sigma_f64_fn(int nb) {
+  switch (nb) {
+    case 2: return row_sigma_f64_kernel<2>;
+    case 4: return row_sigma_f64_kernel<4>;
+    case 6: return row_sigma_f64_kernel<6>;
+    case 8: return row_sigma_f64_kernel<8>;
+    case 10: return row_sigma_f64_kernel<10>;
+    case 12: return row_sigma_f64_kernel<12>;
+  }
+  return nullptr;
+}
+
 typedef void (*DemapFn)(const float2 *, int64_t, int, int, const float *, int,
                         const float *, int64_t, float, const int32_t *,
                         float *, int64_t);
@@ -164,6 +264,61 @@ int32_t demap_launch(const float *cells, int64_t ld_cells, int nblk, int ncell,
                                         ncell, pts, sigma_mode, sigma2,
                                         ld_sigma, s2scalar, lam_of_q, out,
                                         ld_out);
+  ATSC3_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int32_t demap_f64_launch(const double *cells, int64_t ld_cells, int nblk,
+                         int ncell, const double *pts, int nbits,
+                         int sigma_mode, const double *sigma2,
+                         int64_t ld_sigma, double s2scalar,
+                         const int32_t *lam_of_q, double *out, int64_t ld_out,
+                         cudaStream_t st) {
+  ATSC3_ARG(nblk >= 0 && ncell >= 0, "negative size");
+  ATSC3_ARG(sigma_mode >= 0 && sigma_mode <= 2, "sigma_mode must be 0..2");
+  DemapF64Fn fn = demap_f64_fn(nbits);
+  ATSC3_ARG(fn != nullptr, "nbits must be 2, 4, 6, 8, 10 or 12");
+  if (nblk == 0 || ncell == 0) return 0;
+  ATSC3_ARG(cells && pts && out, "null pointer");
+  ATSC3_ARG(ld_cells >= ncell, "ld_cells < ncell");
+  ATSC3_ARG(ld_out >= (int64_t)ncell * nbits, "ld_out < ncell*nbits");
+  ATSC3_ARG(((uintptr_t)cells & 15) == 0, "cells must be 16-byte aligned");
+  ATSC3_ARG(sigma_mode == 0 || sigma2 != nullptr, "sigma2 array required");
+  ATSC3_ARG(sigma_mode != 1 || ld_sigma >= ncell, "ld_sigma < ncell");
+  const int smem = 3 * (1 << nbits) * 8;
+  if (smem > 48 * 1024)
+    ATSC3_CUDA(cudaFuncSetAttribute((const void *)fn,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+  const int64_t total = (int64_t)nblk * ncell;
+  int64_t grid = (total + 255) / 256;
+  const int64_t cap = (int64_t)num_sms() * 8;
+  if (grid > cap) grid = cap;
+  fn<<<(unsigned)grid, 256, smem, st>>>((const double2 *)cells, ld_cells, nblk,
+                                        ncell, pts, sigma_mode, sigma2,
+                                        ld_sigma, s2scalar, lam_of_q, out,
+                                        ld_out);
+  ATSC3_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int32_t row_sigma_f64_launch(const double *cells, int64_t ld_cells, int nblk,
+                             int ncell, const double *pts, int nbits,
+                             double *sigma2, cudaStream_t st) {
+  SigmaF64Fn fn = sigma_f64_fn(nbits);
+  ATSC3_ARG(fn != nullptr, "nbits must be 2, 4, 6, 8, 10 or 12");
+  ATSC3_ARG(nblk >= 0 && ncell > 0, "bad size");
+  if (nblk == 0) return 0;
+  ATSC3_ARG(cells && pts && sigma2, "null pointer");
+  ATSC3_ARG(ld_cells >= ncell, "ld_cells < ncell");
+  ATSC3_ARG(((uintptr_t)cells & 15) == 0, "cells must be 16-byte aligned");
+  const int smem = 3 * (1 << nbits) * 8;
+  if (smem > 48 * 1024)
+    ATSC3_CUDA(cudaFuncSetAttribute((const void *)fn,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+  fn<<<nblk, 256, smem, st>>>((const double2 *)cells, ld_cells, ncell, pts,
+                              sigma2);
   ATSC3_CUDA(cudaGetLastError());
   return 0;
 }
@@ -282,6 +437,25 @@ int32_t atsc3_demap(const float *cells, int64_t ld_cells, int32_t nblk,
   return atsc3::demap_launch(cells, ld_cells, nblk, ncell, pts, nbits,
                              sigma_mode, sigma2, ld_sigma, sigma2_scalar,
                              lam_of_q, out, ld_out, (cudaStream_t)stream);
+}
+
+int32_t atsc3_demap_f64(const double *cells, int64_t ld_cells, int32_t nblk,
+                        int32_t ncell, const double *pts, int32_t nbits,
+                        int32_t sigma_mode, const double *sigma2,
+                        int64_t ld_sigma, double sigma2_scalar,
+                        const int32_t *lam_of_q, double *out, int64_t ld_out,
+                        void *stream) {
+  return atsc3::demap_f64_launch(cells, ld_cells, nblk, ncell, pts, nbits,
+                                 sigma_mode, sigma2, ld_sigma, sigma2_scalar,
+                                 lam_of_q, out, ld_out, (cudaStream_t)stream);
+}
+
+int32_t atsc3_demap_row_sigma2_f64(const double *cells, int64_t ld_cells,
+                                   int32_t nblk, int32_t ncell,
+                                   const double *pts, int32_t nbits,
+                                   double *sigma2, void *stream) {
+  return atsc3::row_sigma_f64_launch(cells, ld_cells, nblk, ncell, pts, nbits,
+                                     sigma2, (cudaStream_t)stream);
 }
 
 int32_t atsc3_demap_row_sigma2(const float *cells, int64_t ld_cells,

@@ -23,11 +23,13 @@
 // coalesced stores.  A packed hard-decision bitmap of the whole codeword is
 // kept in shared memory and refreshed at each write-back, so the per-
 // iteration syndrome is a shared-memory gather.  Waits on the mbarrier are
-// bounded: on timeout the kernel records an error and stops.
+// bounded: on timeout the kernel waits once more for its copies, records an
+// error (1, or 2 when the second wait ran out too) and stops.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <unordered_map>
@@ -66,6 +68,7 @@ struct LayArgs {
   int32_t *its;
   int32_t *bad;
   int32_t *err;
+  int fail_layer;    // test hook: take the timeout path at this layer, or -1
 };
 
 __device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
@@ -188,15 +191,23 @@ __global__ void __launch_bounds__(LTHREADS, 2) ldpc_layered_kernel(const LayArgs
         }
         uint4 ro = make_uint4(0u, 0u, 0u, 0u);
         if (act && it > 0) ro = R[(size_t)r * LZ + k];
-        const bool ok = mbar_wait_bounded(mb, phase);
+        bool ok = mbar_wait_bounded(mb, phase);
+        // test hook: behave as if this (completed) wait had run out, so the
+        // error path runs with no copy in flight
+        if (it * a.Q + r == a.fail_layer) ok = false;
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
-          // copies may still be in flight: give them one more bounded wait
+          // A wait ran out.  Copies may still be landing in this CTA's
+          // shared memory: wait for the same phase once more (bounded).
+          // *err = 1: the copies then completed and the CTA returned with
+          // nothing in flight; *err = 2: the second wait ran out as well,
+          // so copies may still have been in flight when the CTA returned
+          // (the launch's outputs are void and the context is suspect).
+          const bool drained = mbar_wait_bounded(mb, phase ^ 1u);
           if (tid == 0) {
             s_fail = 1;
-            atomicExch(a.err, 1);
+            atomicMax(a.err, drained ? 1 : 2);
           }
-          mbar_wait_bounded(mb, phase ^ 1u);
           return;
         }
         if (act) {
@@ -306,6 +317,10 @@ static int dr_bucket(int dr) {
 struct atsc3_ldpc_layered_plan {
   atsc3::LayPlan p;
 };
+
+namespace atsc3 {
+static std::atomic<int> g_lay_fail_layer{-1};
+}  // namespace atsc3
 
 extern "C" {
 
@@ -437,9 +452,16 @@ int32_t atsc3_ldpc_layered_decode(const atsc3_ldpc_layered_plan *h,
   a.its = its;
   a.bad = bad;
   a.err = err;
+  a.fail_layer = g_lay_fail_layer.exchange(-1);
   const int grid = std::min(ctas, nblk);
   fn<<<grid, LTHREADS, smem, (cudaStream_t)stream>>>(a);
   ATSC3_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int32_t atsc3_ldpc_layered_inject_timeout(int32_t layer) {
+  ATSC3_ARG(layer >= -1, "layer must be >= -1");
+  atsc3::g_lay_fail_layer.store(layer);
   return 0;
 }
 

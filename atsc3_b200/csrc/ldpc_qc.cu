@@ -803,3 +803,9 @@ int32_t atsc3_ldpc_qc_decode_weighted(
 }
 
 }  // extern "C"
+
+namespace atsc3 {
+// Device the plan's tables were built on (internal; used by the
+// allocation-free entry point to refuse a plan from another GPU).
+int qc_plan_device(const atsc3_ldpc_qc_plan *h) { return h->p.device; }
+}  // namespace atsc3

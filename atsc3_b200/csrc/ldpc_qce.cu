@@ -1883,3 +1883,9 @@ int32_t atsc3_ldpc_qce_decode(const atsc3_ldpc_qce_plan *h, const float *llr,
 }
 
 }  // extern "C"
+
+namespace atsc3 {
+// Device the plan's tables were built on (internal; used by the
+// allocation-free entry point to refuse a plan from another GPU).
+int qce_plan_device(const atsc3_ldpc_qce_plan *h) { return h->p.device; }
+}  // namespace atsc3

@@ -21,7 +21,10 @@
 //    before any stream capture;
 //  * all calls share the one scratch: calls that overlap on the GPU (other
 //    streams, other threads) race and corrupt each other -- serialise them;
-//  * every call writes all the scratch it reads, so nothing needs clearing;
+//  * every call writes all the scratch it reads, so nothing needs clearing
+//    (kldpc <= ncell*nbits is enforced so BCH never reads past what the LDPC
+//    step wrote);
+//  * the plan must have been built on the current device (-3 otherwise);
 //  * the LDPC plan is created beforehand (atsc3_ldpc_qce_plan_create /
 //    _create2, atsc3_ldpc_qc_plan_create or atsc3_ldpc_plan_create, at
 //    set-up; float32 plans); this entry point itself calls no allocator.
@@ -60,6 +63,9 @@ int32_t bch_check_launch(const uint8_t *hard, int64_t ld_hard, int nblk,
                          uint8_t *ok, const uint8_t *scr, int kpay,
                          uint8_t *payload, int64_t ld_payload,
                          cudaStream_t st);
+
+int qce_plan_device(const atsc3_ldpc_qce_plan *h);
+int qc_plan_device(const atsc3_ldpc_qc_plan *h);
 
 namespace {
 constexpr int kMaxDevices = 64;
@@ -112,8 +118,14 @@ extern "C" int32_t atsc3_fec_decode_noalloc(
               "split the batch");
     return -3;
   }
+  // BCH reads the first kldpc hard decisions of each scratch row, and the
+  // LDPC step writes only the first n of them: a longer kldpc would read
+  // bits another call left behind.
+  ATSC3_ARG(kldpc > 0 && kldpc <= n, "kldpc must be in 1..ncell*nbits");
+  ATSC3_ARG(kpayload >= 0 && kpayload <= kldpc, "kpayload must be in 0..kldpc");
   if (nblk == 0) return 0;
   ATSC3_ARG(lam_of_q != nullptr, "lam_of_q required (codeword order)");
+  int plan_dev = 0;
   if (plan_kind == 1 || plan_kind == 2) {
     int64_t info[10];
     int32_t rc0 = plan_kind == 1
@@ -121,10 +133,20 @@ extern "C" int32_t atsc3_fec_decode_noalloc(
         : atsc3_ldpc_qce_plan_info((const atsc3_ldpc_qce_plan *)plan, info);
     if (rc0) return rc0;
     ATSC3_ARG(info[0] == n, "ncell*nbits differs from the plan's codeword length");
+    plan_dev = plan_kind == 1
+        ? qc_plan_device((const atsc3_ldpc_qc_plan *)plan)
+        : qce_plan_device((const atsc3_ldpc_qce_plan *)plan);
   } else {
     ATSC3_ARG(((const atsc3_ldpc_plan *)plan)->n == n,
               "ncell*nbits differs from the plan's codeword length");
+    plan_dev = ((const atsc3_ldpc_plan *)plan)->device;
   }
+  // the scratch is per device: the plan's tables and the scratch must be on
+  // the same (current) GPU
+  int cur_dev = 0;
+  ATSC3_CUDA(cudaGetDevice(&cur_dev));
+  ATSC3_ARG(plan_dev == cur_dev,
+            "the plan was built on another device than the current one");
   float *llr = nullptr;
   uint8_t *hard = nullptr;
   int32_t rc = scratch_for_current_device(&llr, &hard);

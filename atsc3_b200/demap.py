@@ -120,13 +120,77 @@ def demap(cells, mod, rate, sigma2=None, n=None, deinterleave=True, out=None,
     return out
 
 
+@functools.lru_cache(maxsize=None)
+def _host_points_f64(mod, rate):
+    # |p|^2 as lab/m16_demap_fast.py:103 forms it: np.abs(pts) ** 2
+    pts = np.asarray(C.alphabet(mod, rate), np.complex128)
+    return np.concatenate([pts.real, pts.imag, np.abs(pts) ** 2])
+
+
+def demap_f64(cells, mod, rate, sigma2=None, n=None, deinterleave=False,
+              out=None, stream=None):
+    """Float64 demapper: (nblk, ncell) complex128 CUDA cells -> float64
+    LLRs, the double-precision arithmetic of the reference's default
+    ``demap_llr_fast`` (lab/m16_demap_fast.py:80-119).  sigma2: None
+    (per-row float64 estimate), a float, or a (nblk, ncell) tensor."""
+    torch = _torch()
+    if cells.dim() == 1:
+        cells = cells[None]
+    if cells.device.type != "cuda" or cells.dtype != torch.complex128:
+        raise TypeError("cells must be a complex128 CUDA tensor")
+    cells = cells.resolve_conj().contiguous()
+    nblk, ncell = cells.shape
+    nb = C.MOD_BITS[mod]
+    dev = cells.device
+    key = ("pts64", mod, rate, str(dev))
+    pts = _DEV.get(key)
+    if pts is None:
+        pts = _DEV[key] = torch.from_numpy(_host_points_f64(mod, rate)).to(dev)
+    zf = torch.view_as_real(cells)
+    lq = None
+    if deinterleave:
+        n = n or ncell * nb
+        lq = device_lam_of_q(n, mod, rate, dev)
+    if out is None:
+        out = torch.empty((nblk, ncell * nb), dtype=torch.float64, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    s2t, s2s, ld_s = None, 0.0, 0
+    if sigma2 is None:
+        s2t = torch.empty(nblk, dtype=torch.float64, device=dev)
+        N.call("atsc3_demap_row_sigma2_f64", zf.data_ptr(), zf.stride(0) // 2,
+               nblk, ncell, pts.data_ptr(), nb, s2t.data_ptr(), st)
+        mode = 2
+    elif isinstance(sigma2, (float, int, np.floating)):
+        mode, s2s = 0, float(sigma2)
+    else:
+        s2t = sigma2.to(device=dev, dtype=torch.float64).reshape(nblk, ncell)
+        s2t = s2t.contiguous()
+        mode, ld_s = 1, s2t.stride(0)
+    N.call("atsc3_demap_f64", zf.data_ptr(), zf.stride(0) // 2, nblk, ncell,
+           pts.data_ptr(), nb, mode, N.ptr(s2t), ld_s, s2s, N.ptr(lq),
+           out.data_ptr(), out.stride(0), st)
+    return out
+
+
 def demap_llr_fast(cells, mod, rate, sigma2=None, dtype=np.float64, ex=None,
                    chunk=20_000):
     """Drop-in for ``m16_demap_fast.demap_llr_fast``: one row of cells ->
-    float64 (ncell*nbits,) LLRs in q order.  ``dtype``, ``ex`` and ``chunk``
-    are accepted for signature compatibility; the GPU computes in float32.
-    ``sigma2`` may also be a per-cell array (divided after the minima)."""
+    float64 (ncell*nbits,) LLRs in q order.  ``dtype`` picks the GPU
+    arithmetic as it picks the reference's: float64 (the default) runs the
+    float64 demapper, float32 the float32 one (the lab/m44_ldm.py:2431-2451
+    operation order).  ``ex`` and ``chunk`` are accepted for signature
+    compatibility.  ``sigma2`` may also be a per-cell array (divided after
+    the minima)."""
     torch = _torch()
+    if np.dtype(dtype) == np.float64:
+        z = np.ascontiguousarray(np.asarray(cells), np.complex128).reshape(1, -1)
+        s2 = sigma2
+        if sigma2 is not None and np.ndim(sigma2) > 0:
+            s2 = torch.from_numpy(np.asarray(sigma2, np.float64).reshape(1, -1)).cuda()
+        elif sigma2 is not None:
+            s2 = float(sigma2)
+        q = demap_f64(torch.from_numpy(z).cuda(), mod, rate, sigma2=s2)
+        return q.cpu().numpy().ravel()
     z = np.ascontiguousarray(np.asarray(cells), np.complex64).reshape(1, -1)
     t = torch.from_numpy(z).cuda()
     s2 = sigma2

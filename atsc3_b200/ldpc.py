@@ -434,11 +434,19 @@ def decode_layered(plan, llr, iters=50, alpha=0.75, want_bits=True,
 
 
 def check_layered_error(plan):
-    """Raise if a layered launch recorded a copy timeout (syncs)."""
-    if int(plan.err.item()) != 0:
+    """Raise if a layered launch recorded a copy timeout (syncs).  Code 1:
+    a wait ran out and the CTA returned after its copies completed; code 2:
+    the second wait ran out as well, so copies may have been in flight when
+    the CTA returned."""
+    code = int(plan.err.item())
+    if code != 0:
         plan.err.zero_()
+        what = ("a staged copy did not complete in time (bounded wait); the "
+                "CTA returned after its copies landed" if code == 1 else
+                "a staged copy did not complete within two bounded waits; "
+                "copies may have been in flight when the CTA returned")
         raise N.FecError("atsc3_ldpc_layered_decode", -2,
-                         "a staged copy did not complete (bounded wait)")
+                         f"{what} (error code {code})")
 
 
 # ---------------------------------------------------------------------------

@@ -99,6 +99,7 @@ SIGNATURES = {
                                           c_f32, c_vp, c_i64, c_vp, c_i64,
                                           c_vp, c_vp, c_vp, c_vp, c_i32, c_vp,
                                           c_vp]),
+    "atsc3_ldpc_layered_inject_timeout": (c_i32, [c_i32]),
     "atsc3_wms_forward": (c_i32, [c_vp] * 7 + [c_i32] * 6 + [c_vp, c_vp, c_vp,
                                                              c_i32, c_vp, c_vp,
                                                              c_vp]),
@@ -123,6 +124,10 @@ SIGNATURES = {
                                    c_vp, c_f32, c_vp, c_vp, c_i64, c_vp]),
     "atsc3_demap_row_sigma2": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,
                                        c_i32, c_vp, c_vp]),
+    "atsc3_demap_f64": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_i32, c_i32,
+                                c_vp, c_i64, c_f64, c_vp, c_vp, c_i64, c_vp]),
+    "atsc3_demap_row_sigma2_f64": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,
+                                           c_i32, c_vp, c_vp]),
     "atsc3_bch_check": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp, c_vp, c_vp,
                                 c_vp, c_i32, c_vp, c_i64, c_vp]),
     "atsc3_bch_syndrome_bits": (c_i32, [c_vp, c_i64, c_i32, c_i32, c_vp,

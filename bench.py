@@ -134,12 +134,15 @@ def make_frames(nframes, seed, device):
     return cells, sig, nblk, tx.kp
 
 
-def cpu_reference_decode(cells, sig, threads, mod=None, rate=None, n=None):
-    """The reference's CPU path on host cores: float32 demap (numpy, the
-    lab/m44_ldm.py:2431-2494 arithmetic) with per-cell sigma2, de-interleave,
-    the reference's compiled lab/ldpc_kernel.c (thread sub-batches, as
-    lab/m44_ldm.py:2558-2576), BCH as a packed GF(2) product
-    (lab/m9_accel.py:212-236).  Returns (#blocks BCH-clean, its)."""
+def cpu_reference_decode(cells, sig, threads, mod=None, rate=None, n=None,
+                         full=False):
+    """The reference's CPU path on host cores, through the oracle: float32
+    demap (numpy, the lab/m44_ldm.py:2431-2494 arithmetic) with per-cell
+    sigma2, de-interleave, the reference's own lab/ldpc_kernel.c compiled
+    into oracle/_ref (thread sub-batches, as lab/m44_ldm.py:2558-2576), BCH
+    as a packed GF(2) product (lab/m9_accel.py:212-236).  Returns
+    (#blocks BCH-clean, its), or with full=True the dict of every output
+    (bits, conv, its, bad, ok, payload)."""
     import oracle
     from concurrent.futures import ThreadPoolExecutor
     from atsc3_b200 import codes as C
@@ -160,11 +163,114 @@ def cpu_reference_decode(cells, sig, threads, mod=None, rate=None, n=None):
     bits, conv, its, bad = oracle.flood_ref(lam, tabs, n, iters=ITERS,
                                             alpha=ALPHA, threads=threads)
     syn = oracle.bch_syndrome_fast(bits[:, :K], n)
-    return sum(1 for s in syn if s == 0), its
+    if not full:
+        return sum(1 for s in syn if s == 0), its
+    kp = C.kpayload(rate, n)
+    pay = np.packbits(bits[:, :kp] ^ C.scrambler_sequence(kp)[None, :], axis=1)
+    return {"bits": bits, "conv": np.asarray(conv, bool), "its": its,
+            "bad": bad, "ok": np.array([s == 0 for s in syn]),
+            "payload": pay}
+
+
+REF_TREE = os.path.join(HERE, "baseline", "_ref")
+
+
+class ReferenceCpuPath:
+    """The reference receiver's own CPU FEC path, imported from the
+    unmodified copy in baseline/_ref (laid out by `python oracle/build.py
+    --ref-tree`; absent -> RuntimeError):
+
+    * m44_ldm._point_metric (lab/m44_ldm.py:2431-2451), the float32 point
+      metric, and the per-bit minima of demap_batch_qam (:2483-2486), with
+      the raw minima difference divided by the per-cell sigma2 (the
+      lab/m9_fast.py:1096-1115 convention; demap_batch_qam itself only
+      estimates a per-row sigma2);
+    * lam[:, ch.lam_of_q] = q (lab/m44_ldm.py:2363), ch = m6_bicm.PlpChain;
+    * m44_ldm.ldpc_batch (:2497-2555) at the single rung alpha = 0.75: the
+      compiled lab/ldpc_kernel.c over thread sub-batches (SP rescue off);
+    * m9_accel.bch_syndrome_batch (lab/m9_accel.py:212-236) and the
+      descramble + pack of lab/m44_ldm.py:2374-2377.
+    """
+
+    def __init__(self, threads, mod=None, rate=None, n=None):
+        from concurrent.futures import ThreadPoolExecutor
+        lab = os.path.join(REF_TREE, "lab")
+        if not (os.path.exists(os.path.join(lab, "m44_ldm.py")) and
+                os.path.exists(os.path.join(lab, "ldpc_kernel.so"))):
+            raise RuntimeError("baseline/_ref is not laid out "
+                               "(python oracle/build.py --ref-tree)")
+        os.environ.pop("ATSC3_LDM_SP", None)        # SP rescue off (default)
+        os.environ.pop("ATSC3_LDPC_KERNEL", None)   # compiled kernel on
+        for pth in (REF_TREE, lab):
+            if pth not in sys.path:
+                sys.path.insert(0, pth)
+        import m3_ldpc
+        import m4_scrambler
+        import m6_bicm
+        import m9_accel
+        import m44_ldm
+        if m3_ldpc._kernel_lib() is None:
+            raise RuntimeError("the reference's compiled ldpc_kernel.so did "
+                               "not load (its numpy fallback would run)")
+        if m44_ldm.SP_RESCUE:
+            raise RuntimeError("ATSC3_LDM_SP rescue is on")
+        self.M44, self.BCH = m44_ldm, m9_accel
+        mod, rate, n = mod or MOD, rate or RATE, n or N_INNER
+        self.ch = ch = m6_bicm.PlpChain(n, mod, rate, iters=ITERS)
+        pts = m6_bicm.points_for(mod, rate)
+        self.pr = np.asarray(pts.real, np.float32)
+        self.pi = np.asarray(pts.imag, np.float32)
+        self.p2 = (pts.real ** 2 + pts.imag ** 2).astype(np.float32)
+        self.nb = ch.mod_bits
+        self.threads = threads
+        self.ex = ThreadPoolExecutor(threads)
+        self.seq = m4_scrambler.sequence(ch.kpayload)
+        # BCH tables built before any clock starts (lab/m9_accel.py:169-194)
+        m9_accel.bch_syndrome_batch(np.zeros((1, ch.kldpc), np.uint8),
+                                    ch.ninner)
+
+    def _demap(self, cells, sig, out, lo, hi):
+        k, ncell = hi - lo, cells.shape[1]
+        z = cells[lo:hi]
+        zr = np.asarray(z.real, np.float32)
+        zi = np.asarray(z.imag, np.float32)
+        q = self.M44._point_metric(zr.ravel(), zi.ravel(), self.pr, self.pi,
+                                   self.p2)
+        m = q.shape[1]
+        s2 = sig[lo:hi] if np.ndim(sig) else sig
+        for i in range(self.nb):
+            # label bit i (MSB first) splits the m points into 2^i runs of
+            # (m >> i) labels: the first half of each run has the bit 0
+            qb = q.reshape(k, ncell, 1 << i, 2, m >> (i + 1))
+            one = qb[:, :, :, 1, :].min(axis=(2, 3))
+            zero = qb[:, :, :, 0, :].min(axis=(2, 3))
+            out[lo:hi, :, i] = (one - zero) / s2
+
+    def decode(self, cells, sig, chunk=4):
+        """(nblk, ncell) complex64 cells, per-cell float32 sigma2 (or a
+        scalar) -> dict(bits, conv, bad, ok, payload) of numpy arrays."""
+        ch = self.ch
+        nblk, ncell = cells.shape
+        q = np.empty((nblk, ncell, self.nb), np.float32)
+        jobs = [(lo, min(nblk, lo + chunk)) for lo in range(0, nblk, chunk)]
+        list(self.ex.map(lambda j: self._demap(cells, sig, q, *j), jobs))
+        lam = np.empty((nblk, ch.ninner), np.float32)
+        lam[:, ch.lam_of_q] = q.reshape(nblk, -1)
+        bits, conv, bad = self.M44.ldpc_batch(lam, ch, None, ITERS, self.ex,
+                                              self.threads, alpha=ALPHA)
+        nouter = bits[:, :ch.kldpc]
+        syn = self.BCH.bch_syndrome_batch(nouter, ch.ninner)
+        pay = np.packbits(nouter[:, :ch.kpayload] ^ self.seq[None, :], axis=1)
+        return {"bits": bits, "conv": np.asarray(conv, bool), "bad": bad,
+                "ok": np.array([s == 0 for s in syn]), "payload": pay}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference CPU path, rank 0 only."""
+    """--impl reference: the reference's CPU path on the host cores, rank 0
+    only, on the same frames (same seed) as rank 0 of the GPU arm, every
+    step one whole 75-block frame.  The reference receiver's own Python
+    from baseline/_ref (ReferenceCpuPath) when it is laid out, else the
+    oracle route around the reference's compiled kernel (oracle/_ref)."""
     if rank != 0:
         return None
     import torch
@@ -173,36 +279,51 @@ def run_reference(args, rank, world):
     kp = C.kpayload(RATE, N_INNER)
     dev = "cuda" if torch.cuda.is_available() else "cpu"
     nsteps = args.steps + args.warmup
-    per = min(75, max(8, threads))
     cells, sig, nblk, _ = make_frames(nsteps, args.seed, dev)
-    cells = cells[:, :per].cpu().numpy()
-    sig = sig[:, :per].cpu().numpy()
-    times, its_all = [], []
+    cells = cells.cpu().numpy()
+    sig = sig.cpu().numpy()
+    try:
+        path = ReferenceCpuPath(threads)
+        what = (f"the reference receiver's own Python from baseline/_ref: "
+                f"m44_ldm._point_metric + per-bit minima / per-cell sigma2, "
+                f"lam[:, lam_of_q] = q, m44_ldm.ldpc_batch (lab/ldpc_kernel.c "
+                f"compiled -O3 -ffp-contract=off, {threads} thread "
+                f"sub-batches), m9_accel.bch_syndrome_batch, descramble")
+
+        def dec(c, g):
+            return path.decode(c, g)
+    except RuntimeError as e:
+        what = (f"oracle route ({e}): numpy float32 demap, lab/ldpc_kernel.c "
+                f"compiled -O3 -ffp-contract=off over {threads} threads "
+                f"(oracle/_ref), packed BCH")
+
+        def dec(c, g):
+            return cpu_reference_decode(c, g, threads, full=True)
+    times, ok, conv = [], 0, 0
     for s in range(nsteps):
         t0 = time.perf_counter()
-        _, its = cpu_reference_decode(cells[s], sig[s], threads)
+        o = dec(cells[s], sig[s])
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             times.append(dt)
-            its_all.append(its)
+            ok += int(np.sum(o["ok"]))
+            conv += int(np.sum(o["conv"]))
     tot = sum(times)
-    value = args.steps * per * kp / tot / 1e6
+    value = args.steps * nblk * kp / tot / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": value,
             "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": config(per),
+            "config": config(nblk),
             "cpu_baseline": {"value": value, "unit": "Mbit/s",
                              "cores": threads, "kind": "reference",
-                             "sample": f"{per} of the 75 blocks of each step's "
-                                       f"frame; demap numpy f32, "
-                                       f"lab/ldpc_kernel.c compiled -O3 "
-                                       f"-ffp-contract=off over {threads} "
-                                       f"threads, packed BCH"},
+                             "sample": f"every step one whole frame ({nblk} "
+                                       f"blocks, the GPU arm's frames); "
+                                       + what},
             "e2e": {"value": value, "unit": "Mbit/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "mean_iters": float(np.mean(np.concatenate(its_all)))}
+            "bch_ok_blocks": ok, "converged_frac": conv / (args.steps * nblk)}
     return line
 
 
@@ -314,7 +435,7 @@ def run_gpu(args, rank, world, local_rank):
     value = total_bits / (ms / 1e3) / 1e6
     # ---- per-stage device time, one stream, no overlap (roofline) ---------
     nprof = min(K, 9)
-    stage_its = []
+    stage_its, stage_hard, stage_flags = [], [], []
     E = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
          for _ in range(nprof)]
     from atsc3_b200 import bch as BCH, demap as DM, ldpc as LDPC
@@ -333,6 +454,11 @@ def run_gpu(args, rank, world, local_rank):
         BCH.bch_check(ws["hard"], p0.kldpc, N_INNER, kp, out=o)
         E[s][3].record(main)
         stage_its.append(int(o["its"].sum()))
+        # kept for the parity check: the full hard decisions of this frame
+        # and its flags from this second, untimed decode
+        stage_hard.append(ws["hard"][:, :N_INNER // 8].clone())
+        stage_flags.append(torch.stack([o["conv"].int(), o["its"], o["bad"],
+                                        o["ok"].int()]))
     torch.cuda.synchronize()
     stage = np.array([[E[s][0].elapsed_time(E[s][1]), E[s][1].elapsed_time(E[s][2]),
                        E[s][2].elapsed_time(E[s][3])] for s in range(nprof)])
@@ -387,11 +513,12 @@ def run_gpu(args, rank, world, local_rank):
               "peak_ncu": 9350.0,
               "peak_note": "xbar-to-L1 distributed shared memory bytes at "
                            "23.7% of peak = 2.22 TB/s (7.55 GB per launch) "
-                           "in the committed ncu capture, i.e. about 9.35 TB/s"}
+                           "in one ncu capture of this workload, i.e. about "
+                           "9.35 TB/s (capture-derived peak)"}
     onchip["frac"] = onchip["achieved"] / onchip["peak_ncu"]
     # instruction issue, the decoder's actual bound (ncu: issue active ~60%,
     # not_selected and math-pipe throttle the leading stalls): warp
-    # instructions per codeword-iteration from the committed capture x the
+    # instructions per codeword-iteration from one ncu capture x the
     # iterations of the timed launch, against 4 schedulers per occupied SM
     issue = None
     if p0.plan.info.get("kind") == "qce" and its_stage:
@@ -405,10 +532,12 @@ def run_gpu(args, rank, world, local_rank):
         peak = sms * 4 * mhz / 1e3
         issue = {"unit": "G warp instructions/s", "achieved": ach, "peak": peak,
                  "frac": ach / peak, "sms": sms, "instructions_per_launch": instr,
-                 "what": "warp instructions per codeword-iteration (1.805 G over "
-                         "75 x 50 in the committed ncu capture) x the launch's "
-                         "iterations / launch time; peak = 4 schedulers x SM "
-                         "clock x the SMs the clusters occupy"}
+                 "instructions_source": "warp instructions per "
+                                        "codeword-iteration, " + CAPTURE_NOTE,
+                 "what": "warp instructions per codeword-iteration (one ncu "
+                         "capture) x the launch's iterations / launch time; "
+                         "peak = 4 schedulers x SM clock x the SMs the "
+                         "clusters occupy"}
     b_ldpc = nblk * (4 * N_INNER + N_INNER // 8 + 9)
     hbm, peak_kind = peaks()
     achieved = b_ldpc / (ldpc_ms / 1e3) / 1e9
@@ -421,6 +550,21 @@ def run_gpu(args, rank, world, local_rank):
         keys = sorted(fer)
         tot = shard.sum_over_ranks([v for k in keys for v in fer[k]], device=dev)
         fer = {k: [tot[2 * i], tot[2 * i + 1]] for i, k in enumerate(keys)}
+    # ---- what the parity check needs: the first nprof timed frames (one
+    # per Es/N0 point), their cells and the GPU outputs of the timed run ---
+    parity = None
+    if rank == 0 and world == 1:
+        fr = list(range(W, W + nprof))
+        parity = {"frames": fr,
+                  "esn0_db": [ESN0[f % len(ESN0)] for f in fr],
+                  "cells": cells[W:W + nprof].cpu().numpy(),
+                  "sig": sig[W:W + nprof].cpu().numpy(),
+                  "conv": conv[:nprof].astype(bool), "its": its[:nprof],
+                  "bad": torch.stack([outs[f]["bad"] for f in fr]).cpu().numpy(),
+                  "ok": ok[:nprof].astype(bool),
+                  "payload": torch.stack([outs[f]["payload"] for f in fr]).cpu().numpy(),
+                  "hard": torch.stack(stage_hard).cpu().numpy(),
+                  "stage_flags": torch.stack(stage_flags).cpu().numpy()}
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mbit/s",
@@ -433,6 +577,9 @@ def run_gpu(args, rank, world, local_rank):
                              "frac": achieved / hbm,
                              "traffic": (TRAFFIC_PER_BLOCK * nblk
                                          if TRAFFIC_PER_BLOCK else None),
+                             "traffic_source": "dram__bytes_read.sum + "
+                                               "dram__bytes_write.sum, "
+                                               + CAPTURE_NOTE,
                              "kernel": KERNEL_NAMES.get(p0.plan.info.get("kind"),
                                                         "ldpc_flood_kernel (CSR flooding)"),
                              "peak_kind": peak_kind,
@@ -452,21 +599,24 @@ def run_gpu(args, rank, world, local_rank):
                                     if v[1]},
                 "learned": learned,
                 "plan": p0.plan.info}
-    return line
+    return line, parity
 
 
 KERNEL_NAMES = {"qce": "ldpc_qce_kernel (quasi-cyclic flooding, edge-buffer layout)",
                 "qc": "ldpc_qc_kernel (quasi-cyclic flooding, record layout)"}
 
-# DRAM bytes (read + write) per 64800-bit block of the LDPC decoder launch:
-# dram__bytes_read.sum + dram__bytes_write.sum of one captured 75-block launch
-# of the edge-buffer decoder (19,542,528 + 0 B) / 75, from
-# profiles/ldpc_qce_flood_6_15_frame.md (the record-layout decoder's capture,
-# profiles/ldpc_qc_flood_6_15_frame.md, read 19,553,792 B).
+# Constants taken from one ncu capture of the edge-buffer decoder on this
+# workload (one 75-block launch of the 64800 6/15 frame, --clock-control
+# none); the bench line labels them as capture-derived, and they are
+# re-taken whenever the kernel changes.
+# DRAM bytes (read + write) per 64800-bit block of the LDPC launch:
+# dram__bytes_read.sum + dram__bytes_write.sum / 75.
 TRAFFIC_PER_BLOCK = 19_542_528 / 75
-# warp instructions per codeword-iteration of ldpc_qce_kernel<0, 8, 1024, 0> on this
-# workload: 1,805,381,535 over 75 blocks x 50 iterations (profiles/ldpc_qce_flood_6_15_frame.md)
+# warp instructions (smsp__inst_executed.sum) per codeword-iteration:
+# the launch's count / (75 blocks x its 50 iterations).
 INSTR_PER_BLOCK_ITER = 1_805_381_535 / 3750
+CAPTURE_NOTE = ("constant from one ncu capture of a 75-block launch of this "
+                "workload (not measured by this run)")
 
 
 def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
@@ -534,28 +684,87 @@ def run_e2e(pipes, streams, cells, sig, W, K, nblk, kp, dev, world):
             "bch_ok_blocks": int(hf[:, 3].sum())}
 
 
-def cpu_baseline(args, nblk_per_esn0=75):
-    """Reference CPU path on a bounded sample: nblk_per_esn0 blocks at each
-    of the 9 Es/N0 points (same mix as the GPU steps; 75 = one whole frame
-    per point, about 6 s over 16 host threads)."""
-    import torch
+def cpu_baseline(par):
+    """The reference CPU path timed on the host cores over the parity
+    frames (the first timed frames, one whole 75-block frame per Es/N0
+    point, 675 blocks): the reference receiver's own Python from
+    baseline/_ref when laid out, else the oracle route around the
+    reference's compiled kernel.  Returns (cpu_baseline dict, outputs)."""
     from atsc3_b200 import codes as C
     threads = os.cpu_count() or 1
     kp = C.kpayload(RATE, N_INNER)
-    cells, sig, nblk, _ = make_frames(len(ESN0), args.seed + 7,
-                                      "cuda" if torch.cuda.is_available() else "cpu")
-    c = cells[:, :nblk_per_esn0].reshape(-1, cells.shape[-1]).cpu().numpy()
-    s = sig[:, :nblk_per_esn0].reshape(-1, sig.shape[-1]).cpu().numpy()
+    c = par["cells"].reshape(-1, par["cells"].shape[-1])
+    g = par["sig"].reshape(-1, par["sig"].shape[-1])
+    try:
+        path = ReferenceCpuPath(threads)
+        what = ("the reference receiver's own Python from baseline/_ref "
+                "(m44_ldm._point_metric + per-bit minima / per-cell sigma2, "
+                "m44_ldm.ldpc_batch over lab/ldpc_kernel.c compiled -O3 "
+                "-ffp-contract=off, m9_accel.bch_syndrome_batch, descramble)")
+    except RuntimeError as e:
+        path = None
+        what = (f"oracle route ({e}): numpy float32 demap + lab/ldpc_kernel.c "
+                f"(-O3 -ffp-contract=off, oracle/_ref) + packed BCH")
     t0 = time.perf_counter()
-    nok, its = cpu_reference_decode(c, s, threads)
+    out = (path.decode(c, g) if path is not None else
+           cpu_reference_decode(c, g, threads, full=True))
     dt = time.perf_counter() - t0
-    return {"value": c.shape[0] * kp / dt / 1e6, "unit": "Mbit/s",
-            "cores": threads, "kind": "reference",
-            "sample": f"{c.shape[0]} blocks ({nblk_per_esn0} per Es/N0 point "
-                      f"4..8 dB, of {nblk} per frame), demap numpy f32 + lab/ldpc_kernel.c "
-                      f"(-O3 -ffp-contract=off) over {threads} threads + "
-                      f"packed BCH; {dt:.1f} s wall, mean its "
-                      f"{float(np.mean(its)):.1f}"}
+    nf = par["cells"].shape[0]
+    return ({"value": c.shape[0] * kp / dt / 1e6, "unit": "Mbit/s",
+             "cores": threads, "kind": "reference",
+             "sample": f"{c.shape[0]} blocks: the first {nf} timed frames "
+                       f"(one whole frame per Es/N0 point "
+                       f"{par['esn0_db'][0]:g}..{par['esn0_db'][-1]:g} dB), "
+                       f"{what}, {threads} threads; {dt:.1f} s wall"},
+            out)
+
+
+def parity_check(par, ref_py):
+    """GPU outputs of the timed frames against the reference on the same
+    blocks: the oracle route around the reference's compiled kernel
+    (bits, conv, its, bad, BCH ok, payload bytes) and, where it ran, the
+    reference's own Python path (all of those but its, which ldpc_batch
+    does not return).  Mismatch counts are blocks."""
+    threads = os.cpu_count() or 1
+    c = par["cells"].reshape(-1, par["cells"].shape[-1])
+    g = par["sig"].reshape(-1, par["sig"].shape[-1])
+    nb = c.shape[0]
+    gpu = {"bits": par["hard"].reshape(nb, -1),
+           "conv": par["conv"].reshape(-1), "its": par["its"].reshape(-1),
+           "bad": par["bad"].reshape(-1), "ok": par["ok"].reshape(-1),
+           "payload": par["payload"].reshape(nb, -1)}
+    sf = par["stage_flags"]                    # (frames, 4, blocks)
+    rerun = int((sf[:, 0].astype(bool).reshape(-1) != gpu["conv"]).sum() +
+                (sf[:, 1].reshape(-1) != gpu["its"]).sum() +
+                (sf[:, 2].reshape(-1) != gpu["bad"]).sum() +
+                (sf[:, 3].astype(bool).reshape(-1) != gpu["ok"]).sum())
+
+    def mism(ref, keys):
+        out = {}
+        for k in keys:
+            r = ref[k]
+            if k == "bits":
+                r = np.packbits(r, axis=1)
+            a, b = gpu[k], r
+            out[k] = int((a != b).reshape(nb, -1).any(axis=1).sum())
+        return out
+    o = cpu_reference_decode(c, g, threads, full=True)
+    res = {"blocks": nb, "frames": par["frames"], "esn0_db": par["esn0_db"],
+           "vs_reference_kernel": mism(o, ("bits", "conv", "its", "bad",
+                                            "ok", "payload")),
+           "gpu_rerun_flag_mismatch": rerun,
+           "reference_kernel": "lab/ldpc_kernel.c compiled -O3 "
+                               "-ffp-contract=off (oracle/_ref), float32 "
+                               "demap with per-cell sigma2, packed BCH"}
+    if ref_py is not None and "its" not in ref_py:
+        res["vs_reference_python"] = mism(ref_py, ("bits", "conv", "bad",
+                                                   "ok", "payload"))
+    tot = sum(res["vs_reference_kernel"].values()) + rerun
+    tot += sum(res.get("vs_reference_python", {}).values())
+    res["mismatch"] = tot
+    res["mean_iters"] = float(gpu["its"].mean())
+    res["converged_blocks"] = int(gpu["conv"].sum())
+    return res
 
 
 def run_uneven(args):
@@ -893,9 +1102,10 @@ def main(argv=None):
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    line = run_gpu(a, rank, world, local_rank)
+    line, par = run_gpu(a, rank, world, local_rank)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(a)
+        line["cpu_baseline"], ref_out = cpu_baseline(par)
+        line["parity"] = parity_check(par, ref_out)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

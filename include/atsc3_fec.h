@@ -366,7 +366,14 @@ int32_t atsc3_cpe_correct(const double *pool, int64_t ncells,
  * flooding only.  One CTA per codeword; per-CTA scratch (posterior + check
  * records) lives in the caller's workspace, sized by
  * atsc3_ldpc_layered_workspace for `ctas` resident CTAs.  Bounded waits: a
- * copy that never completes sets *err = 1 (device int32, caller-zeroed). */
+ * copy wait that runs out makes the CTA wait once more for its copies and
+ * return, setting *err (device int32, caller-zeroed) to 1 when the copies
+ * then completed, or 2 when the second wait ran out too (copies may have
+ * been in flight when the CTA returned: the outputs are void).
+ * atsc3_ldpc_layered_inject_timeout(layer) is a test hook: the next decode
+ * call takes that error path at global layer `layer` (iteration * Q + block
+ * row) right after the layer's copies completed, so the path runs with
+ * nothing in flight (-1 clears the hook). */
 typedef struct atsc3_ldpc_layered_plan atsc3_ldpc_layered_plan;
 
 int32_t atsc3_ldpc_layered_plan_create(int32_t n, int32_t kldpc, int32_t qldpc,
@@ -383,6 +390,7 @@ int32_t atsc3_ldpc_layered_decode(const atsc3_ldpc_layered_plan *plan,
                                   int64_t ld_hard, uint8_t *conv, int32_t *its,
                                   int32_t *bad, void *workspace, int32_t ctas,
                                   int32_t *err, void *stream);
+int32_t atsc3_ldpc_layered_inject_timeout(int32_t layer);
 
 /* ---- differentiable weighted min-sum ---------------------------------------
  * Unrolled flooding min-sum with per-iteration, per-check-degree scale and
@@ -464,6 +472,24 @@ int32_t atsc3_demap_gather(const float *cells, int64_t ncells, int32_t nblk,
 int32_t atsc3_demap_row_sigma2(const float *cells, int64_t ld_cells,
                                int32_t nblk, int32_t ncell, const float *pts,
                                int32_t nbits, float *sigma2, void *stream);
+
+/* Float64 demapper: the same max-log LLRs in double arithmetic, replacing
+ * the reference's default float64 `demap_llr_fast` (lab/m16_demap_fast.py:
+ * 80-119: m = |p|^2 - 2 Re(y p*), per-bit minima, (a - b) / sigma2).
+ * cells: (nblk, ld_cells) complex128 as (re, im) double pairs, 16-byte
+ * aligned; pts: 3*M doubles (Re, Im, |p|^2); sigma_mode 0 scalar, 1 per
+ * cell, 2 per row (sigma2 from atsc3_demap_row_sigma2_f64, the
+ * lab/m16_demap_fast.py:104-106 estimate); lam_of_q nullable (q order). */
+int32_t atsc3_demap_f64(const double *cells, int64_t ld_cells, int32_t nblk,
+                        int32_t ncell, const double *pts, int32_t nbits,
+                        int32_t sigma_mode, const double *sigma2,
+                        int64_t ld_sigma, double sigma2_scalar,
+                        const int32_t *lam_of_q, double *out, int64_t ld_out,
+                        void *stream);
+int32_t atsc3_demap_row_sigma2_f64(const double *cells, int64_t ld_cells,
+                                   int32_t nblk, int32_t ncell,
+                                   const double *pts, int32_t nbits,
+                                   double *sigma2, void *stream);
 
 /* BCH zero-syndrome check (A/322 6.1.2.1) plus descramble of the payload.
  * hard: (nblk, ld_hard) packed hard decisions (as atsc3_ldpc_decode_flood

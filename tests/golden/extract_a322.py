@@ -12,7 +12,7 @@ modules once, on a machine that has the receiver checked out, and stores the
 numbers in a compact archive so the package needs no receiver source at run
 time.  No code is taken from them: only the tables.
 
-Usage:  python atsc3_b200/data/extract_a322.py /path/to/atsc3/checkout
+Usage:  python tests/golden/extract_a322.py /path/to/atsc3/checkout
 """
 from __future__ import annotations
 
@@ -23,7 +23,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-OUT = os.path.join(HERE, "a322_tables.npz")
+OUT = os.path.join(os.path.dirname(os.path.dirname(HERE)), "atsc3_b200", "data",
+                   "a322_tables.npz")
 
 
 def main(argv=None):

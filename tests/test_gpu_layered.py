@@ -47,3 +47,33 @@ def test_layered_golden_cases(name):
     # converged blocks decode to the transmitted codeword
     for i in np.flatnonzero(want[1]):
         assert np.array_equal(want[0][i], cw[i])
+
+
+def test_layered_copy_timeout_path_reports_and_context_survives():
+    """The bounded-wait error path: the test hook makes every CTA take the
+    timeout branch at layer 5 of iteration 0, right after that layer's
+    copies completed (nothing is in flight when the CTAs return).  The
+    launch records error code 1, check_layered_error raises, and the next
+    launch on the same plan decodes bit-exactly again."""
+    import torch
+    from atsc3_b200 import native as N
+    from atsc3_b200.ldpc import LayeredPlan, check_layered_error, decode_layered
+    n, rate = 64800, "8/15"
+    rng = np.random.default_rng(11)
+    llr = (rng.standard_normal((4, n)) * 2.0 + 1.0).astype(np.float32)
+    plan = LayeredPlan(rate, n, ctas=2)
+    d = torch.from_numpy(llr).cuda()
+    N.call("atsc3_ldpc_layered_inject_timeout", 5)
+    decode_layered(plan, d, iters=8, alpha=0.75)
+    torch.cuda.synchronize()
+    assert int(plan.err.item()) == 1
+    with pytest.raises(N.FecError) as e:
+        check_layered_error(plan)
+    assert "error code 1" in str(e.value)
+    assert int(plan.err.item()) == 0           # the checker clears it
+    # the hook is consumed by one call: this launch runs normally
+    want = oracle.layered(llr, rate, n, iters=8, alpha=0.75)
+    o = decode_layered(plan, d, iters=8, alpha=0.75)
+    check_layered_error(plan)
+    assert np.array_equal(o["bits"].cpu().numpy(), want[0])
+    assert o["its"].cpu().numpy().tolist() == want[2].tolist()

@@ -286,15 +286,48 @@ def test_bch_dropins_match_golden(torch):
         assert hex(bch_syndrome(m[0], n)) == want[0]
 
 
+def _exhaustive_f64(cells, pts, nb, s2):
+    """float64 max-log LLRs, |z - p|^2 exhaustively (the lab/m6_bicm.py:
+    213-225 form the reference's demap_llr_fast gate compares against)."""
+    d2 = np.abs(np.asarray(cells, np.complex128)[:, None] - pts[None, :]) ** 2
+    if s2 is None:
+        s2 = max(float(d2.min(1).mean()), 1e-9)
+    m = d2.reshape(len(cells), *([2] * nb))
+    out = np.empty((len(cells), nb))
+    for i in range(nb):
+        ax = tuple(a for a in range(1, nb + 1) if a != i + 1)
+        mn = m.min(axis=ax)
+        out[:, i] = (mn[:, 1] - mn[:, 0]) / (s2 if np.ndim(s2) == 0
+                                              else np.asarray(s2, np.float64))
+    return out.ravel()
+
+
 def test_demap_llr_fast_dropin(torch):
+    from atsc3_b200 import codes as C
     from atsc3_b200.demap import demap_llr_fast
     c, pay, cw, cells, s2, q, lam = oracle_case("c64_16qam_6_15_ray")
-    got = demap_llr_fast(cells[0], c["mod"], c["rate"], sigma2=s2[0])
+    # dtype=float32: bit-exact with the float32 reference arithmetic
+    got = demap_llr_fast(cells[0], c["mod"], c["rate"], sigma2=s2[0],
+                         dtype=np.float32)
     assert got.dtype == np.float64
     assert np.array_equal(got.astype(np.float32), q[0])
     c2, _, _, cells2, s22, q2, _ = oracle_case("c64_256qam_10_15")
-    got = demap_llr_fast(cells2[1], c2["mod"], c2["rate"], sigma2=float(s22))
+    got = demap_llr_fast(cells2[1], c2["mod"], c2["rate"], sigma2=float(s22),
+                         dtype=np.float32)
     assert np.array_equal(got.astype(np.float32), q2[1])
+    # dtype=float64 (the reference's default): within the reference gate's
+    # 1e-12 of the largest LLR (lab/m16_demap_fast.py:134-140) of the
+    # exhaustive float64 demapper, supplied per-cell, scalar and estimated
+    # sigma2
+    for cc, s, mod, rate in ((cells[0], s2[0], c["mod"], c["rate"]),
+                             (cells2[1], float(s22), c2["mod"], c2["rate"]),
+                             (cells2[0], None, c2["mod"], c2["rate"])):
+        pts = C.points_for(mod, rate)
+        want = _exhaustive_f64(cc, pts, C.MOD_BITS[mod], s)
+        got = demap_llr_fast(cc, mod, rate, sigma2=s)
+        assert got.dtype == np.float64 and got.shape == want.shape
+        rel = np.abs(got - want).max() / np.abs(want).max()
+        assert rel < 1e-12, rel
 
 
 @pytest.mark.parametrize("kind,cluster,threads", [

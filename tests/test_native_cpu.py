@@ -144,3 +144,21 @@ def test_install_rebinds_and_restores():
     assert ce.cpe_correct is cpe.cpe_correct
     I.uninstall()
     assert mg.sum_product_decode_batch == "ref" and ce.cpe_correct == "ref"
+
+
+@pytest.mark.parametrize("kldpc,kpay,what", [(64801, 0, "kldpc"),
+                                            (0, 0, "kldpc"),
+                                            (25920, 25921, "kpayload"),
+                                            (25920, -1, "kpayload")])
+def test_noalloc_refuses_bch_lengths_past_the_codeword(kldpc, kpay, what):
+    """The allocation-free entry point reads the first kldpc hard decisions
+    of a scratch row that the LDPC step fills only up to ncell*nbits, so a
+    longer kldpc (or a payload longer than kldpc) is refused with -3 before
+    any plan or device access (the plan pointer here is never read)."""
+    dummy = ctypes.c_void_p(1)
+    rc = N.lib().atsc3_fec_decode_noalloc(
+        dummy, 2, None, 0, 1, 16200, None, 4, 0, None, 0, ctypes.c_float(1.0),
+        None, 50, ctypes.c_float(0.75), None, kldpc, None, kpay, None, 0,
+        None, None, None, None, None, None)
+    assert rc == -3
+    assert what in N.lib().atsc3_last_error().decode()
