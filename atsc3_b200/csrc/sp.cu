@@ -108,8 +108,16 @@ __global__ void __launch_bounds__(256) sp_check_kernel(const SpArgs a, int upd) 
   }
 }
 
-// per block: converged (zero syndrome) or out of iterations
-__global__ void sp_status_kernel(const SpArgs a, int it) {
+// per block: converged (zero syndrome) or out of iterations.  counts
+// (nullable, one CTA launch): [0] blocks still decoding after this
+// iteration, [1] blocks stopped unconverged at this iteration.
+__global__ void sp_status_kernel(const SpArgs a, int it, int32_t *counts) {
+  __shared__ int s_act, s_stop;
+  if (threadIdx.x == 0) {
+    s_act = 0;
+    s_stop = 0;
+  }
+  __syncthreads();
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < a.nblk;
        b += gridDim.x * blockDim.x) {
     if (!a.st[b]) continue;
@@ -121,7 +129,15 @@ __global__ void sp_status_kernel(const SpArgs a, int it) {
       a.conv[b] = badct == 0 ? 1 : 0;
       a.its[b] = it;
       a.bad[b] = badct;
+      if (badct) atomicAdd(&s_stop, 1);
+    } else {
+      atomicAdd(&s_act, 1);
     }
+  }
+  __syncthreads();
+  if (counts && threadIdx.x == 0 && blockIdx.x == 0) {
+    counts[0] = s_act;
+    counts[1] = s_stop;
   }
 }
 
@@ -213,10 +229,68 @@ int32_t atsc3_ldpc_sp_decode(const int32_t *cptr, const int32_t *cidx,
   for (int it = 0; it <= iters; ++it) {
     const int upd = it < iters ? 1 : 0;
     sp_check_kernel<<<grid((int64_t)nblk * nc), 256, 0, st>>>(a, upd);
-    sp_status_kernel<<<1, 256, 0, st>>>(a, it);
+    sp_status_kernel<<<1, 256, 0, st>>>(a, it, nullptr);
     sp_bits_kernel<<<grid((int64_t)nblk * n), 256, 0, st>>>(a, it);
     if (upd) sp_var_kernel<<<grid((int64_t)nblk * n), 256, 0, st>>>(a);
   }
+  ATSC3_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int32_t atsc3_ldpc_sp_step(const int32_t *cptr, const int32_t *cidx,
+                           const int32_t *vptr, const int32_t *vedge,
+                           int32_t n, int32_t nc, int32_t nedges,
+                           const double *llr, int64_t ld_llr, int32_t nblk,
+                           int32_t it, int32_t last, uint8_t *bits,
+                           int64_t ld_bits, uint8_t *conv, int32_t *its,
+                           int32_t *bad, void *work, int32_t *counts,
+                           void *stream) {
+  using namespace atsc3;
+  ATSC3_ARG(n > 0 && nc > 0 && nedges > 0 && nblk >= 0 && it >= 0, "bad size");
+  if (nblk == 0) return 0;
+  ATSC3_ARG(cptr && cidx && vptr && vedge && llr && bits && conv && its && bad &&
+                work && counts, "null pointer");
+  ATSC3_ARG(ld_llr >= n && ld_bits >= n, "leading dimension below n");
+  ATSC3_ARG(((uintptr_t)work & 7) == 0 && ((uintptr_t)llr & 7) == 0,
+            "llr and work must be 8-byte aligned");
+  SpArgs a;
+  a.cptr = cptr;
+  a.cidx = cidx;
+  a.vptr = vptr;
+  a.vedge = vedge;
+  a.n = n;
+  a.nc = nc;
+  a.nedges = nedges;
+  a.nblk = nblk;
+  // the last step retires every block still decoding (as iteration `iters`
+  // of a full decode does); any other step retires only converged blocks
+  a.iters = last ? it : it + 1;
+  a.llr = llr;
+  a.ld_llr = ld_llr;
+  a.tot = (double *)work;
+  a.msg = a.tot + (size_t)nblk * n;
+  a.st = (int32_t *)(a.msg + (size_t)nblk * nedges);
+  a.bits = bits;
+  a.ld_bits = ld_bits;
+  a.conv = conv;
+  a.its = its;
+  a.bad = bad;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, sms = 148;
+  ATSC3_CUDA(cudaGetDevice(&dev));
+  ATSC3_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  auto grid = [&](int64_t work_items) {
+    int64_t g = (work_items + 255) / 256;
+    const int64_t cap = (int64_t)sms * 16;
+    return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+  };
+  if (it == 0)
+    sp_init_kernel<<<grid((int64_t)nblk * (n > nedges ? n : nedges)), 256, 0, st>>>(a);
+  const int upd = last ? 0 : 1;
+  sp_check_kernel<<<grid((int64_t)nblk * nc), 256, 0, st>>>(a, upd);
+  sp_status_kernel<<<1, 256, 0, st>>>(a, it, counts);
+  sp_bits_kernel<<<grid((int64_t)nblk * n), 256, 0, st>>>(a, it);
+  if (upd) sp_var_kernel<<<grid((int64_t)nblk * n), 256, 0, st>>>(a);
   ATSC3_CUDA(cudaGetLastError());
   return 0;
 }

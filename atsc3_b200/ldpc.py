@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes
 import threading
+import time
 
 import numpy as np
 
@@ -502,22 +503,75 @@ def sp_decode(tab, llr, iters=100, out=None, stream=None):
     return o
 
 
+def sp_decode_deadline(tab, llr, iters=100, deadline=None, out=None,
+                       stream=None):
+    """sp_decode one iteration at a time, honouring a wall-clock
+    ``deadline`` (a ``time.perf_counter()`` value) as lab/m16_margin.py:
+    364-371 does: no new iteration starts after it; the iteration at which
+    it is found passed takes the syndrome and retires every block still
+    decoding with its current decisions (conv False unless the syndrome is
+    zero, its = that iteration, bad = the unsatisfied count).  Each
+    iteration waits for the GPU, so the clock is read after the work it
+    follows.  Returns (device tensors bits/conv/its/bad, the number of
+    blocks stopped by the deadline)."""
+    torch = _torch()
+    nblk, n = llr.shape
+    dev = llr.device
+    o = out if out is not None else {}
+    o.setdefault("bits", torch.empty((nblk, n), dtype=torch.uint8, device=dev))
+    o.setdefault("conv", torch.empty(nblk, dtype=torch.uint8, device=dev))
+    o.setdefault("its", torch.empty(nblk, dtype=torch.int32, device=dev))
+    o.setdefault("bad", torch.empty(nblk, dtype=torch.int32, device=dev))
+    if nblk == 0:
+        return o, 0
+    nbytes = ctypes.c_int64()
+    N.call("atsc3_ldpc_sp_workspace", n, tab["nedges"], nblk, ctypes.byref(nbytes))
+    work = torch.empty(max(8, nbytes.value), dtype=torch.uint8, device=dev)
+    counts = torch.zeros(2, dtype=torch.int32, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    c, ci, v, ve = tab["t"]
+    shed = 0
+    for it in range(iters + 1):
+        last = it == iters or (deadline is not None and
+                               time.perf_counter() > deadline)
+        N.call("atsc3_ldpc_sp_step", c.data_ptr(), ci.data_ptr(), v.data_ptr(),
+               ve.data_ptr(), n, tab["nc"], tab["nedges"], llr.data_ptr(),
+               llr.stride(0), nblk, it, int(last), o["bits"].data_ptr(),
+               o["bits"].stride(0), o["conv"].data_ptr(), o["its"].data_ptr(),
+               o["bad"].data_ptr(), work.data_ptr(), counts.data_ptr(), st)
+        active, stopped = (int(x) for x in counts.cpu())   # waits for the step
+        if last:
+            shed = stopped if it < iters else 0
+            break
+        if active == 0:
+            break
+    return o, shed
+
+
 def sum_product_decode_batch(lam2d, checks, n, iters=100, deadline=None,
                              stats=None):
     """Drop-in for ``lab/m16_margin.py:325`` ``sum_product_decode_batch``:
-    numpy (bits uint8, conv bool, its int32, bad int32).  ``deadline`` (a
-    wall-clock budget on the host) has no GPU counterpart: the decode runs
-    to ``iters``; ``stats`` is accepted and left untouched."""
+    numpy (bits uint8, conv bool, its int32, bad int32).  ``deadline``: a
+    ``time.perf_counter()`` value after which no new iteration starts
+    (sp_decode_deadline); the blocks it stops are counted in
+    ``stats["sp_timeout"]``, as the reference counts them.  Without a
+    deadline every iteration is queued at once (sp_decode)."""
     torch = _torch()
     tab = sp_tables(C.csr_from_checks(checks, n), n)
     llr = torch.from_numpy(np.ascontiguousarray(lam2d, np.float64)).cuda()
-    o = sp_decode(tab, llr, iters=iters)
-    torch.cuda.synchronize()
+    if deadline is None:
+        o = sp_decode(tab, llr, iters=iters)
+        torch.cuda.synchronize()
+    else:
+        o, shed = sp_decode_deadline(tab, llr, iters=iters, deadline=deadline)
+        if shed and stats is not None:
+            stats["sp_timeout"] = stats.get("sp_timeout", 0) + shed
     return (o["bits"].cpu().numpy(), o["conv"].cpu().numpy().astype(bool),
             o["its"].cpu().numpy(), o["bad"].cpu().numpy())
 
 
-def rescue_near_misses(tab, lam, out, near_max=1500, max_blocks=8, iters=100):
+def rescue_near_misses(tab, lam, out, near_max=1500, max_blocks=8, iters=100,
+                       budget_s=None, stats=None):
     """The near-miss rescue of ``lab/m44_ldm.py:2527-2554``: the blocks a
     min-sum decode left unconverged with at most ``near_max`` unsatisfied
     checks (the ``max_blocks`` closest ones) are decoded again with the
@@ -525,7 +579,10 @@ def rescue_near_misses(tab, lam, out, near_max=1500, max_blocks=8, iters=100):
     hard decisions (``out["hard"]``) and flags (conv = 1, bad = 0; ``its``
     keeps the min-sum count).  ``lam``: the (nblk, n) float32 LLRs of that
     decode.  Selecting the blocks reads conv/bad on the host (as the
-    reference does).  Returns the indices of the rescued blocks."""
+    reference does).  ``budget_s``: the rescue's wall-clock budget from the
+    call (lab/m44_ldm.py:2544-2545 with SP_BUDGET_S of :135; None = run to
+    ``iters``); blocks it stops are added to ``stats["sp_timeout"]``.
+    Returns the indices of the rescued blocks."""
     torch = _torch()
     conv = out["conv"].cpu().numpy()
     bad = out["bad"].cpu().numpy()
@@ -536,7 +593,14 @@ def rescue_near_misses(tab, lam, out, near_max=1500, max_blocks=8, iters=100):
         return near
     dev = lam.device
     idx = torch.from_numpy(near.astype(np.int64)).to(dev)
-    o = sp_decode(tab, lam.index_select(0, idx).double(), iters=iters)
+    sub = lam.index_select(0, idx).double()
+    if budget_s is None:
+        o = sp_decode(tab, sub, iters=iters)
+    else:
+        o, shed = sp_decode_deadline(tab, sub, iters=iters,
+                                     deadline=time.perf_counter() + budget_s)
+        if shed and stats is not None:
+            stats["sp_timeout"] = stats.get("sp_timeout", 0) + shed
     ok = o["conv"].bool()
     sel = idx[ok]
     if sel.numel():

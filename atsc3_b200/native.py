@@ -87,6 +87,9 @@ SIGNATURES = {
     "atsc3_ldpc_sp_decode": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32,
                                      c_i32, c_vp, c_i64, c_i32, c_i32, c_vp,
                                      c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "atsc3_ldpc_sp_step": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32, c_i32,
+                                   c_vp, c_i64, c_i32, c_i32, c_i32, c_vp,
+                                   c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "atsc3_cpe_workspace": (c_i32, [c_vp]),
     "atsc3_cpe_correct": (c_i32, [c_vp, c_i64, c_vp, c_i32, c_vp, c_vp, c_i32,
                                   c_vp, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp,

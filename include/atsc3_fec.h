@@ -326,9 +326,17 @@ int32_t atsc3_ldpc_qce_decode_weighted(
  * unsatisfied count.  cptr/cidx/vptr/vedge: DEVICE CSR tables
  * (lab/m3_ldpc.py:459-482 layout); llr (nblk, ld_llr) float64; bits (nblk,
  * ld_bits) uint8; conv/its/bad per block; work: atsc3_ldpc_sp_workspace
- * bytes, 8-byte aligned.  The reference's wall-clock deadline has no
- * counterpart: the GPU runs to `iters`.  Launches 4*(iters+1)+1 kernels on
- * `stream`; returns without synchronising. */
+ * bytes, 8-byte aligned.  atsc3_ldpc_sp_decode runs to `iters`: it
+ * launches 4*(iters+1)+1 kernels on `stream` and returns without
+ * synchronising.  atsc3_ldpc_sp_step runs ONE iteration `it` (it = 0
+ * initialises the work area first; steps run in order on one stream),
+ * so a host can honour the reference's wall-clock deadline between
+ * iterations (lab/m16_margin.py:364-371): `last` = 1 takes the syndrome at
+ * `it` and retires every block still decoding with its current decisions
+ * (conv 0 unless the syndrome is zero, its = it, bad = the unsatisfied
+ * count), as iteration `iters` of a full decode does.  counts: device
+ * int32[2] = {blocks still decoding after the step, blocks retired
+ * unconverged by it}. */
 int32_t atsc3_ldpc_sp_workspace(int32_t n, int32_t nedges, int32_t nblk,
                                 int64_t *work_bytes);
 int32_t atsc3_ldpc_sp_decode(const int32_t *cptr, const int32_t *cidx,
@@ -338,6 +346,14 @@ int32_t atsc3_ldpc_sp_decode(const int32_t *cptr, const int32_t *cidx,
                              int32_t iters, uint8_t *bits, int64_t ld_bits,
                              uint8_t *conv, int32_t *its, int32_t *bad,
                              void *work, void *stream);
+int32_t atsc3_ldpc_sp_step(const int32_t *cptr, const int32_t *cidx,
+                           const int32_t *vptr, const int32_t *vedge,
+                           int32_t n, int32_t nc, int32_t nedges,
+                           const double *llr, int64_t ld_llr, int32_t nblk,
+                           int32_t it, int32_t last, uint8_t *bits,
+                           int64_t ld_bits, uint8_t *conv, int32_t *its,
+                           int32_t *bad, void *work, int32_t *counts,
+                           void *stream);
 
 /* ---- common phase error correction ----------------------------------------
  * Replaces lab/m6_cells.py:176-209 cpe_correct (also lab/m9_gpu.py:283-299

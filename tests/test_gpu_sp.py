@@ -42,6 +42,59 @@ def test_sum_product_dropin_signature():
     assert np.array_equal(bits, cw)
 
 
+class TickClock:
+    """A perf_counter that advances by one per reading, so a deadline of
+    k - 0.5 lets iterations 0 .. k-1 start and stops at iteration k."""
+
+    def __init__(self):
+        self.t = -1.0
+
+    def __call__(self):
+        self.t += 1.0
+        return self.t
+
+
+@pytest.mark.parametrize("stop_at", [0, 1, 3])
+def test_sum_product_deadline_stops_like_the_reference(monkeypatch, stop_at):
+    """lab/m16_margin.py:364-371: after the deadline no new iteration
+    starts; the iteration at which it is seen takes the syndrome, rows that
+    converged there keep their verdict, the rest return their current hard
+    decisions with conv False, its = that iteration, bad = the unsatisfied
+    count, and stats["sp_timeout"] counts them.  That is exactly a decode
+    run to iters = stop_at (the oracle), plus the count."""
+    import types
+    from atsc3_b200 import ldpc as LDPC
+    c = cases()["sp_4_15"]
+    n = c["n"]
+    lam, cw = oracle.near_miss_llr(c["rate"], n, c["nblk"], c["mu"], c["seed"])
+    assert min(c["its"]) > 3                 # every row is still decoding
+    # the decoder's clock only (ldpc.time), not the process-wide one
+    monkeypatch.setattr(LDPC, "time", types.SimpleNamespace(perf_counter=TickClock()))
+    stats = {}
+    bits, conv, its, bad = LDPC.sum_product_decode_batch(
+        lam, C.parity_check(c["rate"], n), n, iters=c["iters"],
+        deadline=stop_at - 0.5, stats=stats)
+    wb, wc, wi, wd = oracle.sum_product(lam, C.csr(c["rate"], n), n, iters=stop_at)
+    assert its.tolist() == [stop_at] * len(its) == wi.tolist()
+    assert conv.tolist() == wc.tolist() and bad.tolist() == wd.tolist()
+    assert np.array_equal(bits, wb)
+    assert stats == {"sp_timeout": int((~wc).sum())} and (~wc).sum() > 0
+
+
+def test_sum_product_deadline_not_reached_is_the_full_decode():
+    import time as _time
+    from atsc3_b200 import ldpc as LDPC
+    c = cases()["sp_4_15"]
+    lam, cw = oracle.near_miss_llr(c["rate"], c["n"], c["nblk"], c["mu"], c["seed"])
+    stats = {}
+    bits, conv, its, bad = LDPC.sum_product_decode_batch(
+        lam, C.parity_check(c["rate"], c["n"]), c["n"], iters=c["iters"],
+        deadline=_time.perf_counter() + 3600.0, stats=stats)
+    assert conv.tolist() == c["conv"] and its.tolist() == c["its"]
+    assert bad.tolist() == c["bad"] and stats == {}
+    assert np.array_equal(bits, cw)
+
+
 def test_rescue_replaces_min_sum_failures():
     """Blocks min-sum leaves unconverged get the sum-product; those it
     closes carry the sum-product's hard decisions (packed) and conv = 1."""

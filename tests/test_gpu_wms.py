@@ -184,3 +184,36 @@ def test_weighted_edge_buffer_vs_weighted_oracle(rate, n):
     assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
     assert o["its"].cpu().numpy().tolist() == want[2].tolist()
     assert o["bad"].cpu().numpy().tolist() == want[3].tolist()
+
+
+def test_wms_backward_recomputes_instead_of_storing_messages():
+    """Config 4's batch (256 blocks of 64800 8/15, T = 12): the peak device
+    memory of forward + backward stays below what storing every
+    iteration's per-edge messages alone would take (T x E x 4 bytes per
+    block, 3.5 GB here) -- the forward keeps a 16-byte record per check and
+    iteration, and the backward recomputes each iteration's messages from
+    them."""
+    import torch
+    from atsc3_b200 import synth
+    from atsc3_b200.learned import WeightedMinSum, WmsCode, bce_loss, make_batch
+    rate, n, T, nblk = "8/15", 64800, 12, 256
+    code = WmsCode(rate, n)
+    tx = synth.Transmitter(n, "64QAM", rate, device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    lam, cw = make_batch(tx, g, nblk, 12.1, 14.1)
+    a, b = code.init_params(T, 0.8, 0.05)
+    a.requires_grad_(True)
+    b.requires_grad_(True)
+    bits = cw.float()
+    torch.cuda.synchronize()
+    base = torch.cuda.memory_allocated()
+    torch.cuda.reset_peak_memory_stats()
+    loss = bce_loss(WeightedMinSum.apply(lam, a, b, code, False), bits)
+    loss.backward()
+    torch.cuda.synchronize()
+    peak = torch.cuda.max_memory_allocated() - base
+    stored = T * code.ne * 4 * nblk
+    records = T * code.nc * 16 * nblk
+    assert torch.isfinite(a.grad).all() and a.grad.abs().sum() > 0
+    assert peak < stored, (peak, stored, records)
