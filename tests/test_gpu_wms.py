@@ -46,14 +46,17 @@ def test_wms_forward_and_gradients_vs_float64_reference():
     lref.backward()
     o = out.detach().cpu().double().numpy()
     r = ref.detach().numpy()
-    close = np.abs(o - r) <= 1e-3 * np.maximum(1.0, np.abs(r))
-    assert close.mean() > 0.999, close.mean()
-    assert abs(float(loss.detach()) - float(lref.detach())) <= 1e-4 * abs(float(lref.detach()))
+    # measured on one B200 over three seeds of this case: output LLRs
+    # within 3.0e-6 of max(1, |ref|), loss within 3.3e-7 relative, parameter
+    # gradients within 1.8e-4 of the largest gradient entry (float32
+    # messages against float64); the bars keep a margin of 5-10x
+    assert (np.abs(o - r) <= 3e-5 * np.maximum(1.0, np.abs(r))).all()
+    assert abs(float(loss.detach()) - float(lref.detach())) <= 3e-6 * abs(float(lref.detach()))
     for g, gr in ((a.grad, a64.grad), (b.grad, b64.grad)):
         g = g.cpu().double().numpy()
         gr = gr.numpy()
         rel = np.abs(g - gr).max() / max(np.abs(gr).max(), 1e-12)
-        assert rel < 1e-2, rel
+        assert rel < 1e-3, rel
 
 
 def test_wms_unweighted_equals_plain_minsum_hard_decisions():
