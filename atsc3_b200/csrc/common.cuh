@@ -146,6 +146,12 @@ __device__ __forceinline__ uint32_t vbits(float a) { return __float_as_uint(a); 
 __device__ __forceinline__ unsigned long long vbits(double a) {
   return (unsigned long long)__double_as_longlong(a);
 }
+__device__ __forceinline__ void dsmem_st_bits(uint32_t a, uint32_t bits) {
+  dsmem_st_u32(a, bits);
+}
+__device__ __forceinline__ void dsmem_st_bits(uint32_t a, unsigned long long bits) {
+  dsmem_st_u64(a, bits);
+}
 __device__ __forceinline__ void dsmem_st_msg(uint32_t a, uint32_t mag_bits, uint32_t neg) {
   dsmem_st_u32(a, mag_bits | (neg << 31));
 }

@@ -585,7 +585,9 @@ __device__ __forceinline__ V qce_var_exact(V *col, int s0, V li, bool mv) {
     for (int c = 1; c < D; ++c) v = (s == c) ? m[(c + t) % D] : v;
     acc = add_rn(acc, v);
   }
-  const V tot = TORCH ? acc : add_rn(li, acc);
+  // torch semantics: + 0.0 turns a -0.0 sum into +0.0 (the only way a
+  // slot could receive -0.0; the sign is the same for the hard decision)
+  const V tot = TORCH ? add_rn(acc, V(0)) : add_rn(li, acc);
   if (mv) {
 #pragma unroll
     for (int i = 0; i < D; ++i) col[i * EZ] = sub_rn(tot, m[i]);
@@ -629,7 +631,9 @@ __device__ __forceinline__ V qce_var_generic(V *col, int d, int dA, int s0,
   V acc = TORCH ? li : V(0);
   acc = qce_seg_sum(acc, col, dA, s0);
   if (dA < d) acc = qce_seg_sum(acc, col + dA * EZ, d - dA, s0b);
-  const V tot = TORCH ? acc : add_rn(li, acc);
+  // torch semantics: + 0.0 turns a -0.0 sum into +0.0 (the only way a
+  // slot could receive -0.0; the sign is the same for the hard decision)
+  const V tot = TORCH ? add_rn(acc, V(0)) : add_rn(li, acc);
   if (mv) {
     int i = 0;
     for (; i + 4 <= d; i += 4) {
@@ -648,8 +652,20 @@ __device__ __forceinline__ V qce_var_generic(V *col, int d, int dA, int s0,
 // FULL: every slot is an edge of every lane's check and all 32 lanes are
 // checks (no masking at all); otherwise `live` masks absent slots (rows of
 // lower degree, the missing wrap edge of check (0, 0), lanes past 359), whose
-// loads and stores go to a junk word.  Returns the lane's syndrome bit.
-template <typename V, bool TORCH, int D, bool FULL, typename MASK>
+// loads and stores go to a junk word.  SYN: also form the lane's syndrome
+// bit from the hard-decision bitmap (else 0 is returned: the caller already
+// knows that this iteration's syndrome is not zero).
+//
+// Signs are taken from the sign bits of the slot values: no slot that a
+// check reads holds -0.0 (the prologue and the torch-semantics variable
+// phase add +0.0, which turns -0.0 into +0.0 and changes nothing else; the
+// other sums never produce -0.0), so the sign bit of t is exactly the
+// reference's (v < 0).  Rows of up to 11 edges (their values stay in
+// registers to the end) take the parity as the XOR of the sign bits and a
+// message's sign bit as parity ^ sign(t): one XOR onto the magnitude that
+// already carries the parity.  Longer rows keep a mask of the signs so the
+// values can die early.
+template <typename V, bool TORCH, int D, bool FULL, bool SYN, typename MASK>
 __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
                                               uint32_t lane,
                                               const uint32_t *bm,
@@ -659,6 +675,8 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
   // below, so the syndrome lookup overlaps its latency), syndrome bit; the
   // syndrome-only final pass loads too (valid addresses, values unused)
   constexpr uint32_t VB = sizeof(V);
+  using UB = decltype(vbits(V(0)));
+  constexpr UB SIGN = (UB)1 << (8 * sizeof(UB) - 1);
   uint32_t ad[D];
   V t[D];
   uint32_t synw = 0;
@@ -674,11 +692,13 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
       ad[j] = on ? e.x + VB * o : dummy;
     }
     t[j] = dsmem_ld<V>(ad[j]);
-    const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
-    if constexpr (FULL) {
-      synw ^= hw >> (o & 31);
-    } else {
-      synw ^= (hw >> (o & 31)) & ((uint32_t)(live >> j) & 1u);
+    if constexpr (SYN) {
+      const uint32_t hw = bm[(e.y & 0xFFFFu) + (o >> 5)];
+      if constexpr (FULL) {
+        synw ^= hw >> (o & 31);
+      } else {
+        synw ^= (hw >> (o & 31)) & ((uint32_t)(live >> j) & 1u);
+      }
     }
   }
   if (upd) {
@@ -690,27 +710,29 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
     // message by comparing |t| with min1; longer rows track the first
     // minimum's position instead, so the values can die early (registers).
     constexpr bool BY_VALUE = D <= 11;
+    constexpr bool WIDE = sizeof(MASK) > 4;
     V min1 = inf, min2 = inf;
     uint32_t first = 0;
-    MASK sv = 0;
+    UB pw = 0;                                       // XOR of the sign bits
+    MASK sv = 0;                                     // sign mask (long rows)
 #pragma unroll
     for (int j = 0; j < D; ++j) {
       V mag = vabs(t[j]);
-      bool ng = t[j] < V(0);
+      UB tb = vbits(t[j]);
       if constexpr (!FULL) {
         const bool on = (live >> j) & 1;
         mag = on ? mag : inf;
-        ng = ng && on;
+        tb = on ? tb : (UB)0;
       }
-      sv |= ng ? ((MASK)1 << j) : (MASK)0;
-      if constexpr (!BY_VALUE) first = mag < min1 ? (uint32_t)j : first;
+      if constexpr (BY_VALUE) {
+        pw ^= tb;
+      } else {
+        sv |= (tb & SIGN) ? ((MASK)1 << j) : (MASK)0;
+        first = mag < min1 ? (uint32_t)j : first;
+      }
       min2 = vmin(min2, vmax(min1, mag));
       min1 = vmin(min1, mag);
     }
-    constexpr bool WIDE = sizeof(MASK) > 4;
-    int par;
-    if constexpr (WIDE) par = __popcll((unsigned long long)sv) & 1;
-    else par = __popc((uint32_t)sv) & 1;
     // float32: scale a.alpha or the learned (scale, offset); float64: the
     // scale a.alpha_d (no learned weights)
     V wa, wb = V(0);
@@ -730,23 +752,78 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
     V B = sub_rn(mul_rn(min2, wa), wb);
     A = A > V(0) ? A : V(0);
     B = B > V(0) ? B : V(0);
-    const auto ua = vbits(A), ub = vbits(B);
-    MASK all;
-    if constexpr (FULL) all = (D >= 8 * (int)sizeof(MASK)) ? ~(MASK)0 : (((MASK)1 << D) - 1);
-    else all = live;
-    const MASK neg = par ? (sv ^ all) : sv;          // message signs
     // the edge holding the first minimum gets min2, every other min1; an
     // edge whose magnitude equals min1 but is not the first one has
     // min2 == min1, so testing |t| == min1 picks the same value
+    if constexpr (BY_VALUE) {
+      // magnitudes with the check's parity in the sign bit
+      const UB psign = pw & SIGN;
+      const UB ua = vbits(A) | psign, ub = vbits(B) | psign;
 #pragma unroll
-    for (int j = 0; j < D; ++j) {
-      bool take2;
-      if constexpr (BY_VALUE) take2 = vabs(t[j]) == min1;
-      else take2 = (uint32_t)j == first;
-      dsmem_st_msg(ad[j], take2 ? ub : ua, (uint32_t)(neg >> j) & 1u);
+      for (int j = 0; j < D; ++j) {
+        const bool take2 = vabs(t[j]) == min1;
+        dsmem_st_bits(ad[j], (take2 ? ub : ua) ^ (vbits(t[j]) & SIGN));
+      }
+    } else {
+      int par;
+      if constexpr (WIDE) par = __popcll((unsigned long long)sv) & 1;
+      else par = __popc((uint32_t)sv) & 1;
+      const auto ua = vbits(A), ub = vbits(B);
+      MASK all;
+      if constexpr (FULL) all = (D >= 8 * (int)sizeof(MASK)) ? ~(MASK)0 : (((MASK)1 << D) - 1);
+      else all = live;
+      const MASK neg = par ? (sv ^ all) : sv;        // message signs
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        dsmem_st_msg(ad[j], (uint32_t)j == first ? ub : ua, (uint32_t)(neg >> j) & 1u);
     }
   }
   return (int)(synw & 1u);
+}
+
+// One light check item (check-phase item wl of this CTA): chunks 0 ..
+// ECHUNK-2 of a row on the unmasked paths where the row allows it, else the
+// masked path; the rows' last chunks packed TAILG rows to a warp.  Returns
+// the lane's syndrome bit (0 without SYN, and for lanes past the tails).
+template <typename V, bool TORCH, int NS, bool SYN, typename MASK>
+__device__ __forceinline__ int qce_light_item(int wl, int nlead, int coff,
+                                              int ntail, const uint2 *rtab,
+                                              const MASK *rinfo, uint32_t lane,
+                                              const uint32_t *bm, uint32_t dummy,
+                                              bool upd, const QceArgs &a, int it) {
+  constexpr int TAILW = EZ - 32 * (ECHUNK - 1);
+  constexpr int TAILG = 32 / TAILW;
+  if (wl < nlead) {                              // chunks 0 .. ECHUNK-2 of a row
+    const int u = wl + coff;
+    const int rl = u / (ECHUNK - 1);
+    const int ch = u - rl * (ECHUNK - 1);
+    const MASK wm = rinfo[3 * rl + 1];
+    const int deg = (int)rinfo[3 * rl + 2];
+    const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
+    if (wm == 0 && deg == NS)
+      return qce_check_item<V, TORCH, NS, true, SYN, MASK>(te, (MASK)0, lane, bm, dummy,
+                                                          upd, a, it);
+    if (wm == 0 && deg == NS - 1)
+      return qce_check_item<V, TORCH, NS - 1, true, SYN, MASK>(te, (MASK)0, lane, bm,
+                                                              dummy, upd, a, it);
+    if constexpr (NS >= 10) {                    // rows two short of the template
+      if (wm == 0 && deg == NS - 2)
+        return qce_check_item<V, TORCH, NS - 2, true, SYN, MASK>(te, (MASK)0, lane, bm,
+                                                                dummy, upd, a, it);
+    }
+    MASK live = rinfo[3 * rl];
+    if (ch == 0 && lane == 0) live &= ~wm;       // check (0, 0): no wrap edge
+    return qce_check_item<V, TORCH, NS, false, SYN, MASK>(te, live, lane, bm, dummy, upd,
+                                                         a, it);
+  }
+  const int t = (wl - nlead) * TAILG + (int)lane / TAILW;   // last chunks
+  const bool valid = t < ntail;
+  const int rl = valid ? t : 0;
+  const uint2 *te = rtab + (rl * ECHUNK + ECHUNK - 1) * NS;
+  const MASK live = valid ? rinfo[3 * rl] : (MASK)0;
+  const int syn = qce_check_item<V, TORCH, NS, false, SYN, MASK>(
+      te, live, lane % TAILW, bm, dummy, upd, a, it);
+  return valid ? syn : 0;
 }
 
 // Heavy rows (more edges than the compile-time slot count; the accumulator
@@ -906,6 +983,9 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const uint32_t sm_sa = smem_u32(smem);
   const uint32_t part_sa = smem_u32(part);
   const uint32_t dummy = part_sa + 40 * 4;   // junk word for masked slots
+  // "an unsatisfied check was seen" flags (2, alternating iterations),
+  // written into every CTA of the cluster by the first warps that see one
+  volatile int *seen = part + 2;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
   // check items g = row*12 + chunk in [c0, c0 + ncitems); rows r0 .. r0+nr-1
@@ -930,6 +1010,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   const int h0 = a.hoff[rank], nhi = HV ? a.hoff[rank + 1] - h0 : 0;
   // this lane's cluster address of CTA `lane`'s bitmap (ballot broadcast)
   const uint32_t bm_peer = lane < CL ? dsmem_map(sm_sa, (uint32_t)lane) : 0u;
+  // this lane's cluster address of CTA `lane`'s seen flags
+  const uint32_t seen_peer = lane < CL ? dsmem_map(part_sa + 8u, (uint32_t)lane) : 0u;
 
   // ---- per-launch tables ---------------------------------------------------
   // row slot (rl, chunk, j): {shared::cluster address of the slot block in
@@ -997,6 +1079,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   if (tid == 0) {
     part[0] = 0;
     part[1] = 0;
+    part[2] = 0;
+    part[3] = 0;
   }
   __syncthreads();
 
@@ -1022,8 +1106,11 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         const bool absent = sub == asub && ((iw.z >> 24) & 1u) && lane == ABSENT_LANE;
         const V li = mv ? lam[iw.y + 32 * sub + lane] : V(0);
         V *col = reinterpret_cast<V *>(smem + iw.x) + 32 * sub + lane;
+        // q = lam - 0; stored as lam + 0 (+0.0 for a -0.0 LLR, which the
+        // check phase's sign-bit tests then read like the reference's v < 0)
+        const V lq = add_rn(li, V(0));
         if (mv)
-          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == wrapi) ? V(-0.0) : li;
+          for (int i = 0; i < d; ++i) col[i * EZ] = (absent && i == wrapi) ? V(-0.0) : lq;
         const uint32_t hb = __ballot_sync(0xffffffffu, mv && li < V(0));
         if (lane < CL) dsmem_st_u32(bm_peer + ((iw.w & 0xFFFFu) + sub) * 4u, hb);
       }
@@ -1034,7 +1121,10 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       const bool upd = it < a.iters;   // the last pass only needs the syndrome
       // the count of the previous iteration has been read by every thread
       // (a barrier ago); its slot is reused two iterations later
-      if (tid == 0 && it > 0) part[(it - 1) & 1] = 0;
+      if (tid == 0 && it > 0) {
+        part[(it - 1) & 1] = 0;
+        part[2 + ((it - 1) & 1)] = 0;
+      }
       // ---------------- check phase ----------------------------------------
       int mybad = 0;
       // Type A with heavy rows: this CTA's heavy items first, one warp each,
@@ -1067,48 +1157,24 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
               make_float4(r.min1, r.min2, __int_as_float(r.first), __uint_as_float(r.bits));
           continue;
         }
+        // Light items form their syndrome bits only while no warp of the
+        // cluster has reported an unsatisfied check in this iteration: once
+        // one has, the iteration's syndrome is known to be nonzero, which is
+        // all an updating iteration needs (the count itself is only output
+        // by the final, update-free pass, which always forms every bit).
+        // Rows of more than 14 slots always form them: a second copy of
+        // their unrolled item code would cost those kernels registers.
         const int wl = w - nhp;
-        const uint2 *te;
-        MASK live;
-        uint32_t el;                               // the lane's check within its chunk
-        bool valid = true;
-        if (wl < nlead) {                          // chunks 0 .. ECHUNK-2 of a row
-          const int u = wl + coff;
-          const int rl = u / (ECHUNK - 1);
-          const int ch = u - rl * (ECHUNK - 1);
-          const MASK wm = rinfo[3 * rl + 1];
-          const int deg = (int)rinfo[3 * rl + 2];
-          te = rtab + (rl * ECHUNK + ch) * NS;
-          if (wm == 0 && deg == NS) {
-            mybad += qce_check_item<V, TORCH, NS, true, MASK>(te, (MASK)0, lane, bm, dummy,
-                                                              upd, a, it);
-            continue;
-          }
-          if (wm == 0 && deg == NS - 1) {
-            mybad += qce_check_item<V, TORCH, NS - 1, true, MASK>(te, (MASK)0, lane, bm, dummy,
-                                                                  upd, a, it);
-            continue;
-          }
-          if constexpr (NS >= 10) {                // rows two short of the template
-            if (wm == 0 && deg == NS - 2) {
-              mybad += qce_check_item<V, TORCH, NS - 2, true, MASK>(te, (MASK)0, lane, bm,
-                                                                    dummy, upd, a, it);
-              continue;
-            }
-          }
-          live = rinfo[3 * rl];
-          if (ch == 0 && lane == 0) live &= ~wm;     // check (0, 0): no wrap edge
-          el = (uint32_t)lane;
-        } else {                                   // last chunks, TAILG rows a warp
-          const int t = (wl - nlead) * TAILG + lane / TAILW;
-          valid = t < ntail;
-          const int rl = valid ? t : 0;
-          te = rtab + (rl * ECHUNK + ECHUNK - 1) * NS;
-          live = valid ? rinfo[3 * rl] : (MASK)0;
-          el = (uint32_t)(lane % TAILW);
+        if (NS > 14 || !upd || seen[it & 1] == 0) {
+          syn = qce_light_item<V, TORCH, NS, true, MASK>(wl, nlead, coff, ntail, rtab, rinfo,
+                                                         (uint32_t)lane, bm, dummy, upd, a, it);
+          mybad += syn;
+          if (NS <= 14 && upd && __any_sync(0xffffffffu, syn != 0) && lane < CL)
+            dsmem_st_u32(seen_peer + (uint32_t)((it & 1) * 4), 1u);
+        } else if constexpr (NS <= 14) {
+          qce_light_item<V, TORCH, NS, false, MASK>(wl, nlead, coff, ntail, rtab, rinfo,
+                                                    (uint32_t)lane, bm, dummy, upd, a, it);
         }
-        syn = qce_check_item<V, TORCH, NS, false, MASK>(te, live, el, bm, dummy, upd, a, it);
-        mybad += valid ? syn : 0;
       }
       if (split) {
         __syncthreads();
@@ -1200,6 +1266,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         if (tid == 0) {
           part[0] = 0;
           part[1] = 0;
+          part[2] = 0;
+          part[3] = 0;
         }
         break;
       }
@@ -1226,8 +1294,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
             V s0 = TORCH ? li0 : V(0), s1 = TORCH ? li1 : V(0);
             s0 = add_rn(add_rn(s0, a0), b0);
             s1 = add_rn(add_rn(s1, a1), b1);
-            t0 = TORCH ? s0 : add_rn(li0, s0);
-            t1 = TORCH ? s1 : add_rn(li1, s1);
+            t0 = TORCH ? add_rn(s0, V(0)) : add_rn(li0, s0);   // no -0.0 (see
+            t1 = TORCH ? add_rn(s1, V(0)) : add_rn(li1, s1);   // qce_var_exact)
             const bool absent = ((iw.z >> 24) & 1u) && lane == ABSENT_LANE;
             if (mv0) {
               col0[0] = sub_rn(t0, a0);
