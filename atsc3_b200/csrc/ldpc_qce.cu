@@ -557,6 +557,7 @@ struct QceArgs {
   const float *wbeta;
   const int8_t *dbucket;
   int wT, wnb;
+  int wrow;          // 1: dbucket is indexed by the check's block row, not its degree
   uint8_t *bits;
   int64_t ld_bits;
   uint8_t *hard;
@@ -670,7 +671,7 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
                                               uint32_t lane,
                                               const uint32_t *bm,
                                               uint32_t dummy, bool upd,
-                                              const QceArgs &a, int it) {
+                                              const QceArgs &a, int it, int row) {
   // per slot: address, remote load (its value is first used by the update
   // below, so the syndrome lookup overlaps its latency), syndrome bit; the
   // syndrome-only final pass loads too (valid addresses, values unused)
@@ -744,7 +745,7 @@ __device__ __forceinline__ int qce_check_item(const uint2 *te, MASK live,
         if constexpr (WIDE) nl = __popcll((unsigned long long)live);
         else nl = __popc((uint32_t)live);
       }
-      const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+      const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + (a.wrow ? row : nl));
       wa = __ldg(a.walpha + wi);
       wb = __ldg(a.wbeta + wi);
     }
@@ -790,7 +791,8 @@ __device__ __forceinline__ int qce_light_item(int wl, int nlead, int coff,
                                               int ntail, const uint2 *rtab,
                                               const MASK *rinfo, uint32_t lane,
                                               const uint32_t *bm, uint32_t dummy,
-                                              bool upd, const QceArgs &a, int it) {
+                                              bool upd, const QceArgs &a, int it,
+                                              int r0) {
   constexpr int TAILW = EZ - 32 * (ECHUNK - 1);
   constexpr int TAILG = 32 / TAILW;
   if (wl < nlead) {                              // chunks 0 .. ECHUNK-2 of a row
@@ -802,19 +804,19 @@ __device__ __forceinline__ int qce_light_item(int wl, int nlead, int coff,
     const uint2 *te = rtab + (rl * ECHUNK + ch) * NS;
     if (wm == 0 && deg == NS)
       return qce_check_item<V, TORCH, NS, true, SYN, MASK>(te, (MASK)0, lane, bm, dummy,
-                                                          upd, a, it);
+                                                          upd, a, it, r0 + rl);
     if (wm == 0 && deg == NS - 1)
       return qce_check_item<V, TORCH, NS - 1, true, SYN, MASK>(te, (MASK)0, lane, bm,
-                                                              dummy, upd, a, it);
+                                                              dummy, upd, a, it, r0 + rl);
     if constexpr (NS >= 10) {                    // rows two short of the template
       if (wm == 0 && deg == NS - 2)
         return qce_check_item<V, TORCH, NS - 2, true, SYN, MASK>(te, (MASK)0, lane, bm,
-                                                                dummy, upd, a, it);
+                                                                dummy, upd, a, it, r0 + rl);
     }
     MASK live = rinfo[3 * rl];
     if (ch == 0 && lane == 0) live &= ~wm;       // check (0, 0): no wrap edge
     return qce_check_item<V, TORCH, NS, false, SYN, MASK>(te, live, lane, bm, dummy, upd,
-                                                         a, it);
+                                                         a, it, r0 + rl);
   }
   const int t = (wl - nlead) * TAILG + (int)lane / TAILW;   // last chunks
   const bool valid = t < ntail;
@@ -822,7 +824,7 @@ __device__ __forceinline__ int qce_light_item(int wl, int nlead, int coff,
   const uint2 *te = rtab + (rl * ECHUNK + ECHUNK - 1) * NS;
   const MASK live = valid ? rinfo[3 * rl] : (MASK)0;
   const int syn = qce_check_item<V, TORCH, NS, false, SYN, MASK>(
-      te, live, lane % TAILW, bm, dummy, upd, a, it);
+      te, live, lane % TAILW, bm, dummy, upd, a, it, r0 + rl);
   return valid ? syn : 0;
 }
 
@@ -907,7 +909,7 @@ template <typename V, bool TORCH>
 __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wrapj,
                                             uint32_t lane, int ch,
                                             const uint32_t *bm, uint32_t dummy,
-                                            bool upd, const QceArgs &a, int it) {
+                                            bool upd, const QceArgs &a, int it, int row) {
   const int k0 = ch * 32 + (int)lane;
   const bool lv = k0 < EZ;
   constexpr uint32_t VB = sizeof(V);
@@ -939,7 +941,7 @@ __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wra
     else wa = a.alpha;
     if (sizeof(V) == 4 && a.walpha) {
       const int nl = deg - ((k0 == 0 && wrapj >= 0) ? 1 : 0);
-      const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+      const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + (a.wrow ? row : nl));
       wa = __ldg(a.walpha + wi);
       wb = __ldg(a.wbeta + wi);
     }
@@ -1142,7 +1144,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           const int row = hi / ECHUNK;
           const int4 hf = hinfo[row];
           mybad += qce_check_heavy<V, TORCH>(htab + hf.x, hf.z, hf.y - 1, (uint32_t)lane,
-                                          hi - row * ECHUNK, bm, dummy, upd, a, it);
+                                          hi - row * ECHUNK, bm, dummy, upd, a, it, row);
           continue;
         }
         if (HV && w < nhp) {
@@ -1167,13 +1169,13 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         const int wl = w - nhp;
         if (NS > 14 || !upd || seen[it & 1] == 0) {
           syn = qce_light_item<V, TORCH, NS, true, MASK>(wl, nlead, coff, ntail, rtab, rinfo,
-                                                         (uint32_t)lane, bm, dummy, upd, a, it);
+                                                         (uint32_t)lane, bm, dummy, upd, a, it, r0);
           mybad += syn;
           if (NS <= 14 && upd && __any_sync(0xffffffffu, syn != 0) && lane < CL)
             dsmem_st_u32(seen_peer + (uint32_t)((it & 1) * 4), 1u);
         } else if constexpr (NS <= 14) {
           qce_light_item<V, TORCH, NS, false, MASK>(wl, nlead, coff, ntail, rtab, rinfo,
-                                                    (uint32_t)lane, bm, dummy, upd, a, it);
+                                                    (uint32_t)lane, bm, dummy, upd, a, it, r0);
         }
       }
       if (split) {
@@ -1209,7 +1211,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
             float wa = a.alpha, wb = 0.f;
             if (a.walpha) {
               const int nl = hf.z - ((k0 == 0 && hf.y > 0) ? 1 : 0);
-              const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + nl);
+              const int wi = min(it, a.wT - 1) * a.wnb + __ldg(a.dbucket + (a.wrow ? row : nl));
               wa = __ldg(a.walpha + wi);
               wb = __ldg(a.wbeta + wi);
             }
@@ -1819,7 +1821,7 @@ static int32_t qce_decode_impl(
     const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
     const int8_t *dbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
     int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
-    int32_t threads, void *stream, bool f64) {
+    int32_t threads, void *stream, bool f64, int wrow = 0) {
   using namespace atsc3;
   ATSC3_ARG(h != nullptr, "null plan");
   const QcePlan &p = h->p;
@@ -1891,6 +1893,7 @@ static int32_t qce_decode_impl(
     a.dbucket = dbucket;
     a.wT = wT;
     a.wnb = wnb;
+    a.wrow = wrow;
   }
   a.bits = bits;
   a.ld_bits = ld_bits;
@@ -1925,6 +1928,21 @@ int32_t atsc3_ldpc_qce_decode_weighted(
   return qce_decode_impl(h, llr, ld_llr, nblk, iters, alpha, semantics, walpha, wbeta,
                          wT, wnb, dbucket, bits, ld_bits, hard, ld_hard, conv, its, bad,
                          threads, stream, false);
+}
+
+int32_t atsc3_ldpc_qce_decode_weighted_rows(
+    const atsc3_ldpc_qce_plan *h, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *rbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream) {
+  using namespace atsc3;
+  ATSC3_ARG(walpha && rbucket, "row weights need walpha and rbucket");
+  ATSC3_ARG(h && h->p.qa + h->p.qb <= 256, "null plan or more than 256 block rows");
+  return qce_decode_impl(h, llr, ld_llr, nblk, iters, alpha, semantics, walpha, wbeta,
+                         wT, wnb, rbucket, bits, ld_bits, hard, ld_hard, conv, its, bad,
+                         threads, stream, false, 1);
 }
 
 int32_t atsc3_ldpc_qce_decode_f64(const atsc3_ldpc_qce_plan *h, const double *llr,

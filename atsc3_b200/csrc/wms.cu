@@ -226,7 +226,7 @@ int32_t atsc3_wms_forward(const int32_t *cptr, const int32_t *cidx,
                           const float *beta, int32_t bf16, void *records,
                           float *tot_out, void *stream) {
   using namespace atsc3;
-  ATSC3_ARG(n > 0 && nc > 0 && ne > 0 && nbucket > 0 && nbucket <= 64, "bad sizes");
+  ATSC3_ARG(n > 0 && nc > 0 && ne > 0 && nbucket > 0 && nbucket <= 127, "bad sizes");
   ATSC3_ARG(iters >= 1 && nblk >= 0, "bad sizes");
   if (nblk == 0) return 0;
   ATSC3_ARG(cptr && cidx && vptr && vedge && vchk && vpos && cbucket && llr &&
@@ -263,7 +263,7 @@ int32_t atsc3_wms_backward(const int32_t *cptr, const int32_t *cidx,
                            float *galpha, float *gbeta, float *work,
                            void *stream) {
   using namespace atsc3;
-  ATSC3_ARG(n > 0 && nc > 0 && ne > 0 && nbucket > 0 && nbucket <= 64, "bad sizes");
+  ATSC3_ARG(n > 0 && nc > 0 && ne > 0 && nbucket > 0 && nbucket <= 127, "bad sizes");
   ATSC3_ARG(iters >= 1 && nblk >= 0, "bad sizes");
   if (nblk == 0) return 0;
   ATSC3_ARG(gtot && galpha && gbeta && work && records, "null pointer");
@@ -280,9 +280,16 @@ int32_t atsc3_wms_backward(const int32_t *cptr, const int32_t *cidx,
     const WmsRec *rp = t > 1 ? rec + (size_t)(t - 2) * per : nullptr;
     wms_var_fwd<<<nblocks((int64_t)nblk * n, 256), 256, 0, st>>>(T, nblk, llr, rp, alpha, beta, t - 1, tot);
     float *gx = (gx_next == gxa) ? gxb : gxa;
-    wms_check_bwd<64><<<nblocks((int64_t)nblk * nc, 256), 256, 0, st>>>(
-        T, nblk, tot, rp, rec + (size_t)(t - 1) * per, alpha, beta, t, gtot,
-        gx_next, gx, galpha, gbeta);
+    // per-CTA gradient partials in shared memory, one entry per bucket
+    // (check degrees: a handful; block rows: up to 127)
+    if (nbucket <= 64)
+      wms_check_bwd<64><<<nblocks((int64_t)nblk * nc, 256), 256, 0, st>>>(
+          T, nblk, tot, rp, rec + (size_t)(t - 1) * per, alpha, beta, t, gtot,
+          gx_next, gx, galpha, gbeta);
+    else
+      wms_check_bwd<128><<<nblocks((int64_t)nblk * nc, 256), 256, 0, st>>>(
+          T, nblk, tot, rp, rec + (size_t)(t - 1) * per, alpha, beta, t, gtot,
+          gx_next, gx, galpha, gbeta);
     // gtot^(t-1): the edges of tot^(t-1) through x^(t)
     wms_var_bwd<<<nblocks((int64_t)nblk * n, 256), 256, 0, st>>>(T, nblk, gx, gtot);
     gx_next = gx;

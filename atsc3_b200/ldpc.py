@@ -211,7 +211,9 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     """Decode (nblk, n) device LLRs.  Returns a dict of device tensors:
     bits (uint8, nblk x n) and/or hard (packed, nblk x ceil(n/32)*4 bytes),
     conv (uint8), its (int32), bad (int32).  weights: optional learned
-    (walpha, wbeta, dbucket) device tensors (quasi-cyclic plans only)."""
+    (walpha, wbeta, dbucket) device tensors (quasi-cyclic plans only), or
+    (walpha, wbeta, rbucket, "row") for weights per block row (the
+    edge-buffer plan only; ``learned.inference_weights``)."""
     torch = _torch()
     want_t = torch.float64 if plan.dtype == "float64" else torch.float32
     if llr.dtype != want_t or llr.device.type != "cuda":
@@ -248,10 +250,15 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     if kind in ("qc", "qce"):
         wa = wb = db = None
         wT = wnb = 0
+        rows = False
         if weights is not None:
-            wa, wb, db = weights
+            wa, wb, db = weights[:3]
+            rows = len(weights) > 3 and weights[3] == "row"
             wT, wnb = wa.shape
+        if rows and kind != "qce":
+            raise ValueError("per-row weights run on the edge-buffer decoder")
         fn = ("atsc3_ldpc_qc_decode_weighted" if kind == "qc"
+              else "atsc3_ldpc_qce_decode_weighted_rows" if rows
               else "atsc3_ldpc_qce_decode_weighted")
         N.call(fn, plan.handle, llr.data_ptr(),
                llr.stride(0), nblk, int(iters), float(alpha),

@@ -32,30 +32,56 @@ def _torch():
     return torch
 
 
+def block_rows(rate, n):
+    """Block row of every check of an A/322 code: accumulator checks
+    r + QA*k (k = 0..359) are row r; a Type A code's identity checks
+    360*QA + (r - QA) + QB*k are row r (QA <= r < QA + QB)."""
+    typ, K, M1, M2, Q1, Q2 = C.ldpc_params(rate, n)
+    nc = n - K
+    c = np.arange(nc)
+    if typ == "A":
+        qa, qb = Q1, Q2
+        return np.where(c < 360 * qa, c % qa,
+                        qa + (c - 360 * qa) % max(qb, 1)).astype(np.int64)
+    return (c % Q2).astype(np.int64)
+
+
 @functools.lru_cache(maxsize=None)
-def host_tables(rate, n):
+def host_tables(rate, n, mode="degree"):
     """CSR tables + per variable-major edge (check, position) + per-check
-    degree bucket.  Buckets = the code's distinct check degrees, ascending."""
+    bucket.  mode "degree": buckets = the code's distinct check degrees,
+    ascending; "row": one bucket per block row (at most 127)."""
     cptr, cidx, vptr, vedge = C.csr(rate, n)
     deg = np.diff(cptr)
     if deg.max() > 32:
         raise ValueError("weighted min-sum serves check degrees <= 32")
     chk = np.repeat(np.arange(len(deg), dtype=np.int32), deg)
     pos = (np.arange(len(cidx)) - cptr[chk]).astype(np.int32)
-    buckets = np.unique(deg)
-    cb = np.searchsorted(buckets, deg).astype(np.int8)
+    if mode == "row":
+        rows = block_rows(rate, n)
+        buckets = np.arange(int(rows.max()) + 1)
+        if len(buckets) > 127:
+            raise ValueError("per-row weights serve codes of at most 127 block rows")
+        cb = rows.astype(np.int8)
+    elif mode == "degree":
+        buckets = np.unique(deg)
+        cb = np.searchsorted(buckets, deg).astype(np.int8)
+    else:
+        raise ValueError(f"unknown bucket mode {mode}")
     return dict(cptr=cptr, cidx=cidx, vptr=vptr, vedge=vedge,
                 vchk=chk[vedge].astype(np.int32), vpos=pos[vedge],
-                cbucket=cb, buckets=buckets, n=n, nc=len(deg), ne=len(cidx))
+                cbucket=cb, buckets=buckets, n=n, nc=len(deg), ne=len(cidx),
+                mode=mode)
 
 
 class WmsCode:
-    """Device copy of host_tables for one code."""
+    """Device copy of host_tables for one code; mode "degree" (weights per
+    iteration and check degree) or "row" (per iteration and block row)."""
 
-    def __init__(self, rate, n, device="cuda"):
+    def __init__(self, rate, n, device="cuda", mode="degree"):
         torch = _torch()
-        h = host_tables(rate, n)
-        self.rate, self.n = rate, n
+        h = host_tables(rate, n, mode)
+        self.rate, self.n, self.mode = rate, n, mode
         self.nc, self.ne = h["nc"], h["ne"]
         self.buckets = h["buckets"]
         self.nbucket = len(self.buckets)
@@ -134,12 +160,12 @@ class WeightedMinSum:
         return cls._F.apply(llr, alpha, beta, code, bf16)
 
 
-def reference_f64(llr, alpha, beta, rate, n):
+def reference_f64(llr, alpha, beta, rate, n, mode="degree"):
     """The weighted min-sum forward in float64 torch ops (CPU), for autograd
     and finite-difference checks.  Same rules as csrc/wms.cu: first-minimum
     arg-min, sign(x) = -1 iff x < 0, relu(alpha*mu - beta)."""
     torch = _torch()
-    h = host_tables(rate, n)
+    h = host_tables(rate, n, mode)
     cptr, cidx = h["cptr"], h["cidx"]
     deg = np.diff(cptr)
     nc, dmax = len(deg), int(deg.max())
@@ -240,7 +266,7 @@ def load_weights(path, device="cuda"):
 
 def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
           channel="awgn", seed=1, bf16=False, log_every=50, resume=None,
-          device="cuda", depths=None):
+          device="cuda", depths=None, mode="degree"):
     """Adam on (alpha, beta) of the unrolled decoder; returns (alpha, beta,
     history).  Fresh seeded blocks every step.  depths: None (the loss is the
     BCE of the output after all `iters` iterations) or a list of unrolled
@@ -248,7 +274,7 @@ def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
     first t rows of the weights), which rewards being right early."""
     torch = _torch()
     from . import synth
-    code = WmsCode(rate, n, device)
+    code = WmsCode(rate, n, device, mode)
     tx = synth.Transmitter(n, mod, rate, device=device)
     alpha, beta = code.init_params(iters)
     start = 0
@@ -280,19 +306,23 @@ def train(rate, n, mod, steps=200, nblk=64, iters=12, lr=0.02, esn0=(0.0, 2.0),
         if step % log_every == 0 or step == start + steps - 1:
             hist.append((step, float(loss.detach())))
     manifest = {"rate": rate, "n": n, "mod": mod, "iters": iters,
-                "buckets": [int(x) for x in code.buckets], "seed": seed,
+                "buckets": [int(x) for x in code.buckets], "mode": mode,
+                "seed": seed,
                 "step": start + steps, "esn0": list(esn0), "channel": channel,
                 "bf16": bool(bf16), "depths": list(depths) if depths else None}
     return alpha.detach(), beta.detach(), hist, manifest
 
 
-def inference_weights(alpha, beta, buckets, device="cuda"):
+def inference_weights(alpha, beta, buckets, device="cuda", mode="degree"):
     """(walpha, wbeta, dbucket) device tensors for the quasi-cyclic decoder:
-    dbucket[degree] = bucket index of that check degree."""
+    dbucket[degree] = bucket index of that check degree; mode "row":
+    (walpha, wbeta, rbucket, "row") with rbucket[block row] = its bucket
+    (the edge-buffer decoder's per-row weights)."""
     torch = _torch()
     db = np.zeros(256, np.int8)          # every check degree the decoders take (<= 250)
     for i, d in enumerate(buckets):
         db[int(d)] = i
-    return (alpha.detach().float().contiguous().to(device),
-            beta.detach().float().contiguous().to(device),
-            torch.from_numpy(db).to(device))
+    w = (alpha.detach().float().contiguous().to(device),
+         beta.detach().float().contiguous().to(device),
+         torch.from_numpy(db).to(device))
+    return w + ("row",) if mode == "row" else w

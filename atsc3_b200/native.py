@@ -83,6 +83,11 @@ SIGNATURES = {
                                                c_vp, c_i32, c_i32, c_vp, c_vp,
                                                c_i64, c_vp, c_i64, c_vp, c_vp,
                                                c_vp, c_i32, c_vp]),
+    "atsc3_ldpc_qce_decode_weighted_rows": (c_i32, [c_vp, c_vp, c_i64, c_i32,
+                                               c_i32, c_f32, c_i32, c_vp,
+                                               c_vp, c_i32, c_i32, c_vp, c_vp,
+                                               c_i64, c_vp, c_i64, c_vp, c_vp,
+                                               c_vp, c_i32, c_vp]),
     "atsc3_ldpc_sp_workspace": (c_i32, [c_i32, c_i32, c_i32, c_vp]),
     "atsc3_ldpc_sp_decode": (c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32,
                                      c_i32, c_vp, c_i64, c_i32, c_i32, c_vp,

@@ -317,6 +317,19 @@ int32_t atsc3_ldpc_qce_decode_weighted(
     int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
     int32_t threads, void *stream);
 
+/* As atsc3_ldpc_qce_decode_weighted with the weights indexed by the check's
+ * block row instead of its degree: the minima of a check of block row r
+ * become relu(min * walpha[i][rbucket[r]] - wbeta[i][rbucket[r]]), i =
+ * min(it, wT - 1); rbucket (>= the code's block rows, at most 256) int8
+ * device array.  No reference counterpart (a learned parameterisation). */
+int32_t atsc3_ldpc_qce_decode_weighted_rows(
+    const atsc3_ldpc_qce_plan *plan, const float *llr, int64_t ld_llr,
+    int32_t nblk, int32_t iters, float alpha, int32_t semantics,
+    const float *walpha, const float *wbeta, int32_t wT, int32_t wnb,
+    const int8_t *rbucket, uint8_t *bits, int64_t ld_bits, uint8_t *hard,
+    int64_t ld_hard, uint8_t *conv, int32_t *its, int32_t *bad,
+    int32_t threads, void *stream);
+
 /* ---- exact sum-product (near-miss rescue) ----------------------------------
  * Float64 log-tanh belief propagation over nblk codewords, replacing
  * lab/m16_margin.py:325-390 sum_product_decode_batch (the rescue
@@ -412,8 +425,9 @@ int32_t atsc3_ldpc_layered_inject_timeout(int32_t layer);
  * Unrolled flooding min-sum with per-iteration, per-check-degree scale and
  * offset: m = sgn * relu(alpha[t][d] * mu - beta[t][d]) (csrc/wms.cu).  No
  * reference counterpart.  Tables: device CSR (cptr, cidx, vptr, vedge), the
- * check and position of each variable-major edge (vchk, vpos), the degree
- * bucket of each check (int8).  records: (iters, nblk, nc) 16-byte per-check
+ * check and position of each variable-major edge (vchk, vpos), the bucket
+ * of each check (int8, at most 127 buckets: its degree class, or its block
+ * row for the per-row parameterisation).  records: (iters, nblk, nc) 16-byte per-check
  * checkpoints written by the forward and read by the backward.  Forward
  * writes tot_out = the posterior after `iters` iterations (no early stop).
  * Backward: gtot in = dL/dtot_out (overwritten), galpha/gbeta accumulate

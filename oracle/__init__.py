@@ -108,7 +108,8 @@ def flood(llr, tables, n, iters=50, alpha=0.75, semantics=0, dtype=np.float32):
     return bits, conv.astype(bool), its, bad
 
 
-def flood_weighted(llr, tables, n, walpha, wbeta, dbucket, iters=50):
+def flood_weighted(llr, tables, n, walpha, wbeta, dbucket, iters=50,
+                   cbucket=None):
     """Weighted flooding min-sum, kernel semantics (lab/ldpc_kernel.c:95-142
     with the check messages of the learned decoder): per iteration t and
     check of degree d, the minima become relu(min * walpha[min(t, T-1),
@@ -117,6 +118,8 @@ def flood_weighted(llr, tables, n, walpha, wbeta, dbucket, iters=50):
     variable sums from +0 in vedge order, then + llr.  numpy float32,
     vectorised per check degree and per variable degree.  With walpha = alpha
     and wbeta = 0 it is ``flood(..., alpha)`` bit for bit (tests pin that).
+    cbucket (optional, one entry per check) replaces dbucket[degree] by a
+    bucket per check (the per-block-row weights).
     Returns (bits, conv bool, its, bad)."""
     cptr, cidx, vptr, vedge = [np.asarray(t, np.int64) for t in tables]
     walpha = np.asarray(walpha, np.float32)
@@ -162,8 +165,12 @@ def flood_weighted(llr, tables, n, walpha, wbeta, dbucket, iters=50):
                 mag2 = mag.copy()
                 mag2[rows, first] = np.inf
                 min2 = mag2.min(axis=1) if d > 1 else np.full(len(cs), np.inf, f32)
-                wa = walpha[ti, dbucket[d]]
-                wb = wbeta[ti, dbucket[d]]
+                if cbucket is None:
+                    wa = walpha[ti, dbucket[d]]
+                    wb = wbeta[ti, dbucket[d]]
+                else:
+                    wa = walpha[ti, np.asarray(cbucket)[cs]]
+                    wb = wbeta[ti, np.asarray(cbucket)[cs]]
                 A = np.maximum(f32(min1 * wa) - wb, f32(0)).astype(f32)
                 B = np.maximum(f32(min2 * wa) - wb, f32(0)).astype(f32)
                 ng = vv < 0

@@ -220,3 +220,70 @@ def test_wms_backward_recomputes_instead_of_storing_messages():
     records = T * code.nc * 16 * nblk
     assert torch.isfinite(a.grad).all() and a.grad.abs().sum() > 0
     assert peak < stored, (peak, stored, records)
+
+
+@pytest.mark.parametrize("rate,n", [("6/15", 64800), ("8/15", 64800),
+                                    ("7/15", 64800), ("3/15", 16200)])
+def test_row_weighted_edge_buffer_vs_weighted_oracle(rate, n):
+    """Learned weights per (iteration, block row) on the edge-buffer decoder
+    against the numpy weighted oracle with the same per-check buckets: Type B
+    codes, Type A 64800 7/15 (its heavy accumulator rows take the split
+    path) and a 16200-bit Type A code."""
+    import torch
+    import oracle
+    from atsc3_b200 import learned as LR
+    from atsc3_b200.ldpc import decode_flood, plan_for
+    tabs = C.csr(rate, n)
+    rows = LR.block_rows(rate, n)
+    nr = int(rows.max()) + 1
+    T = 5
+    rng = np.random.default_rng(n + nr)
+    wa = (0.7 + 0.25 * rng.random((T, nr))).astype(np.float32)
+    wb = (0.15 * rng.random((T, nr))).astype(np.float32)
+    llr = (rng.standard_normal((3, n)) * 1.8 + np.array([[2.4], [1.8], [8.0]])).astype(np.float32)
+    want = oracle.flood_weighted(llr, tabs, n, wa, wb, np.zeros(256, np.int64),
+                                 iters=16, cbucket=rows)
+    w = LR.inference_weights(torch.from_numpy(wa), torch.from_numpy(wb),
+                             np.arange(nr), mode="row")
+    o = decode_flood(plan_for(rate, n, kind="qce"), torch.from_numpy(llr).cuda(),
+                     iters=16, weights=w)
+    assert np.array_equal(o["bits"].cpu().numpy(), want[0])
+    assert o["conv"].cpu().numpy().astype(bool).tolist() == want[1].tolist()
+    assert o["its"].cpu().numpy().tolist() == want[2].tolist()
+    assert o["bad"].cpu().numpy().tolist() == want[3].tolist()
+
+
+def test_row_weighted_training_step_gradients_vs_float64():
+    """The training kernels with one bucket per block row (108 buckets for
+    64800 6/15) against the float64 autograd reference on the same buckets."""
+    import torch
+    from atsc3_b200.learned import WeightedMinSum, WmsCode, bce_loss
+    rate, n, T = "6/15", 64800, 4
+    import oracle
+    pay, cells, s2 = oracle.synth_case(
+        lambda p: oracle.transmit(p, n, "16QAM", rate)[0], 2, C.kpayload(rate, n),
+        C.cells_per_block(n, "16QAM"), 7.0, "awgn", 4)
+    q = oracle.demap(cells, C.points_for("16QAM", rate), 4, s2)
+    lam = oracle.deinterleave(q, C.bicm_map(n, "16QAM", rate), n)
+    cw = oracle.transmit(pay, n, "16QAM", rate)[1]
+    code = WmsCode(rate, n, mode="row")
+    assert code.nbucket == 108
+    rng = np.random.default_rng(6)
+    a0 = (0.7 + 0.2 * rng.random((T, code.nbucket))).astype(np.float32)
+    b0 = (0.1 * rng.random((T, code.nbucket))).astype(np.float32)
+    a = torch.tensor(a0, device="cuda", requires_grad=True)
+    b = torch.tensor(b0, device="cuda", requires_grad=True)
+    loss = bce_loss(WeightedMinSum.apply(torch.from_numpy(lam).cuda(), a, b, code,
+                                         False), torch.from_numpy(cw).cuda())
+    loss.backward()
+    a64 = torch.tensor(a0, dtype=torch.float64, requires_grad=True)
+    b64 = torch.tensor(b0, dtype=torch.float64, requires_grad=True)
+    from atsc3_b200.learned import reference_f64
+    lref = bce_loss(reference_f64(torch.from_numpy(lam), a64, b64, rate, n,
+                                  mode="row"), torch.from_numpy(cw).double())
+    lref.backward()
+    for g, gr in ((a.grad, a64.grad), (b.grad, b64.grad)):
+        g = g.cpu().double().numpy()
+        gr = gr.numpy()
+        rel = np.abs(g - gr).max() / max(np.abs(gr).max(), 1e-12)
+        assert rel < 1e-3, rel

@@ -29,3 +29,26 @@ def test_weighted_oracle_matches_c_oracle(rate, n):
         want = oracle.flood(llr, tabs, n, iters=14, alpha=alpha)
         for g, w in zip(got, want):
             assert np.array_equal(g, w), (rate, n, alpha)
+
+
+def test_row_buckets_with_equal_rows_equal_degree_buckets():
+    """Per-block-row weights whose rows all carry the same (scale, offset)
+    decode exactly like per-degree weights with that value."""
+    from atsc3_b200 import learned as LR
+    rate, n, T = "11/15", 16200, 4
+    tabs = C.csr(rate, n)
+    rng = np.random.default_rng(2)
+    llr = (rng.standard_normal((2, n)) * 2.0 + 2.0).astype(np.float32)
+    rows = LR.block_rows(rate, n)
+    nr = int(rows.max()) + 1
+    a_t = (0.7 + 0.2 * rng.random(T)).astype(np.float32)
+    b_t = (0.1 * rng.random(T)).astype(np.float32)
+    wa_r = np.repeat(a_t[:, None], nr, 1)
+    wb_r = np.repeat(b_t[:, None], nr, 1)
+    db = np.zeros(256, np.int64)
+    got = oracle.flood_weighted(llr, tabs, n, wa_r, wb_r, db, iters=8,
+                                cbucket=rows)
+    want = oracle.flood_weighted(llr, tabs, n, a_t[:, None], b_t[:, None], db,
+                                 iters=8)
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
