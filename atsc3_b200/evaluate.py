@@ -133,7 +133,7 @@ def sweep(rate, mod, weights, esn0s, nblk, n=64800, seed=99, chunk=2000):
 
 
 def run(steps=2000, batch=256, nblk=100000, points=9, out_dir=None, seed=1,
-        iters=12, window=(-0.5, 1.5), tag="", depths=None):
+        iters=12, window=(-0.5, 1.5), tag="", depths=None, mode="degree"):
     """iters: unrolled depth of the training decoder; window: training Es/N0
     range relative to the plain threshold (dB); tag: weights file infix."""
     report = {}
@@ -146,13 +146,13 @@ def run(steps=2000, batch=256, nblk=100000, points=9, out_dir=None, seed=1,
                                      esn0=(thr + window[0], thr + window[1]),
                                      channel="mixed", seed=seed,
                                      log_every=max(1, steps // 10),
-                                     depths=depths)
+                                     depths=depths, mode=mode)
         man["threshold_db"] = thr
         name = f"weights_{tag + '_' if tag else ''}{rate.replace('/', '_')}_{mod}.pt"
         path = os.path.join(out_dir, name)
         LR.save_weights(path, al, be, man)
-        code = LR.WmsCode(rate, 64800)
-        w = LR.inference_weights(al, be, code.buckets)
+        code = LR.WmsCode(rate, 64800, mode=mode)
+        w = LR.inference_weights(al, be, code.buckets, mode=mode)
         lthr = threshold(rate, mod, lo=thr - 3.0, hi=thr, weights=w)
         esn0s = [round(thr - 0.5 + 0.25 * i, 2) for i in range(points)]
         rows = sweep(rate, mod, w, esn0s, nblk // points)
@@ -246,6 +246,149 @@ def compare_decoders(rate, mod, esn0, nblk, weights_path=None, n=64800,
                          for k, (er, it, ms) in acc.items()}}
 
 
+# ---------------------------------------------------------------------------
+# settling the target: thresholds of every decoder and a large sample at the
+# plain decoder's FER 1e-4 point, AWGN and Rayleigh
+# ---------------------------------------------------------------------------
+
+def clopper_pearson(k, n, conf=0.95):
+    """Exact two-sided binomial confidence interval for k events in n."""
+    from scipy.stats import beta
+    a = 1.0 - conf
+    lo = 0.0 if k == 0 else float(beta.ppf(a / 2, k, n - k + 1))
+    hi = 1.0 if k == n else float(beta.ppf(1 - a / 2, k + 1, n - k))
+    return [lo, hi]
+
+
+def load_decoder_weights(path, n=64800):
+    """Inference weights of a saved set (degree or row buckets) + manifest."""
+    al, be, man = LR.load_weights(path)
+    mode = man.get("mode", "degree")
+    code = LR.WmsCode(man["rate"], n, mode=mode)
+    return LR.inference_weights(al, be, code.buckets, mode=mode), man
+
+
+def _decoders(rate, n, weight_sets, alphas=(0.75,), sp=False):
+    """name -> callable(lam) -> device dict with bits, conv, its."""
+    plan = LDPC.plan_for(rate, n)
+    out = {}
+    for a in alphas:
+        out[f"plain alpha {a:g}"] = (lambda lam, a=a: LDPC.decode_flood(
+            plan, lam, iters=50, alpha=a))
+    for name, w in weight_sets.items():
+        out[name] = (lambda lam, w=w: LDPC.decode_flood(
+            plan, lam, iters=50, alpha=0.75, weights=w))
+    if sp:
+        tab = LDPC.sp_tables(C.csr(rate, n), n)
+        out["float64 sum-product"] = (lambda lam: LDPC.sp_decode(
+            tab, lam.double(), iters=50))
+    return out
+
+
+def _errors(o, cw, K):
+    return (o["bits"][:, :K] != cw[:, :K]).any(dim=1) | (o["conv"] == 0)
+
+
+def threshold_of(rate, mod, fn, channel="awgn", n=64800, target=1e-2,
+                 nblk=2000, seed=11, lo=-2.0, hi=24.0, step=0.1, chunk=500):
+    """Lowest Es/N0 (on a `step` grid, bisection in (lo, hi]) at which the
+    decoder `fn` has a block error rate <= target over `nblk` seeded blocks
+    (a wrong information bit or no zero syndrome within 50 iterations)."""
+    torch = _torch()
+    tx = synth.Transmitter(n, mod, rate, device="cuda")
+    K = C.kldpc(rate, n)
+
+    def fer(e):
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        errs = 0
+        for lo_ in range(0, nblk, chunk):
+            lam, cw = blocks(tx, gen, min(chunk, nblk - lo_), e, channel)
+            errs += int(_errors(fn(lam), cw, K).sum())
+        return errs / nblk
+
+    while hi - lo > step + 1e-9:
+        mid = round((lo + hi) / 2 / step) * step
+        if mid <= lo or mid >= hi:
+            break
+        if fer(mid) <= target:
+            hi = mid
+        else:
+            lo = mid
+    return round(hi, 2)
+
+
+def op_eval(rate, mod, esn0, nblk, decoders, channel="awgn", n=64800, seed=7,
+            chunk=2000):
+    """Every decoder on the same `nblk` held-out seeded blocks at one Es/N0:
+    block errors with their 95% Clopper-Pearson interval, mean iterations
+    (a failing block counts 50) and decoded Mbit/s over the decode-only GPU
+    time."""
+    torch = _torch()
+    tx = synth.Transmitter(n, mod, rate, device="cuda")
+    K = C.kldpc(rate, n)
+    kp = C.kpayload(rate, n)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed + int(round(esn0 * 100)) + (0 if channel == "awgn" else 1))
+    acc = {k: [0, 0, 0.0] for k in decoders}
+    for lo in range(0, nblk, chunk):
+        lam, cw = blocks(tx, gen, min(chunk, nblk - lo), esn0, channel)
+        for name, fn in decoders.items():
+            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            e0.record()
+            o = fn(lam)
+            e1.record()
+            err = _errors(o, cw, K)
+            torch.cuda.synchronize()
+            a = acc[name]
+            a[0] += int(err.sum())
+            a[1] += int(o["its"].sum())
+            a[2] += e0.elapsed_time(e1)
+    return {name: {"block_errors": er, "fer": er / nblk,
+                   "fer_cp95": clopper_pearson(er, nblk),
+                   "mean_iters": it / nblk,
+                   "mbit_s": nblk * kp / (ms / 1e3) / 1e6}
+            for name, (er, it, ms) in acc.items()}
+
+
+def settle(rate, mod, weight_paths, channel="awgn", nblk=100000, n=64800,
+           max_points=6):
+    """Thresholds (FER 1e-2, 2000 blocks) of plain min-sum at alpha 0.75,
+    0.85 and 1.0, of each learned set and of the float64 sum-product
+    decoder; then the plain (alpha 0.75) decoder's FER 1e-4 point: from 0.75
+    dB above its threshold in 0.25 dB steps, `nblk` held-out blocks at each
+    point until plain reaches <= 1e-4, with every decoder on the same blocks."""
+    sets, mans = {}, {}
+    for pth in weight_paths:
+        w, man = load_decoder_weights(pth, n)
+        name = f"learned {os.path.basename(pth)}"
+        sets[name], mans[name] = w, man
+    dec = _decoders(rate, n, sets, alphas=(0.75, 0.85, 1.0), sp=True)
+    thr = {name: threshold_of(rate, mod, fn, channel) for name, fn in dec.items()}
+    base = thr["plain alpha 0.75"]
+    evald = {k: v for k, v in dec.items() if k != "float64 sum-product"}
+    points = []
+    for i in range(max_points):
+        e = round(base + 0.75 + 0.25 * i, 2)
+        res = op_eval(rate, mod, e, nblk, evald, channel, n)
+        points.append({"esn0_db": e, "blocks": nblk, "decoders": res})
+        if res["plain alpha 0.75"]["fer"] <= 1e-4:
+            break
+    op = points[-1]
+    plain = op["decoders"]["plain alpha 0.75"]
+    gains = {name: {"iteration_reduction": 1 - r["mean_iters"] / plain["mean_iters"],
+                    "mbit_s_ratio": r["mbit_s"] / plain["mbit_s"]}
+             for name, r in op["decoders"].items() if name.startswith("learned")}
+    return {"rate": rate, "mod": mod, "n": n, "channel": channel,
+            "thresholds_db_fer_1e-2": thr, "points": points,
+            "operating_point_db": op["esn0_db"],
+            "operating_point_reached": plain["fer"] <= 1e-4,
+            "learned_vs_plain_at_op": gains,
+            "weights": {k: {kk: m.get(kk) for kk in ("iters", "esn0", "channel",
+                                                     "step", "mode")}
+                        for k, m in mans.items()}}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
@@ -266,7 +409,20 @@ def main(argv=None):
                          "layered and sum-product decoders at one Es/N0 on "
                          "--blocks held-out blocks")
     ap.add_argument("--weights", default=None, help="weights file for --compare")
+    ap.add_argument("--buckets", default="degree", choices=["degree", "row"],
+                    help="learned parameters per (iteration, check degree) or "
+                         "per (iteration, block row)")
+    ap.add_argument("--settle", nargs="+", metavar="RATE MOD WEIGHTS...",
+                    default=None,
+                    help="thresholds of every decoder and --blocks held-out "
+                         "blocks at the plain decoder's FER 1e-4 point, for "
+                         "one MODCOD and the given weight files")
+    ap.add_argument("--channel", default="awgn", choices=["awgn", "rayleigh"])
     a = ap.parse_args(argv)
+    if a.settle:
+        rate, mod, *paths = a.settle
+        print(json.dumps(settle(rate, mod, paths, a.channel, a.blocks)), flush=True)
+        return
     if a.compare:
         rate, mod, e = a.compare
         print(json.dumps(compare_decoders(rate, mod, float(e), a.blocks,
@@ -274,7 +430,7 @@ def main(argv=None):
         return
     print(json.dumps(run(a.steps, a.batch, a.blocks, a.points, a.out,
                          iters=a.iters, window=tuple(a.window), tag=a.tag,
-                         depths=a.depths)),
+                         depths=a.depths, mode=a.buckets)),
           flush=True)
 
 
