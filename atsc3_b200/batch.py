@@ -70,14 +70,15 @@ def min_cluster(rate, n):
 _QCE = {}
 
 
-def qce_plan(rate, n):
-    """The edge-buffer quasi-cyclic plan of a code (every A/322 code), or
-    None if that decoder does not take it."""
-    key = (rate, n)
+def qce_plan(rate, n, cluster=0):
+    """The edge-buffer quasi-cyclic plan of a code (every A/322 code) at a
+    cluster size (0: the smallest that holds a codeword), or None if that
+    decoder does not take it at that size."""
+    key = (rate, n, cluster)
     if key not in _QCE:
         p = None
         try:
-            p = LDPC.QcePlan(rate, n)
+            p = LDPC.QcePlan(rate, n, cluster=cluster)
         except N.FecError as e:
             if e.rc != -4:
                 raise
@@ -118,6 +119,9 @@ class UnevenBatch:
             self.groups.append((qp[code], first, cnt, code[1]))
             first += cnt
         self.csr_ids = list(range(first, len(user)))
+        # launch shape of each edge-buffer group: (cluster, CTA threads),
+        # (0, 0) = the plan's own choice; autotune() moves them
+        self.gshape = [(0, 0)] * len(self.groups)
         nb = len(self.specs)
         self.nblk = nb
         ncell = [C.cells_per_block(n, m) for n, m, r in self.specs]
@@ -268,7 +272,7 @@ class UnevenBatch:
                    self.hard.data_ptr() + int(self.hard_off[first]),
                    self.hb[first], self.conv.data_ptr() + first,
                    self.its.data_ptr() + 4 * first, self.bad.data_ptr() + 4 * first,
-                   0, gst)
+                   int(self.gshape[gi][1]), gst)
         if self.ncsr:
             cst = self.side[-1].cuda_stream if (main is not None and self.groups) else st
             N.call("atsc3_ldpc_batch_decode", self.desc.data_ptr(), self.cluster,
@@ -305,40 +309,91 @@ class UnevenBatch:
             self.capture()
         self.graph.replay()
 
+    def set_group_shape(self, gi, cluster, threads):
+        """Launch shape of edge-buffer group gi: cluster size (0 = the
+        smallest that holds a codeword) and CTA threads (0 = default, 512 or
+        1024).  Raises FecError (-4) when the code does not fit that shape."""
+        plan, first, cnt, n = self.groups[gi]
+        rate = self.specs[first][2]
+        p = qce_plan(rate, n, cluster)
+        if p is None:
+            raise N.FecError("atsc3_ldpc_qce_plan_create2", -4,
+                             f"{n} {rate} does not fit {cluster} CTAs")
+        self.groups[gi] = (p, first, cnt, n)
+        self.gshape[gi] = (cluster, threads)
+        self.graph = None
+
+    def _time(self, reps):
+        torch = _torch()
+        self.capture()
+        self.graph.replay()
+        torch.cuda.synchronize(self.dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            self.graph.replay()
+        e1.record()
+        torch.cuda.synchronize(self.dev)
+        return e0.elapsed_time(e1) / reps
+
     def signature(self):
         return (tuple(sorted(self.specs)), self.iters, len(self.groups))
 
-    def autotune(self, reps=3, clusters=None, threads=(512, 1024)):
-        """Time the captured graph for each (cluster, threads) and keep the
-        fastest; returns the table of timings (ms)."""
+    def autotune(self, reps=3, clusters=None, threads=(512, 1024), shapes=None):
+        """Time the captured graph over the launch knobs and keep the
+        fastest; returns the table of timings (ms), keyed ("csr", cluster,
+        threads) for the persistent CSR launch and (code, cluster, threads)
+        for each edge-buffer group.  The CSR launch (when it has blocks) is
+        swept over cluster x threads; then each edge-buffer group, most edges
+        first, over its cluster size (the smallest that holds a codeword and
+        the next two) x threads with the others fixed (coordinate descent).
+        Results are cached per batch signature."""
         torch = _torch()
         key = self.signature()
         if key in _TUNED:
-            best = _TUNED[key][0]
-            self.set_config(*best)
-            return _TUNED[key][1]
-        clusters = clusters or [c for c in (1, 2, 4, 8, 16) if c >= self.cl_min]
+            (csr_best, gbest), table = _TUNED[key]
+            self.set_config(*csr_best)
+            for gi, shp in enumerate(gbest):
+                self.set_group_shape(gi, *shp)
+            self.capture()
+            return table
         table = {}
-        for cl in clusters:
-            for th in threads:
+        if self.ncsr:
+            clusters = clusters or [c for c in (1, 2, 4, 8, 16) if c >= self.cl_min]
+            for cl in clusters:
+                for th in threads:
+                    try:
+                        self.set_config(cl, th)
+                        table[("csr", cl, th)] = self._time(reps)
+                    except N.FecError:
+                        continue
+            best = min((k for k in table if k[0] == "csr"), key=table.get)
+            self.set_config(best[1], best[2])
+        csr_best = (self.cluster, self.threads)
+        base = self._time(reps)
+        order = sorted(range(len(self.groups)),
+                       key=lambda g: -self.groups[g][2] * self.groups[g][3])
+        for gi in order:
+            plan, first, cnt, n = self.groups[gi]
+            code = f"{n} {self.specs[first][2]}"
+            c0 = int(plan.info["cluster"])
+            cur = self.gshape[gi]
+            cands = shapes or [(c, t) for c in (c0, c0 + 1, c0 + 2)
+                               for t in threads]
+            best_t, best_s = base, cur
+            for cl, th in cands:
                 try:
-                    self.set_config(cl, th)
-                    self.capture()
+                    self.set_group_shape(gi, cl, th)
+                    t = self._time(reps)
                 except N.FecError:
                     continue
-                self.graph.replay()
-                torch.cuda.synchronize(self.dev)
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(reps):
-                    self.graph.replay()
-                e1.record()
-                torch.cuda.synchronize(self.dev)
-                table[(cl, th)] = e0.elapsed_time(e1) / reps
-        best = min(table, key=table.get)
-        _TUNED[key] = (best, table)
-        self.set_config(*best)
+                table[(code, cl, th)] = t
+                if t < best_t:
+                    best_t, best_s = t, (cl, th)
+            self.set_group_shape(gi, *best_s)
+            base = best_t
+        _TUNED[key] = ((csr_best, list(self.gshape)), table)
         self.capture()
         return table
 

@@ -813,10 +813,21 @@ def run_uneven(args):
     # per-code edge-buffer launches (every A/322 code) beside the CSR queue
     ub = UnevenBatch(specs, iters=ITERS, alpha=ALPHA)
     ub.load(cells, s2s)
+    ms_default = timed(ub)
     table = ub.autotune(reps=2)
     ms = timed(ub)
-    bits = sum(C.kpayload(r, n) for n, m, r in specs)
+    tuned_shapes = {f"{ub.groups[g][3]} {ub.specs[ub.groups[g][1]][2]}": list(ub.gshape[g])
+                    for g in range(len(ub.groups))}
     res = ub.results()
+    # every code on one shared launch shape (the largest cluster any code
+    # needs, 512 threads: what one launch over all codes would have to use)
+    cl_all = max(int(g[0].info["cluster"]) for g in ub.groups) if ub.groups else 0
+    ms_shared = None
+    if ub.groups:
+        for g in range(len(ub.groups)):
+            ub.set_group_shape(g, cl_all, 512)
+        ms_shared = timed(ub)
+    bits = sum(C.kpayload(r, n) for n, m, r in specs)
     # per-MODCOD sequential launches (eager)
     groups = {}
     for b, sp in enumerate(specs):
@@ -844,7 +855,11 @@ def run_uneven(args):
             "sequential_mbit_s": bits / (ms_seq / 1e3) / 1e6,
             "sequential_ms_per_step": ms_seq, "speedup_vs_sequential": ms_seq / ms,
             "blocks": len(specs), "distinct_modcods": len(groups),
-            "autotune_ms": {f"cl{k[0]}_t{k[1]}": v for k, v in table.items()},
+            "untuned_mbit_s": bits / (ms_default / 1e3) / 1e6,
+            "shared_shape_mbit_s": (bits / (ms_shared / 1e3) / 1e6) if ms_shared else None,
+            "shared_shape": {"cluster": cl_all, "threads": 512},
+            "tuned_shapes": tuned_shapes,
+            "autotune_ms": {f"{k[0]} cl{k[1]} t{k[2]}": v for k, v in table.items()},
             "config": ub.config,
             "bch_ok": int(sum(r["ok"] for r in res)),
             "mean_iters": float(np.mean([r["its"] for r in res])),
