@@ -253,37 +253,73 @@ def test_row_weighted_edge_buffer_vs_weighted_oracle(rate, n):
     assert o["bad"].cpu().numpy().tolist() == want[3].tolist()
 
 
-def test_row_weighted_training_step_gradients_vs_float64():
+def test_row_weighted_training_step_gradients():
     """The training kernels with one bucket per block row (108 buckets for
-    64800 6/15) against the float64 autograd reference on the same buckets."""
+    64800 6/15).  Exact: with every row carrying its degree's (scale,
+    offset), the forward is the degree-bucket forward, so the row gradients
+    summed over each degree class equal the degree-bucket gradients of the
+    same launch (only the reduction buckets differ; row 0 holds the one
+    degree-6 check, missing its wrap edge, and 359 degree-7 checks).  And
+    against the float64 autograd reference on the same row buckets (1e-2 of
+    the largest entry; measured 3.3e-3: with 720 checks per parameter a
+    first/second-minimum choice that float32 and float64 make differently
+    weighs more than with degree buckets)."""
     import torch
-    from atsc3_b200.learned import WeightedMinSum, WmsCode, bce_loss
-    rate, n, T = "6/15", 64800, 4
     import oracle
+    from atsc3_b200 import learned as LR
+    from atsc3_b200.learned import WeightedMinSum, WmsCode, bce_loss, reference_f64
+    rate, n, T = "6/15", 64800, 4
     pay, cells, s2 = oracle.synth_case(
         lambda p: oracle.transmit(p, n, "16QAM", rate)[0], 2, C.kpayload(rate, n),
         C.cells_per_block(n, "16QAM"), 7.0, "awgn", 4)
     q = oracle.demap(cells, C.points_for("16QAM", rate), 4, s2)
     lam = oracle.deinterleave(q, C.bicm_map(n, "16QAM", rate), n)
     cw = oracle.transmit(pay, n, "16QAM", rate)[1]
-    code = WmsCode(rate, n, mode="row")
-    assert code.nbucket == 108
+    x = torch.from_numpy(lam).cuda()
+    bits = torch.from_numpy(cw).cuda()
+    rcode = WmsCode(rate, n, mode="row")
+    dcode = WmsCode(rate, n)
+    assert rcode.nbucket == 108 and list(dcode.buckets) == [6, 7, 8]
     rng = np.random.default_rng(6)
-    a0 = (0.7 + 0.2 * rng.random((T, code.nbucket))).astype(np.float32)
-    b0 = (0.1 * rng.random((T, code.nbucket))).astype(np.float32)
+    ad = (0.7 + 0.2 * rng.random((T, 3))).astype(np.float32)
+    bd = (0.1 * rng.random((T, 3))).astype(np.float32)
+    # each row's degree class (all 360 checks of a row share it, but row 0's
+    # check 0, which lacks the wrap edge)
+    cptr = C.csr(rate, n)[0]
+    deg = np.diff(cptr)
+    rows = LR.block_rows(rate, n)
+    rdeg = np.array([np.bincount(deg[rows == r]).argmax() for r in range(108)])
+    cls = np.searchsorted(dcode.buckets, rdeg)
+    assert deg[0] == 6 and rows[0] == 0 and rdeg[0] == 7
+    ga = {}
+    for mode, code, a0, b0 in (("row", rcode, ad[:, cls], bd[:, cls]),
+                               ("degree", dcode, ad, bd)):
+        # the degree-6 check has its own bucket; give it row 0's values
+        if mode == "degree":
+            a0 = a0.copy(); b0 = b0.copy()
+            a0[:, 0] = a0[:, 1]; b0[:, 0] = b0[:, 1]
+        a = torch.tensor(a0, device="cuda", requires_grad=True)
+        b = torch.tensor(b0, device="cuda", requires_grad=True)
+        bce_loss(WeightedMinSum.apply(x, a, b, code, False), bits).backward()
+        ga[mode] = (a.grad.double().cpu().numpy(), b.grad.double().cpu().numpy())
+    for k in range(2):
+        gr, gd = ga["row"][k], ga["degree"][k]
+        for c in (1, 2):                     # degree 7 (+ the degree-6 check), 8
+            want = gd[:, c] + (gd[:, 0] if c == 1 else 0.0)
+            got = gr[:, cls == c].sum(axis=1)
+            assert np.allclose(got, want, rtol=1e-4, atol=1e-9), (k, c, got, want)
+    # against the float64 reference with distinct per-row values
+    a0 = (0.7 + 0.2 * rng.random((T, 108))).astype(np.float32)
+    b0 = (0.1 * rng.random((T, 108))).astype(np.float32)
     a = torch.tensor(a0, device="cuda", requires_grad=True)
     b = torch.tensor(b0, device="cuda", requires_grad=True)
-    loss = bce_loss(WeightedMinSum.apply(torch.from_numpy(lam).cuda(), a, b, code,
-                                         False), torch.from_numpy(cw).cuda())
-    loss.backward()
+    bce_loss(WeightedMinSum.apply(x, a, b, rcode, False), bits).backward()
     a64 = torch.tensor(a0, dtype=torch.float64, requires_grad=True)
     b64 = torch.tensor(b0, dtype=torch.float64, requires_grad=True)
-    from atsc3_b200.learned import reference_f64
-    lref = bce_loss(reference_f64(torch.from_numpy(lam), a64, b64, rate, n,
-                                  mode="row"), torch.from_numpy(cw).double())
-    lref.backward()
+    bce_loss(reference_f64(torch.from_numpy(lam), a64, b64, rate, n, mode="row"),
+             torch.from_numpy(cw).double()).backward()
     for g, gr in ((a.grad, a64.grad), (b.grad, b64.grad)):
         g = g.cpu().double().numpy()
         gr = gr.numpy()
         rel = np.abs(g - gr).max() / max(np.abs(gr).max(), 1e-12)
-        assert rel < 1e-3, rel
+        assert rel < 1e-2, rel
