@@ -63,7 +63,6 @@ constexpr int EZ = 360;
 constexpr int ECHUNK = 12;                // ceil(360 / 32) warps per row/column
 constexpr int EMAXCL = 16;
 constexpr int EWRAP = 1 << 8;
-constexpr int ESLOT = EZ * 4;             // bytes of one float32 circulant slot
 constexpr int EPART = 256;                // syndrome exchange bytes
 
 // Compile-time slot counts per block row (NS >= the code's largest block-row
@@ -1097,10 +1096,10 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
     for (int w = warp; w < nvitems; w += nwarps) {
       const uint4 iw = itab[w];
       const int d = (int)(iw.z & 0xFFu);
-#pragma unroll
       // the absent entry: bit 359 = lane 7 of the item's last sub-chunk
       const int asub = ((iw.z >> 16) & 0xFFu) ? 1 : 0;
       const int wrapi = (int)(iw.w >> 24);
+#pragma unroll
       for (int sub = 0; sub < 2; ++sub) {
         const uint32_t nval = (iw.z >> (8 + 8 * sub)) & 0xFFu;
         if (nval == 0) break;                         // 32-bit item
