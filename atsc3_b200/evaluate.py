@@ -285,15 +285,31 @@ def _decoders(rate, n, weight_sets, alphas=(0.75,), sp=False):
     return out
 
 
-def _errors(o, cw, K):
-    return (o["bits"][:, :K] != cw[:, :K]).any(dim=1) | (o["conv"] == 0)
+def _errors(o, cw, K, n, arbiter="bch"):
+    """Block errors of one decode: a wrong information bit, or (arbiter
+    "bch", the judge the evaluation names) a nonzero BCH syndrome of the
+    K_ldpc decoded bits, or (arbiter "conv", the reference receiver's
+    delivery rule: lab/m44_ldm.py:2380-2382 drops a block whose LDPC did not
+    converge) no zero LDPC syndrome within the iteration cap."""
+    torch = _torch()
+    wrong = (o["bits"][:, :K] != cw[:, :K]).any(dim=1)
+    if arbiter == "conv":
+        return wrong | (o["conv"] == 0)
+    bits = o["bits"]
+    nblk = bits.shape[0]
+    syn = torch.empty((nblk, 6), dtype=torch.int32, device=bits.device)
+    N.call("atsc3_bch_syndrome_bits", bits.data_ptr(), bits.stride(0), nblk, K,
+           BCH.device_rtab(K, n, bits.device).data_ptr(), syn.data_ptr(),
+           torch.cuda.current_stream(bits.device).cuda_stream)
+    return wrong | (syn != 0).any(dim=1)
 
 
 def threshold_of(rate, mod, fn, channel="awgn", n=64800, target=1e-2,
-                 nblk=2000, seed=11, lo=-2.0, hi=24.0, step=0.1, chunk=500):
+                 nblk=2000, seed=11, lo=-2.0, hi=24.0, step=0.1, chunk=500,
+                 arbiter="bch"):
     """Lowest Es/N0 (on a `step` grid, bisection in (lo, hi]) at which the
     decoder `fn` has a block error rate <= target over `nblk` seeded blocks
-    (a wrong information bit or no zero syndrome within 50 iterations)."""
+    (errors as `_errors` counts them)."""
     torch = _torch()
     tx = synth.Transmitter(n, mod, rate, device="cuda")
     K = C.kldpc(rate, n)
@@ -304,7 +320,7 @@ def threshold_of(rate, mod, fn, channel="awgn", n=64800, target=1e-2,
         errs = 0
         for lo_ in range(0, nblk, chunk):
             lam, cw = blocks(tx, gen, min(chunk, nblk - lo_), e, channel)
-            errs += int(_errors(fn(lam), cw, K).sum())
+            errs += int(_errors(fn(lam), cw, K, n, arbiter).sum())
         return errs / nblk
 
     while hi - lo > step + 1e-9:
@@ -319,7 +335,7 @@ def threshold_of(rate, mod, fn, channel="awgn", n=64800, target=1e-2,
 
 
 def op_eval(rate, mod, esn0, nblk, decoders, channel="awgn", n=64800, seed=7,
-            chunk=2000):
+            chunk=2000, arbiter="bch"):
     """Every decoder on the same `nblk` held-out seeded blocks at one Es/N0:
     block errors with their 95% Clopper-Pearson interval, mean iterations
     (a failing block counts 50) and decoded Mbit/s over the decode-only GPU
@@ -338,7 +354,7 @@ def op_eval(rate, mod, esn0, nblk, decoders, channel="awgn", n=64800, seed=7,
             e0.record()
             o = fn(lam)
             e1.record()
-            err = _errors(o, cw, K)
+            err = _errors(o, cw, K, n, arbiter)
             torch.cuda.synchronize()
             a = acc[name]
             a[0] += int(err.sum())
@@ -352,25 +368,27 @@ def op_eval(rate, mod, esn0, nblk, decoders, channel="awgn", n=64800, seed=7,
 
 
 def settle(rate, mod, weight_paths, channel="awgn", nblk=100000, n=64800,
-           max_points=6):
+           max_points=8, arbiter="bch", start=0.25):
     """Thresholds (FER 1e-2, 2000 blocks) of plain min-sum at alpha 0.75,
     0.85 and 1.0, of each learned set and of the float64 sum-product
-    decoder; then the plain (alpha 0.75) decoder's FER 1e-4 point: from 0.75
-    dB above its threshold in 0.25 dB steps, `nblk` held-out blocks at each
-    point until plain reaches <= 1e-4, with every decoder on the same blocks."""
+    decoder; then the plain (alpha 0.75) decoder's FER 1e-4 point: from
+    `start` dB above its threshold in 0.25 dB steps, `nblk` held-out blocks at
+    each point until plain reaches <= 1e-4, with every decoder on the same
+    blocks.  Block errors as `_errors` counts them under `arbiter`."""
     sets, mans = {}, {}
     for pth in weight_paths:
         w, man = load_decoder_weights(pth, n)
         name = f"learned {os.path.basename(pth)}"
         sets[name], mans[name] = w, man
     dec = _decoders(rate, n, sets, alphas=(0.75, 0.85, 1.0), sp=True)
-    thr = {name: threshold_of(rate, mod, fn, channel) for name, fn in dec.items()}
+    thr = {name: threshold_of(rate, mod, fn, channel, arbiter=arbiter)
+           for name, fn in dec.items()}
     base = thr["plain alpha 0.75"]
     evald = {k: v for k, v in dec.items() if k != "float64 sum-product"}
     points = []
     for i in range(max_points):
-        e = round(base + 0.75 + 0.25 * i, 2)
-        res = op_eval(rate, mod, e, nblk, evald, channel, n)
+        e = round(base + start + 0.25 * i, 2)
+        res = op_eval(rate, mod, e, nblk, evald, channel, n, arbiter=arbiter)
         points.append({"esn0_db": e, "blocks": nblk, "decoders": res})
         if res["plain alpha 0.75"]["fer"] <= 1e-4:
             break
@@ -380,7 +398,7 @@ def settle(rate, mod, weight_paths, channel="awgn", nblk=100000, n=64800,
                     "mbit_s_ratio": r["mbit_s"] / plain["mbit_s"]}
              for name, r in op["decoders"].items() if name.startswith("learned")}
     return {"rate": rate, "mod": mod, "n": n, "channel": channel,
-            "thresholds_db_fer_1e-2": thr, "points": points,
+            "arbiter": arbiter, "thresholds_db_fer_1e-2": thr, "points": points,
             "operating_point_db": op["esn0_db"],
             "operating_point_reached": plain["fer"] <= 1e-4,
             "learned_vs_plain_at_op": gains,
@@ -418,10 +436,16 @@ def main(argv=None):
                          "blocks at the plain decoder's FER 1e-4 point, for "
                          "one MODCOD and the given weight files")
     ap.add_argument("--channel", default="awgn", choices=["awgn", "rayleigh"])
+    ap.add_argument("--arbiter", default="bch", choices=["bch", "conv"],
+                    help="--settle block errors: BCH syndrome (default) or no "
+                         "LDPC convergence (the receiver's delivery rule)")
+    ap.add_argument("--start", type=float, default=0.25,
+                    help="--settle: first point above the plain threshold (dB)")
     a = ap.parse_args(argv)
     if a.settle:
         rate, mod, *paths = a.settle
-        print(json.dumps(settle(rate, mod, paths, a.channel, a.blocks)), flush=True)
+        print(json.dumps(settle(rate, mod, paths, a.channel, a.blocks,
+                                arbiter=a.arbiter, start=a.start)), flush=True)
         return
     if a.compare:
         rate, mod, e = a.compare
