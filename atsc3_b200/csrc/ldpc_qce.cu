@@ -64,6 +64,7 @@ constexpr int ECHUNK = 12;                // ceil(360 / 32) warps per row/column
 constexpr int EMAXCL = 16;
 constexpr int EWRAP = 1 << 8;
 constexpr int EPART = 256;                // syndrome exchange bytes
+constexpr int QBINS = 32;                 // variable-item bins per CTA (one per warp at 1024 threads)
 
 // Compile-time slot counts per block row (NS >= the code's largest block-row
 // degree; rows with fewer edges mask the rest) (the kernel templates).
@@ -94,11 +95,13 @@ struct QcePlan {
   int nhrows = 0;               // heavy rows (the accumulator rows) or 0
   int hsplit = 1;               // parts per heavy item (warps sharing it)
   int hpb_off = 0;              // shared-memory offset of the heavy partials
+  int vbin_lo = 0, vbin_hi = 0; // least / most loaded variable-item bin (estimated cost)
   int ib[EMAXCL + 1] = {0};     // variable-phase items of CTA c in d_itab
   int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
   int32_t *d_ccols = nullptr;   // (nb) columns grouped by owner CTA
   int4 *d_itab = nullptr;       // variable-phase items, grouped by CTA
+  int32_t *d_wbin = nullptr;    // (cluster, QBINS+1) bin offsets into each CTA's items
   int32_t *d_rptr = nullptr;    // (Q+1)
   int4 *d_cdesc = nullptr;      // per column
   uint8_t *d_s0 = nullptr;      // (nb*360) rotation start (zone A / only zone)
@@ -125,6 +128,7 @@ struct QceTables {
   std::vector<int4> cdesc;
   std::vector<int32_t> ccols;
   std::vector<int4> itab;
+  std::vector<int32_t> wbin;    // (cluster, QBINS+1) bin offsets, relative to ib[c]
   std::vector<uint8_t> s0, s0b;
   std::vector<int16_t> hitems;
 };
@@ -500,8 +504,12 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
   // << 16 | absent wrap entry << 24 | mode << 25, bitmap word of sub-chunk 0
   // | zone-A slots << 16 | wrap slot << 24 (0xFF: none)}
   t->itab.clear();
+  t->wbin.assign((size_t)cluster * (QBINS + 1), 0);
   p->ib[0] = 0;
+  p->vbin_lo = 1 << 30;
+  p->vbin_hi = 0;
   for (int c = 0; c < cluster; ++c) {
+    std::vector<int4> items;
     for (int q = p->cb[c]; q < p->cb[c + 1]; ++q) {
       const int g = t->ccols[q];
       const int d = (int)cols[g].size();
@@ -513,12 +521,43 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
         const int absent = (wrap >= 0 && mm0 + step >= EZ) ? 1 : 0;
         const uint32_t w = (uint32_t)(g * ECHUNK + mm0 / 32) | ((uint32_t)dzA[g] << 16) |
                            ((wrap >= 0 ? (uint32_t)wrap : VNOWRAP) << 24);
-        t->itab.push_back(make_int4(base[g] + vb * mm0, g * EZ + mm0,
-                                    d | (v0 << 8) | (v1 << 16) | (absent << 24) |
-                                        (vmode[g] << 25),
-                                    (int)w));
+        items.push_back(make_int4(base[g] + vb * mm0, g * EZ + mm0,
+                                  d | (v0 << 8) | (v1 << 16) | (absent << 24) |
+                                      (vmode[g] << 25),
+                                  (int)w));
       }
     }
+    // Deal the CTA's items to QBINS bins, the most expensive first, each to
+    // the least-loaded bin (longest-processing-time rule), so that every
+    // warp walking its own bin has about the same work; a bin keeps its
+    // items in column order.  Estimated cost (instructions per item):
+    // pair 44, 1-4 slots in registers 20 + 2 d (d + 3), any slots 30 + 7 d
+    // (two zones: 40 + 7 d).
+    std::vector<int> cost(items.size()), order(items.size());
+    for (size_t i = 0; i < items.size(); ++i) {
+      const int d = items[i].z & 0xFF, mode = (items[i].z >> 25) & 3;
+      cost[i] = mode == VM_PAIR ? 44 : mode == VM_EXACT ? 20 + 2 * d * (d + 3)
+              : mode == VM_GEN ? 30 + 7 * d : 40 + 7 * d;
+      order[i] = (int)i;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<std::vector<int>> bins(QBINS);
+    std::vector<int> load(QBINS, 0);
+    for (int i : order) {
+      const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      bins[b].push_back(i);
+      load[b] += cost[i];
+    }
+    const int first = (int)t->itab.size();
+    for (int b = 0; b < QBINS; ++b) {
+      std::sort(bins[b].begin(), bins[b].end());
+      t->wbin[(size_t)c * (QBINS + 1) + b] = (int)t->itab.size() - first;
+      for (int i : bins[b]) t->itab.push_back(items[i]);
+      p->vbin_lo = std::min(p->vbin_lo, load[b]);
+      p->vbin_hi = std::max(p->vbin_hi, load[b]);
+    }
+    t->wbin[(size_t)c * (QBINS + 1) + QBINS] = (int)t->itab.size() - first;
     p->ib[c + 1] = (int)t->itab.size();
   }
   for (int c = cluster + 1; c <= EMAXCL; ++c) p->ib[c] = p->ib[cluster];
@@ -544,6 +583,7 @@ struct QceArgs {
   const int16_t *hitems;
   const int32_t *ccols;
   const int4 *itab;
+  const int32_t *wbin;          // (cluster, QBINS+1) item-bin offsets per CTA
   const int4 *rdesc;
   const int32_t *rptr;
   const int4 *cdesc;
@@ -1072,7 +1112,11 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       rinfo[3 * rl + 2] = (MASK)deg;
     }
   }
-  // variable-phase items of this CTA (built on the host)
+  // variable-phase items of this CTA (built on the host), and the bins the
+  // host dealt them into (part[4 .. 4 + QBINS]): warp w walks bins
+  // w*bpw .. (w+1)*bpw - 1, contiguous in the item list
+  int *vbin = part + 4;
+  for (int q = tid; q <= QBINS; q += blockDim.x) vbin[q] = __ldg(a.wbin + rank * (QBINS + 1) + q);
   for (int q = tid; q < nvitems; q += blockDim.x) {
     const int4 v = __ldg(a.itab + i0 + q);
     itab[q] = make_uint4((uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z, (uint32_t)v.w);
@@ -1088,12 +1132,18 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   // the absent wrap entry (last parity column, bit 359, its wrap slot) is
   // lane 7 of sub-chunk 1 of that column's last item, slot 1 of the column
   constexpr int ABSENT_LANE = EZ - 32 * (ECHUNK - 1) - 1;
+  // this warp's variable items: bins warp*BPW .. (warp+1)*BPW - 1 (NT is
+  // 512 or 1024), their offsets read from shared memory at each phase
+  // (volatile: not kept in registers across the codeword loop)
+  constexpr int BPW = QBINS / (NT / 32);
+  static_assert(BPW >= 1 && QBINS % (NT / 32) == 0, "512 or 1024 threads");
 
   for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
     const V *lam = reinterpret_cast<const V *>(a.llr) + (size_t)b * a.ld_llr;
     // ---- prologue: q = lam - 0 = lam on every slot, hard bits of lam; the
     // absent entry holds -0.0 (adding it is exact) ---------------------------
-    for (int w = warp; w < nvitems; w += nwarps) {
+    for (int w = ((volatile int *)part)[4 + warp * BPW],
+             we = ((volatile int *)part)[4 + (warp + 1) * BPW]; w < we; ++w) {
       const uint4 iw = itab[w];
       const int d = (int)(iw.z & 0xFFu);
       // the absent entry: bit 359 = lane 7 of the item's last sub-chunk
@@ -1273,7 +1323,8 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         break;
       }
       // ---------------- variable phase (local) -----------------------------
-      for (int w = warp; w < nvitems; w += nwarps) {
+      for (int w = ((volatile int *)part)[4 + warp * BPW],
+               we = ((volatile int *)part)[4 + (warp + 1) * BPW]; w < we; ++w) {
         const uint4 iw = itab[w];
         const int d = (int)(iw.z & 0xFFu);
         const int mode = (int)((iw.z >> 25) & 3u);
@@ -1545,6 +1596,7 @@ static int32_t qce_plan_create_vb(int32_t n, int32_t kldpc, int32_t qa, int32_t 
   if (e == cudaSuccess) e = up((void **)&h->p.d_cdesc, t.cdesc.data(), t.cdesc.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_ccols, t.ccols.data(), t.ccols.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_itab, t.itab.data(), t.itab.size() * 16);
+  if (e == cudaSuccess) e = up((void **)&h->p.d_wbin, t.wbin.data(), t.wbin.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0b, t.s0b.data(), t.s0b.size());
   if (e == cudaSuccess)
@@ -1584,6 +1636,7 @@ void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
   cudaFree(h->p.d_cdesc);
   cudaFree(h->p.d_ccols);
   cudaFree(h->p.d_itab);
+  cudaFree(h->p.d_wbin);
   cudaFree(h->p.d_s0);
   cudaFree(h->p.d_s0b);
   cudaFree(h->p.d_hitems);
@@ -1637,6 +1690,8 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
   meta[61] = (int32_t)t.itab.size();
   for (int c = 0; c <= EMAXCL; ++c) meta[62 + c] = p.hoff[c];
   meta[79] = p.nhrows;
+  meta[80] = p.vbin_lo;
+  meta[81] = p.vbin_hi;
   if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
@@ -1878,6 +1933,7 @@ static int32_t qce_decode_impl(
   a.hitems = p.d_hitems;
   a.ccols = p.d_ccols;
   a.itab = p.d_itab;
+  a.wbin = p.d_wbin;
   for (int c = 0; c <= EMAXCL; ++c) a.ib[c] = p.ib[c];
   a.rdesc = p.d_rdesc;
   a.rptr = p.d_rptr;

@@ -242,3 +242,19 @@ def test_qce_shared_memory_fits_b200_at_cluster_6():
     for num in (6, 7, 8, 9, 10, 11, 12, 13):
         meta = qce_tables(f"{num}/15", 16200, 2)[3]
         assert meta[2] <= 232448, (num, meta[2])
+
+
+@pytest.mark.parametrize("rate,n,cluster", [("6/15", 64800, 6), ("10/15", 64800, 6),
+                                            ("7/15", 64800, 7), ("11/15", 16200, 2)])
+def test_variable_items_dealt_evenly_to_warp_bins(rate, n, cluster):
+    """The host deals each CTA's variable-phase items to 32 warp bins, the
+    most expensive first, each to the least-loaded bin: the bins' estimated
+    costs then differ by at most the largest item's (30 + 7 x the column
+    degree, two zones +10), and the item list keeps every item once."""
+    K, QA, QB, meta, rdesc, rptr, cdesc, ccols, s0, s0b, itab, hitems = \
+        qce_tables(rate, n, cluster)
+    lo, hi = int(meta[80]), int(meta[81])
+    dmax = int(cdesc[:, 0].max())
+    assert 0 < lo <= hi and hi - lo <= 40 + 7 * dmax
+    starts = sorted((int(y), int(x)) for x, y, z, w in itab)
+    assert len(starts) == len(set(starts)) == len(itab)
