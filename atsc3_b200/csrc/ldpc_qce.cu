@@ -96,15 +96,12 @@ struct QcePlan {
   int hsplit = 1;               // parts per heavy item (warps sharing it)
   int hpb_off = 0;              // shared-memory offset of the heavy partials
   int vbin_lo = 0, vbin_hi = 0; // least / most loaded variable-item bin (estimated cost)
-  int cbin_lo = 0, cbin_hi = 0; // the same for the light check items (0: not binned)
   int ib[EMAXCL + 1] = {0};     // variable-phase items of CTA c in d_itab
   int cb[EMAXCL + 1] = {0};     // CTA c owns columns ccols[cb[c] .. cb[c+1])
   int4 *d_rdesc = nullptr;      // per row edge slot
   int32_t *d_ccols = nullptr;   // (nb) columns grouped by owner CTA
   int4 *d_itab = nullptr;       // variable-phase items, grouped by CTA
   int32_t *d_wbin = nullptr;    // (cluster, QBINS+1) bin offsets into each CTA's items
-  int16_t *d_citem = nullptr;   // light check items of every CTA in warp-bin order
-  int32_t *d_cbin = nullptr;    // (cluster, QBINS+1) bin offsets into d_citem
   int32_t *d_rptr = nullptr;    // (Q+1)
   int4 *d_cdesc = nullptr;      // per column
   uint8_t *d_s0 = nullptr;      // (nb*360) rotation start (zone A / only zone)
@@ -132,8 +129,6 @@ struct QceTables {
   std::vector<int32_t> ccols;
   std::vector<int4> itab;
   std::vector<int32_t> wbin;    // (cluster, QBINS+1) bin offsets, relative to ib[c]
-  std::vector<int16_t> citem;   // light check items, per CTA, in warp-bin order
-  std::vector<int32_t> cbin;    // (cluster, QBINS+1) offsets into citem (empty: none)
   std::vector<uint8_t> s0, s0b;
   std::vector<int16_t> hitems;
 };
@@ -566,59 +561,6 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     p->ib[c + 1] = (int)t->itab.size();
   }
   for (int c = cluster + 1; c <= EMAXCL; ++c) p->ib[c] = p->ib[cluster];
-  // Light check items dealt to QBINS warp bins the same way (plans without
-  // heavy rows): item wl of CTA c maps to a block row and chunk exactly as
-  // the kernel maps it; estimated cost 16 + 4 deg on the unmasked paths,
-  // 24 + 5 NS on the masked path and for the packed last chunks.
-  t->citem.clear();
-  t->cbin.clear();
-  p->cbin_lo = p->cbin_hi = 0;
-  if (p->nhrows == 0) {
-    constexpr int TAILW = EZ - 32 * (ECHUNK - 1);
-    constexpr int TAILG = 32 / TAILW;
-    t->cbin.assign((size_t)cluster * (QBINS + 1), 0);
-    p->cbin_lo = 1 << 30;
-    for (int c = 0; c < cluster; ++c) {
-      const int c0 = p->ci[c], nci = p->ci[c + 1] - c0;
-      const int r0 = c0 / ECHUNK;
-      const int nr = nci > 0 ? (c0 + nci + ECHUNK - 1) / ECHUNK - r0 : 0;
-      const int coff = c0 - r0 * ECHUNK;
-      const int ntail = std::max(0, std::min(nr, (c0 + nci) / ECHUNK - r0));
-      const int nlead = nci - ntail;
-      const int ncpk = nlead + (ntail + TAILG - 1) / TAILG;
-      std::vector<int> cost(ncpk), order(ncpk);
-      for (int wl = 0; wl < ncpk; ++wl) {
-        int cst = 24 + 5 * ns;
-        if (wl < nlead) {
-          const int row = r0 + (wl + coff) / (ECHUNK - 1);
-          const int deg = (int)rows[row].size();
-          bool wrap = false;
-          for (auto &sl : rows[row]) wrap = wrap || sl.wrap;
-          if (!wrap && (deg == ns || deg == ns - 1 || (ns >= 10 && deg == ns - 2)))
-            cst = 16 + 4 * deg;
-        }
-        cost[wl] = cst;
-        order[wl] = wl;
-      }
-      std::stable_sort(order.begin(), order.end(),
-                       [&](int x, int y) { return cost[x] > cost[y]; });
-      std::vector<std::vector<int>> bins(QBINS);
-      std::vector<int> load(QBINS, 0);
-      for (int i : order) {
-        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        bins[b].push_back(i);
-        load[b] += cost[i];
-      }
-      for (int b = 0; b < QBINS; ++b) {
-        std::sort(bins[b].begin(), bins[b].end());
-        t->cbin[(size_t)c * (QBINS + 1) + b] = (int)t->citem.size();
-        for (int i : bins[b]) t->citem.push_back((int16_t)i);
-        p->cbin_lo = std::min(p->cbin_lo, load[b]);
-        p->cbin_hi = std::max(p->cbin_hi, load[b]);
-      }
-      t->cbin[(size_t)c * (QBINS + 1) + QBINS] = (int)t->citem.size();
-    }
-  }
   return 0;
 }
 
@@ -642,8 +584,6 @@ struct QceArgs {
   const int32_t *ccols;
   const int4 *itab;
   const int32_t *wbin;          // (cluster, QBINS+1) item-bin offsets per CTA
-  const int16_t *citem;         // light check items in warp-bin order, or null
-  const int32_t *cbin;          // (cluster, QBINS+1) offsets into citem
   const int4 *rdesc;
   const int32_t *rptr;
   const int4 *cdesc;
@@ -1246,14 +1186,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
       // (the parts path is float32 only; float64 plans keep one warp per item)
       const bool split = HV && sizeof(V) == 4 && a.nhrows && a.hsplit > 1;
       const int nhp = (HV && a.nhrows) ? (split ? nhi * a.hsplit : nhi) : 0;
-      // light items of plans without heavy rows: this warp's bins of the
-      // host's deal (citem holds the item indices); else round-robin
-      const bool binned = a.cbin != nullptr;
-      const int kbeg = binned ? __ldg(a.cbin + rank * (QBINS + 1) + warp * BPW) : warp;
-      const int kend = binned ? __ldg(a.cbin + rank * (QBINS + 1) + (warp + 1) * BPW)
-                              : nhp + ncpk;
-      for (int k = kbeg; k < kend; k += binned ? 1 : nwarps) {
-        const int w = binned ? (int)__ldg(a.citem + k) : k;
+      for (int w = warp; w < nhp + ncpk; w += nwarps) {
         int syn;
         if (HV && w < nhp && !split) {             // one warp per heavy item
           const int hi = __ldg(a.hitems + h0 + w);
@@ -1664,10 +1597,6 @@ static int32_t qce_plan_create_vb(int32_t n, int32_t kldpc, int32_t qa, int32_t 
   if (e == cudaSuccess) e = up((void **)&h->p.d_ccols, t.ccols.data(), t.ccols.size() * 4);
   if (e == cudaSuccess) e = up((void **)&h->p.d_itab, t.itab.data(), t.itab.size() * 16);
   if (e == cudaSuccess) e = up((void **)&h->p.d_wbin, t.wbin.data(), t.wbin.size() * 4);
-  if (e == cudaSuccess && !t.cbin.empty()) {
-    e = up((void **)&h->p.d_citem, t.citem.data(), t.citem.size() * 2);
-    if (e == cudaSuccess) e = up((void **)&h->p.d_cbin, t.cbin.data(), t.cbin.size() * 4);
-  }
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0, t.s0.data(), t.s0.size());
   if (e == cudaSuccess) e = up((void **)&h->p.d_s0b, t.s0b.data(), t.s0b.size());
   if (e == cudaSuccess)
@@ -1708,8 +1637,6 @@ void atsc3_ldpc_qce_plan_destroy(atsc3_ldpc_qce_plan *h) {
   cudaFree(h->p.d_ccols);
   cudaFree(h->p.d_itab);
   cudaFree(h->p.d_wbin);
-  cudaFree(h->p.d_citem);
-  cudaFree(h->p.d_cbin);
   cudaFree(h->p.d_s0);
   cudaFree(h->p.d_s0b);
   cudaFree(h->p.d_hitems);
@@ -1765,8 +1692,6 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
   meta[79] = p.nhrows;
   meta[80] = p.vbin_lo;
   meta[81] = p.vbin_hi;
-  meta[82] = p.cbin_lo;
-  meta[83] = p.cbin_hi;
   if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
@@ -2009,8 +1934,6 @@ static int32_t qce_decode_impl(
   a.ccols = p.d_ccols;
   a.itab = p.d_itab;
   a.wbin = p.d_wbin;
-  a.citem = p.d_citem;
-  a.cbin = p.d_cbin;
   for (int c = 0; c <= EMAXCL; ++c) a.ib[c] = p.ib[c];
   a.rdesc = p.d_rdesc;
   a.rptr = p.d_rptr;
