@@ -403,10 +403,10 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     else
       vmode[g] = one_zone ? VM_GEN : VM_GEN2;
   }
-  // variable-phase items per CTA: a pair or exact column is cut into six
-  // 64-bit items (lane L takes bits 64p + L and 64p + 32 + L), any other
-  // into twelve 32-bit items
-  auto items_of = [&](int g) { return vmode[g] <= VM_EXACT ? 6 : ECHUNK; };
+  // variable-phase items per CTA: every column is cut into six 64-bit
+  // items (lane L takes bits 64p + L and 64p + 32 + L: two independent
+  // sums a lane)
+  auto items_of = [&](int g) { (void)g; return 6; };
   int maxitems = 0;
   for (int c = 0; c < cluster; ++c) {
     int ni = 0;
@@ -531,13 +531,13 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     // the least-loaded bin (longest-processing-time rule), so that every
     // warp walking its own bin has about the same work; a bin keeps its
     // items in column order.  Estimated cost (instructions per item):
-    // pair 44, 1-4 slots in registers 20 + 2 d (d + 3), any slots 30 + 7 d
-    // (two zones: 40 + 7 d).
+    // pair 44, 1-4 slots in registers 20 + 2 d (d + 3), any slots 50 + 12 d
+    // (two zones: 60 + 12 d).
     std::vector<int> cost(items.size()), order(items.size());
     for (size_t i = 0; i < items.size(); ++i) {
       const int d = items[i].z & 0xFF, mode = (items[i].z >> 25) & 3;
       cost[i] = mode == VM_PAIR ? 44 : mode == VM_EXACT ? 20 + 2 * d * (d + 3)
-              : mode == VM_GEN ? 30 + 7 * d : 40 + 7 * d;
+              : mode == VM_GEN ? 50 + 12 * d : 60 + 12 * d;
       order[i] = (int)i;
     }
     std::stable_sort(order.begin(), order.end(),
@@ -635,57 +635,83 @@ __device__ __forceinline__ V qce_var_exact(V *col, int s0, V li, bool mv) {
   return tot;
 }
 
-// Sum of one zone's slots of a column (`col` = its first slot, d slots) in
-// the reference order: slots s0 .. d-1, then 0 .. s0-1.  Inside a warp the
-// lanes' s0 differ little, so with lo/hi = the warp's least/greatest s0 the
-// common parts [hi, d) and [0, lo) are summed unconditionally and only
-// [lo, hi) needs a per-lane choice (adding -0.0 leaves a float sum
-// unchanged).  The order of additions is each lane's own, so the sum is
-// exact.
+
+
+// Sums of one zone's slots of a column (`c0`, `c1` = the first slot of the
+// two bits a lane takes in a 64-bit item, d slots) in each bit's reference
+// order: slots s0 .. d-1, then 0 .. s0-1.  The two sums run interleaved, so
+// a warp advances two independent chains of additions.  Inside a warp the
+// bits' s0 differ little, so with lo/hi = the least/greatest s0 of both
+// bits over the warp the common parts [hi, d) and [0, lo) are summed
+// unconditionally and only [lo, hi) needs a per-bit choice (adding -0.0
+// leaves a float sum unchanged).  The order of additions is each bit's own,
+// so the sums are exact.
 template <typename V>
-__device__ __forceinline__ V qce_seg_sum(V acc, const V *col, int d, int s0) {
-  const int lo = (int)__reduce_min_sync(0xffffffffu, (uint32_t)s0);
-  const int hi = (int)__reduce_max_sync(0xffffffffu, (uint32_t)s0);
-  for (int i = lo; i < hi; ++i) {                  // own tail, first part
-    const V m = col[i * EZ];
-    acc = add_rn(acc, i >= s0 ? m : V(-0.0));
+__device__ __forceinline__ void qce_seg_sum2(V &acc0, V &acc1, const V *c0,
+                                             const V *c1, int d, int s00,
+                                             int s01) {
+  const int lo = (int)min(__reduce_min_sync(0xffffffffu, (uint32_t)s00),
+                          __reduce_min_sync(0xffffffffu, (uint32_t)s01));
+  const int hi = (int)max(__reduce_max_sync(0xffffffffu, (uint32_t)s00),
+                          __reduce_max_sync(0xffffffffu, (uint32_t)s01));
+  for (int i = lo; i < hi; ++i) {
+    const V m0 = c0[i * EZ], m1 = c1[i * EZ];
+    acc0 = add_rn(acc0, i >= s00 ? m0 : V(-0.0));
+    acc1 = add_rn(acc1, i >= s01 ? m1 : V(-0.0));
   }
 #pragma unroll 4
-  for (int i = hi; i < d; ++i) acc = add_rn(acc, col[i * EZ]);
-#pragma unroll 4
-  for (int i = 0; i < lo; ++i) acc = add_rn(acc, col[i * EZ]);
-  for (int i = lo; i < hi; ++i) {                  // own head, last part
-    const V m = col[i * EZ];
-    acc = add_rn(acc, i < s0 ? m : V(-0.0));
+  for (int i = hi; i < d; ++i) {
+    acc0 = add_rn(acc0, c0[i * EZ]);
+    acc1 = add_rn(acc1, c1[i * EZ]);
   }
-  return acc;
+#pragma unroll 4
+  for (int i = 0; i < lo; ++i) {
+    acc0 = add_rn(acc0, c0[i * EZ]);
+    acc1 = add_rn(acc1, c1[i * EZ]);
+  }
+  for (int i = lo; i < hi; ++i) {
+    const V m0 = c0[i * EZ], m1 = c1[i * EZ];
+    acc0 = add_rn(acc0, i < s00 ? m0 : V(-0.0));
+    acc1 = add_rn(acc1, i < s01 ? m1 : V(-0.0));
+  }
 }
 
-// Variable phase of one bit for a column of d edges (any d >= 1) whose
-// first dA slots lie in the accumulator rows and the rest in the identity
-// rows (dA == d for one zone): the reference order is zone A rotated at s0,
-// then zone B rotated at s0b; every slot is rewritten as tot - m.
+// Variable phase of the two bits a lane takes in a 64-bit item, for a column
+// of d edges (any d >= 1) whose first dA slots lie in the accumulator rows
+// and the rest in the identity rows (dA == d for one zone): per bit the
+// reference order is zone A rotated at s0, then zone B rotated at s0b;
+// every slot of a bit that is live (mv) is rewritten as tot - m.  Returns
+// the two posteriors.
 template <typename V, bool TORCH>
-__device__ __forceinline__ V qce_var_generic(V *col, int d, int dA, int s0,
-                                             int s0b, V li, bool mv) {
-  V acc = TORCH ? li : V(0);
-  acc = qce_seg_sum(acc, col, dA, s0);
-  if (dA < d) acc = qce_seg_sum(acc, col + dA * EZ, d - dA, s0b);
-  // torch semantics: + 0.0 turns a -0.0 sum into +0.0 (the only way a
-  // slot could receive -0.0; the sign is the same for the hard decision)
-  const V tot = TORCH ? add_rn(acc, V(0)) : add_rn(li, acc);
-  if (mv) {
-    int i = 0;
-    for (; i + 4 <= d; i += 4) {
-      V v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = col[(i + u) * EZ];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) col[(i + u) * EZ] = sub_rn(tot, v[u]);
+__device__ __forceinline__ void qce_var_generic2(V *c0, V *c1, int d, int dA,
+                                                 int s00, int s01, int s0b0,
+                                                 int s0b1, V li0, V li1,
+                                                 bool mv0, bool mv1, V &t0,
+                                                 V &t1) {
+  V a0 = TORCH ? li0 : V(0), a1 = TORCH ? li1 : V(0);
+  qce_seg_sum2(a0, a1, c0, c1, dA, s00, s01);
+  if (dA < d) qce_seg_sum2(a0, a1, c0 + dA * EZ, c1 + dA * EZ, d - dA, s0b0, s0b1);
+  // torch semantics: + 0.0 turns a -0.0 sum into +0.0 (see qce_var_exact)
+  t0 = TORCH ? add_rn(a0, V(0)) : add_rn(li0, a0);
+  t1 = TORCH ? add_rn(a1, V(0)) : add_rn(li1, a1);
+  int i = 0;
+  for (; i + 2 <= d; i += 2) {
+    const V m00 = c0[i * EZ], m01 = c0[(i + 1) * EZ];
+    const V m10 = c1[i * EZ], m11 = c1[(i + 1) * EZ];
+    if (mv0) {
+      c0[i * EZ] = sub_rn(t0, m00);
+      c0[(i + 1) * EZ] = sub_rn(t0, m01);
     }
-    for (; i < d; ++i) col[i * EZ] = sub_rn(tot, col[i * EZ]);
+    if (mv1) {
+      c1[i * EZ] = sub_rn(t1, m10);
+      c1[(i + 1) * EZ] = sub_rn(t1, m11);
+    }
   }
-  return tot;
+  if (i < d) {
+    const V m0 = c0[i * EZ], m1 = c1[i * EZ];
+    if (mv0) c0[i * EZ] = sub_rn(t0, m0);
+    if (mv1) c1[i * EZ] = sub_rn(t1, m1);
+  }
 }
 
 // One check item: block row rl, chunk ch (32 consecutive checks), D slots.
@@ -1380,25 +1406,35 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
             if (nv1) dsmem_st_u32(bm_peer + (bw + 1) * 4u, h1);
           }
         } else {
-          // 32-bit item: any degree, one zone or both
-          const bool mv = (uint32_t)lane < ((iw.z >> 8) & 0xFFu);
-          const int ln = mv ? lane : 0;          // lanes past 359 read bit 0
-          const int lamidx = (int)iw.y + ln;
-          const V li = lam[lamidx];
-          V *col = reinterpret_cast<V *>(smem + iw.x) + ln;
-          const int s0 = __ldg(a.s0 + lamidx);
-          int dA = d, s0b = 0;
+          // 64-bit item of any degree, one zone or both: lane L takes bits
+          // y + L and y + 32 + L (lanes past 359 read bit y)
+          const uint32_t nv0 = (iw.z >> 8) & 0xFFu, nv1 = (iw.z >> 16) & 0xFFu;
+          const bool mv0 = (uint32_t)lane < nv0, mv1 = (uint32_t)lane < nv1;
+          const int x0 = (int)iw.y + (mv0 ? lane : 0);
+          const int x1 = (int)iw.y + (mv1 ? 32 + lane : 0);
+          const V li0 = lam[x0], li1 = lam[x1];
+          V *c0 = reinterpret_cast<V *>(smem + iw.x) + (x0 - (int)iw.y);
+          V *c1 = reinterpret_cast<V *>(smem + iw.x) + (x1 - (int)iw.y);
+          const int s00 = __ldg(a.s0 + x0), s01 = __ldg(a.s0 + x1);
+          int dA = d, s0b0 = 0, s0b1 = 0;
           if (TA && mode == VM_GEN2) {
             dA = (int)((iw.w >> 16) & 0xFFu);
-            s0b = __ldg(a.s0b + lamidx);
+            s0b0 = __ldg(a.s0b + x0);
+            s0b1 = __ldg(a.s0b + x1);
           }
-          const V tot = qce_var_generic<V, TORCH>(col, d, dA, s0, s0b, li, mv);
-          // the absent wrap entry (bit 359 = lane 7 of the last item) stays
-          // -0.0
+          V t0, t1;
+          qce_var_generic2<V, TORCH>(c0, c1, d, dA, s00, s01, s0b0, s0b1, li0, li1,
+                                     mv0, mv1, t0, t1);
+          // the absent wrap entry (bit 359 = lane 7 of the column's last
+          // item's last sub-chunk) stays -0.0
           if (((iw.z >> 24) & 1u) && lane == ABSENT_LANE)
-            col[(int)(iw.w >> 24) * EZ] = V(-0.0);
-          const uint32_t hb = __ballot_sync(0xffffffffu, mv && tot < V(0));
-          if (lane < CL) dsmem_st_u32(bm_peer + bw * 4u, hb);
+            (nv1 ? c1 : c0)[(int)(iw.w >> 24) * EZ] = V(-0.0);
+          const uint32_t h0 = __ballot_sync(0xffffffffu, mv0 && t0 < V(0));
+          const uint32_t h1 = __ballot_sync(0xffffffffu, mv1 && t1 < V(0));
+          if (lane < CL) {
+            dsmem_st_u32(bm_peer + bw * 4u, h0);
+            if (nv1) dsmem_st_u32(bm_peer + (bw + 1) * 4u, h1);
+          }
         }
       }
       cluster_sync_all();

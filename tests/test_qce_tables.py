@@ -159,14 +159,16 @@ def test_qce_descriptors_reproduce_csr(rate, n, cluster):
         got_s = [x for x in got if not (isinstance(x, tuple) and x[0] == "unvisited")]
         assert got_s == sampled, lam
         assert len(got) == len(want), lam
-    # variable-phase items: the pair path sums slot 0 then slot 1 (no
-    # rotation), the register path takes 1..4 slots of one zone, the
-    # two-segment path only columns with slots in both zones
+    # variable-phase items (64 bits each: two bits a lane): the pair path
+    # sums slot 0 then slot 1 (no rotation), the register path takes 1..4
+    # slots of one zone, the two-segment path only columns with slots in
+    # both zones
     for x, y, z, w in itab:
         g, mm0 = divmod(int(y), QZ)
         d, dA, mode = z & 0xFF, (w >> 16) & 0xFF, (z >> 25) & 3
         assert d == cdesc[g][0] and dA == dA_of[g]
-        bits = range(g * QZ + mm0, g * QZ + min(QZ, mm0 + (64 if mode <= 1 else 32)))
+        bits = range(g * QZ + mm0, g * QZ + min(QZ, mm0 + 64))   # 64-bit items
+        assert mm0 % 64 == 0
         if mode == 0:
             # (bit 359 of the wrap column has one real edge and the -0.0
             # entry, whose place in the sum does not matter)
