@@ -650,10 +650,36 @@ template <typename V>
 __device__ __forceinline__ void qce_seg_sum2(V &acc0, V &acc1, const V *c0,
                                              const V *c1, int d, int s00,
                                              int s01) {
-  const int lo = (int)min(__reduce_min_sync(0xffffffffu, (uint32_t)s00),
-                          __reduce_min_sync(0xffffffffu, (uint32_t)s01));
-  const int hi = (int)max(__reduce_max_sync(0xffffffffu, (uint32_t)s00),
-                          __reduce_max_sync(0xffffffffu, (uint32_t)s01));
+  // s0 runs 0 .. d (d: no slot wrapped, the same order as 0)
+  const int lo = (int)__reduce_min_sync(0xffffffffu, (uint32_t)min(s00, s01));
+  const int hi = (int)__reduce_max_sync(0xffffffffu, (uint32_t)max(s00, s01));
+  if (hi - lo <= 2 && d > 0) {
+    // the common case: at most two slots whose place differs between the
+    // warp's bits, loaded once and held in registers for both passes
+    const int i0 = min(lo, d - 1), i1 = min(lo + 1, d - 1);
+    const bool h0 = lo < hi, h1 = lo + 1 < hi;
+    const V w00 = c0[i0 * EZ], w01 = c0[i1 * EZ];
+    const V w10 = c1[i0 * EZ], w11 = c1[i1 * EZ];
+    acc0 = add_rn(acc0, h0 && lo >= s00 ? w00 : V(-0.0));
+    acc1 = add_rn(acc1, h0 && lo >= s01 ? w10 : V(-0.0));
+    acc0 = add_rn(acc0, h1 && lo + 1 >= s00 ? w01 : V(-0.0));
+    acc1 = add_rn(acc1, h1 && lo + 1 >= s01 ? w11 : V(-0.0));
+#pragma unroll 4
+    for (int i = hi; i < d; ++i) {
+      acc0 = add_rn(acc0, c0[i * EZ]);
+      acc1 = add_rn(acc1, c1[i * EZ]);
+    }
+#pragma unroll 4
+    for (int i = 0; i < lo; ++i) {
+      acc0 = add_rn(acc0, c0[i * EZ]);
+      acc1 = add_rn(acc1, c1[i * EZ]);
+    }
+    acc0 = add_rn(acc0, h0 && lo < s00 ? w00 : V(-0.0));
+    acc1 = add_rn(acc1, h0 && lo < s01 ? w10 : V(-0.0));
+    acc0 = add_rn(acc0, h1 && lo + 1 < s00 ? w01 : V(-0.0));
+    acc1 = add_rn(acc1, h1 && lo + 1 < s01 ? w11 : V(-0.0));
+    return;
+  }
   for (int i = lo; i < hi; ++i) {
     const V m0 = c0[i * EZ], m1 = c1[i * EZ];
     acc0 = add_rn(acc0, i >= s00 ? m0 : V(-0.0));
@@ -1034,6 +1060,31 @@ __device__ __forceinline__ int qce_check_heavy(const uint2 *he, int deg, int wra
 
 // NS: compile-time slots per block row (qce_ns); NT: threads per CTA; TA:
 // the Type A paths (rows above NS, columns in both zones) are compiled in.
+// A variable item's inputs that the slots do not hold: its table entry, the
+// channel LLRs of the lane's two bits (lane L takes bits y + L and y + 32 + L;
+// lanes past the item's bit count read bit y) and their first-slot indices.
+// None of them changes during a codeword, so the variable phase can fetch the
+// next item's while it works on the current one.
+template <typename V>
+struct QceVarIn {
+  uint4 iw;
+  V li0, li1;
+  int s00, s01;
+};
+
+template <typename V>
+__device__ __forceinline__ void qce_var_fetch(QceVarIn<V> &f, const uint4 *itab, int w,
+                                              int lane, const V *lam, const uint8_t *s0) {
+  f.iw = itab[w];
+  const uint32_t nv0 = (f.iw.z >> 8) & 0xFFu, nv1 = (f.iw.z >> 16) & 0xFFu;
+  const int x0 = (int)f.iw.y + ((uint32_t)lane < nv0 ? lane : 0);
+  const int x1 = (int)f.iw.y + ((uint32_t)lane < nv1 ? 32 + lane : 0);
+  f.li0 = lam[x0];
+  f.li1 = lam[x1];
+  f.s00 = __ldg(s0 + x0);
+  f.s01 = __ldg(s0 + x1);
+}
+
 template <typename V, bool TORCH, int NS, int NT, bool TA>
 __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   using MASK = typename std::conditional<(NS > 32), unsigned long long,
@@ -1163,6 +1214,10 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
   // (volatile: not kept in registers across the codeword loop)
   constexpr int BPW = QBINS / (NT / 32);
   static_assert(BPW >= 1 && QBINS % (NT / 32) == 0, "512 or 1024 threads");
+  // the variable phase fetches item k+1's inputs while it works on item k
+  // (their global loads leave the item's chain) where the registers allow:
+  // float32 kernels of up to 8 slots (Type B) at 1024 threads, up to 22 at 512
+  constexpr bool VPF = sizeof(V) == 4 && (NT >= 1024 ? (NS <= 8 && !TA) : NS <= 22);
 
   for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
     const V *lam = reinterpret_cast<const V *>(a.llr) + (size_t)b * a.ld_llr;
@@ -1349,9 +1404,21 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
         break;
       }
       // ---------------- variable phase (local) -----------------------------
-      for (int w = ((volatile int *)part)[4 + warp * BPW],
-               we = ((volatile int *)part)[4 + (warp + 1) * BPW]; w < we; ++w) {
-        const uint4 iw = itab[w];
+      // (the first item's inputs are fetched after the barrier: its release
+      // would wait for loads issued before it)
+      const int vw0 = ((volatile int *)part)[4 + warp * BPW];
+      const int vwe = ((volatile int *)part)[4 + (warp + 1) * BPW];
+      QceVarIn<V> nx;
+      if (VPF && vw0 < vwe) qce_var_fetch(nx, itab, vw0, lane, lam, a.s0);
+      for (int vw = vw0; vw < vwe; ++vw) {
+        QceVarIn<V> cur;
+        if constexpr (VPF) {
+          cur = nx;
+          if (vw + 1 < vwe) qce_var_fetch(nx, itab, vw + 1, lane, lam, a.s0);
+        } else {
+          qce_var_fetch(cur, itab, vw, lane, lam, a.s0);
+        }
+        const uint4 iw = cur.iw;
         const int d = (int)(iw.z & 0xFFu);
         const int mode = (int)((iw.z >> 25) & 3u);
         const uint32_t bw = iw.w & 0xFFFFu;            // bitmap word
@@ -1360,7 +1427,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           const uint32_t nv0 = (iw.z >> 8) & 0xFFu, nv1 = (iw.z >> 16) & 0xFFu;
           const bool mv0 = (uint32_t)lane < nv0, mv1 = (uint32_t)lane < nv1;
           const int l0 = mv0 ? lane : 0, l1 = mv1 ? 32 + lane : 0;
-          const V li0 = lam[iw.y + l0], li1 = lam[iw.y + l1];
+          const V li0 = cur.li0, li1 = cur.li1;
           V *col0 = reinterpret_cast<V *>(smem + iw.x) + l0;
           V *col1 = reinterpret_cast<V *>(smem + iw.x) + l1;
           V t0, t1;
@@ -1384,7 +1451,7 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
               col1[EZ] = absent ? V(-0.0) : sub_rn(t1, b1);
             }
           } else {
-            const int r0s = __ldg(a.s0 + iw.y + l0), r1s = __ldg(a.s0 + iw.y + l1);
+            const int r0s = cur.s00, r1s = cur.s01;
             if (d == 3) {
               t0 = qce_var_exact<V, TORCH, 3>(col0, r0s, li0, mv0);
               t1 = qce_var_exact<V, TORCH, 3>(col1, r1s, li1, mv1);
@@ -1412,10 +1479,10 @@ __global__ void __launch_bounds__(NT, 1) ldpc_qce_kernel(const QceArgs a) {
           const bool mv0 = (uint32_t)lane < nv0, mv1 = (uint32_t)lane < nv1;
           const int x0 = (int)iw.y + (mv0 ? lane : 0);
           const int x1 = (int)iw.y + (mv1 ? 32 + lane : 0);
-          const V li0 = lam[x0], li1 = lam[x1];
+          const V li0 = cur.li0, li1 = cur.li1;
           V *c0 = reinterpret_cast<V *>(smem + iw.x) + (x0 - (int)iw.y);
           V *c1 = reinterpret_cast<V *>(smem + iw.x) + (x1 - (int)iw.y);
-          const int s00 = __ldg(a.s0 + x0), s01 = __ldg(a.s0 + x1);
+          const int s00 = cur.s00, s01 = cur.s01;
           int dA = d, s0b0 = 0, s0b1 = 0;
           if (TA && mode == VM_GEN2) {
             dA = (int)((iw.w >> 16) & 0xFFu);
