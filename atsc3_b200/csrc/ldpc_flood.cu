@@ -34,6 +34,8 @@
 // Tables (built on the host, see build_tables): sliced-ELL lists of 32
 // checks / 32 variables per warp, padded with sentinels.
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -296,6 +298,21 @@ __device__ __forceinline__ uint64_t low_mask64(int d) {
   return d >= 64 ? ~0ull : ((1ull << d) - 1ull);
 }
 
+// Semantics of the per-codeword decoder: SEM_KERNEL = lab/ldpc_kernel.c;
+// SEM_TORCH = lab/m9_gpu.py in float32/float64; SEM_TORCH_BF16 / _F16 =
+// lab/m9_gpu.py with dtype bfloat16 / float16, whose torch operations each
+// compute in float32 and round the result to the narrow type: the decoder
+// keeps float32 values that are all exact in the narrow type and rounds every
+// subtraction, scaled minimum and partial sum the same way.
+constexpr int SEM_KERNEL = 0, SEM_TORCH = 1, SEM_TORCH_BF16 = 2, SEM_TORCH_F16 = 3;
+
+template <int SEM> __device__ __forceinline__ float narrow(float x) {
+  if constexpr (SEM == SEM_TORCH_BF16) return __bfloat162float(__float2bfloat16_rn(x));
+  else if constexpr (SEM == SEM_TORCH_F16) return __half2float(__float2half_rn(x));
+  else return x;
+}
+template <int SEM> __device__ __forceinline__ double narrow(double x) { return x; }
+
 // Geometry and tables of one code, as the per-codeword decoder sees them.
 struct CwView {
   int n, nc, ncp, nvlog2, nslc, nslv;
@@ -310,13 +327,17 @@ struct CwView {
 // codeword (posteriors, records, partial counts).  Writes bits_row /
 // hard_row (nullable) and *conv, *its, *bad (rank 0).  Ends after a
 // __syncthreads, with no distributed-shared-memory access in flight.
-template <typename T, int RB, bool TORCH>
+template <typename T, int RB, int SEM>
 __device__ __forceinline__ void flood_codeword(
     const CwView &g, const T *lam, int iters, T alpha, unsigned char *sm,
     int rank, int CL, uint8_t *bits_row, uint8_t *hard_row, uint8_t *conv,
     int32_t *its, int32_t *bad) {
   using R = Rec<T, RB>;
   constexpr int NV = R::NV;
+  constexpr bool TORCH = SEM != SEM_KERNEL;
+  // the narrow types scale by alpha rounded to them (torch: alpha * sign
+  // computed in float32, then rounded)
+  alpha = narrow<SEM>(alpha);
   const int nvp = 1 << g.nvlog2;
   const uint32_t vmask = (uint32_t)nvp - 1u;
   T *tot = reinterpret_cast<T *>(sm);
@@ -383,7 +404,7 @@ __device__ __forceinline__ void flood_codeword(
             syn ^= (t[u] < T(0)) ? 1u : 0u;
             T mo = (j == Fo) ? Bo : Ao;
             if (R::sign(ro, j)) mo = -mo;
-            const T v = sub_rn(t[u], mo);
+            const T v = narrow<SEM>(sub_rn(t[u], mo));
             const uint64_t sg = (v < T(0)) ? 1ull : 0ull;
             if (j < 64) slo |= sg << j; else shi |= sg << (j - 64);
             const T mag = fabs(v);
@@ -398,7 +419,8 @@ __device__ __forceinline__ void flood_codeword(
           shi ^= deg > 64 ? low_mask64(deg - 64) : 0ull;
         }
         uint4 rn[NV];
-        R::pack(rn, mul_rn(min1, alpha), mul_rn(min2, alpha), first, slo, shi);
+        R::pack(rn, narrow<SEM>(mul_rn(min1, alpha)), narrow<SEM>(mul_rn(min2, alpha)),
+                first, slo, shi);
 #pragma unroll
         for (int q = 0; q < NV; ++q) rec[(c - cbase) * NV + q] = rn[q];
         mybad += (int)syn;
@@ -478,7 +500,7 @@ __device__ __forceinline__ void flood_codeword(
             const int j = (int)(en[u] >> 20);
             T m = (j == R::F(rr[u])) ? R::B(rr[u]) : R::A(rr[u]);
             if (R::sign(rr[u], j)) m = -m;
-            acc = add_rn(acc, m);
+            acc = narrow<SEM>(add_rn(acc, m));
           }
         }
         tot[i - vbase] = TORCH ? acc : add_rn(li, acc);
@@ -489,7 +511,7 @@ __device__ __forceinline__ void flood_codeword(
   }
 }
 
-template <typename T, int RB, bool TORCH>
+template <typename T, int RB, int SEM>
 __global__ void __launch_bounds__(1024, 1) ldpc_flood_kernel(const FloodArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int rank = (int)cluster_ctarank();
@@ -498,7 +520,7 @@ __global__ void __launch_bounds__(1024, 1) ldpc_flood_kernel(const FloodArgs a) 
                  a.cent, a.cslice, a.vent, a.vslice};
   for (int b = (int)cluster_id_x(); b < a.nblk; b += (int)ncluster_x()) {
     const T *lam = reinterpret_cast<const T *>(a.llr) + (size_t)b * a.ld_llr;
-    flood_codeword<T, RB, TORCH>(
+    flood_codeword<T, RB, SEM>(
         g, lam, a.iters, (T)a.alpha, smem, rank, CL,
         a.bits ? a.bits + (size_t)b * a.ld_bits : nullptr,
         a.hard ? a.hard + (size_t)b * a.ld_hard : nullptr, a.conv + b,
@@ -516,14 +538,24 @@ __global__ void __launch_bounds__(1024, 1) ldpc_flood_kernel(const FloodArgs a) 
 typedef void (*FloodFn)(const FloodArgs);
 
 static FloodFn flood_fn(int dtype, int rb, int semantics) {
-  if (dtype == 0 && rb == 16)
-    return semantics ? ldpc_flood_kernel<float, 16, true>
-                     : ldpc_flood_kernel<float, 16, false>;
-  if (dtype == 0 && rb == 32)
-    return semantics ? ldpc_flood_kernel<float, 32, true>
-                     : ldpc_flood_kernel<float, 32, false>;
+  if (dtype == 0 && rb == 16) {
+    switch (semantics) {
+      case SEM_KERNEL: return ldpc_flood_kernel<float, 16, SEM_KERNEL>;
+      case SEM_TORCH: return ldpc_flood_kernel<float, 16, SEM_TORCH>;
+      case SEM_TORCH_BF16: return ldpc_flood_kernel<float, 16, SEM_TORCH_BF16>;
+      case SEM_TORCH_F16: return ldpc_flood_kernel<float, 16, SEM_TORCH_F16>;
+    }
+  }
+  if (dtype == 0 && rb == 32) {
+    switch (semantics) {
+      case SEM_KERNEL: return ldpc_flood_kernel<float, 32, SEM_KERNEL>;
+      case SEM_TORCH: return ldpc_flood_kernel<float, 32, SEM_TORCH>;
+      case SEM_TORCH_BF16: return ldpc_flood_kernel<float, 32, SEM_TORCH_BF16>;
+      case SEM_TORCH_F16: return ldpc_flood_kernel<float, 32, SEM_TORCH_F16>;
+    }
+  }
   if (dtype == 1 && rb == 32)
-    return semantics ? ldpc_flood_kernel<double, 32, true> : nullptr;
+    return semantics == SEM_TORCH ? ldpc_flood_kernel<double, 32, SEM_TORCH> : nullptr;
   return nullptr;
 }
 
@@ -615,9 +647,10 @@ int32_t flood_launch(const atsc3_ldpc_plan *p, const void *llr, int64_t ld_llr,
   ATSC3_ARG(p != nullptr, "null plan");
   ATSC3_ARG(nblk >= 0, "nblk < 0");
   ATSC3_ARG(iters >= 0, "iters < 0");
-  ATSC3_ARG(semantics == 0 || semantics == 1, "semantics must be 0 or 1");
-  ATSC3_ARG(!(semantics == 1 && iters == 0), "semantics 1 needs iters >= 1");
-  ATSC3_ARG(!(p->dtype == 1 && semantics == 0),
+  ATSC3_ARG(semantics >= SEM_KERNEL && semantics <= SEM_TORCH_F16,
+            "semantics must be 0, 1, 2 or 3");
+  ATSC3_ARG(!(semantics != SEM_KERNEL && iters == 0), "semantics 1-3 need iters >= 1");
+  ATSC3_ARG(!(p->dtype == 1 && semantics != SEM_TORCH),
             "float64 messages are only offered with semantics 1");
   ATSC3_ARG(ld_llr >= p->n, "ld_llr < n");
   ATSC3_ARG(bits == nullptr || ld_bits >= p->n, "ld_bits < n");
@@ -1062,11 +1095,11 @@ __global__ void __launch_bounds__(1024, 1) ldpc_batch_kernel(const BatchArgs a) 
     const float *lam = a.llr + __ldg(a.llr_off + b);
     uint8_t *hr = a.hard ? a.hard + __ldg(a.hard_off + b) : nullptr;
     if (P.rb == 16)
-      flood_codeword<float, 16, false>(P.g, lam, a.iters, a.alpha, smem + 16,
+      flood_codeword<float, 16, SEM_KERNEL>(P.g, lam, a.iters, a.alpha, smem + 16,
                                        rank, CL, nullptr, hr, a.conv + b,
                                        a.its + b, a.bad + b);
     else
-      flood_codeword<float, 32, false>(P.g, lam, a.iters, a.alpha, smem + 16,
+      flood_codeword<float, 32, SEM_KERNEL>(P.g, lam, a.iters, a.alpha, smem + 16,
                                        rank, CL, nullptr, hr, a.conv + b,
                                        a.its + b, a.bad + b);
   }

@@ -29,7 +29,10 @@ import numpy as np
 from . import codes as C
 from . import native as N
 
-SEMANTICS = {"kernel": 0, "torch": 1}
+# torch_bf16 / torch_f16: lab/m9_gpu.py with dtype bfloat16 / float16 (every
+# operation computed in float32 and rounded to the narrow type), on float32
+# CSR plans only
+SEMANTICS = {"kernel": 0, "torch": 1, "torch_bf16": 2, "torch_f16": 3}
 _DTYPES = {"float32": 0, "float64": 1}
 
 
@@ -320,23 +323,33 @@ class GpuMinSum:
     def __init__(self, checks, n, iters=50, alpha=0.75, device="cuda",
                  dtype="float64", semantics="torch", cluster=0):
         torch = _torch()
-        if dtype not in ("float64", "float32"):
-            raise ValueError("GpuMinSum on B200 decodes in float64 or float32 "
-                             "(bit-exact); bfloat16/float16 are not offered")
+        if dtype not in ("float64", "float32", "bfloat16", "float16"):
+            raise ValueError("dtype must be float64, float32, bfloat16 or float16")
         if semantics == "kernel" and dtype != "float32":
             raise ValueError("kernel semantics are float32 only")
+        narrow = dtype in ("bfloat16", "float16")
         self.n, self.iters, self.alpha = int(n), iters, alpha
         self.dev = torch.device(device)
-        self.dt = {"float64": torch.float64, "float32": torch.float32}[dtype]
+        # bfloat16/float16 (lab/m9_gpu.py:100-101): the LLRs are rounded to
+        # that type as the reference's .to(dtype) does, and the CSR decoder
+        # rounds every operation's result to it (semantics torch_bf16 /
+        # torch_f16), holding the values in float32
+        self.dt = {"float64": torch.float64, "float32": torch.float32,
+                   "bfloat16": torch.bfloat16, "float16": torch.float16}[dtype]
         self.dtype_name = dtype
         self.semantics = semantics
+        if narrow:
+            self.semantics = "torch_bf16" if dtype == "bfloat16" else "torch_f16"
         with torch.cuda.device(self.dev):
             tabs = C.csr_from_checks(checks, n)
+            pdt = "float32" if narrow else dtype
             # an A/322 code (recognised from its CSR tables) takes the
-            # edge-buffer decoder, any other matrix the CSR decoder
-            self.plan = qce_plan_from_csr(tabs, n, dtype=dtype, cluster=cluster)
+            # edge-buffer decoder, any other matrix (and the narrow types)
+            # the CSR decoder
+            self.plan = None if narrow else qce_plan_from_csr(tabs, n, dtype=pdt,
+                                                              cluster=cluster)
             if self.plan is None:
-                self.plan = Plan(*tabs, n, dtype=dtype, cluster=cluster)
+                self.plan = Plan(*tabs, n, dtype=pdt, cluster=cluster)
         self.nc = self.plan.nc
         self.stats = dict(calls=0, iters=0, blocks=0)
 
@@ -349,6 +362,8 @@ class GpuMinSum:
         else:
             a = np.ascontiguousarray(np.asarray(llr2d, np.float64))
             llr = torch.from_numpy(a).to(self.dev, dtype=self.dt)
+        if self.dt in (torch.bfloat16, torch.float16):
+            llr = llr.float()           # exact: the decoder holds float32
         if llr.dim() != 2 or llr.shape[1] != self.n:
             raise ValueError(f"expected (nblk, {self.n}) LLRs")
         nb = llr.shape[0]

@@ -103,6 +103,10 @@ int32_t atsc3_ldpc_tables_host(const int32_t *cptr, const int32_t *cidx,
  *   variable sum from +0 then added to the channel LLR);
  * semantics 1: lab/m9_gpu.py:168-211 / lab/m3_ldpc.py:560-630 float64 path
  *   (update first, its >= 1, variable sum accumulated onto the channel LLR).
+ * semantics 2 / 3 (float32 plans): semantics 1 as lab/m9_gpu.py runs it with
+ *   dtype bfloat16 / float16 (lab/m9_gpu.py:100-101): every subtraction,
+ *   scaled minimum (alpha itself rounded first) and partial variable sum is
+ *   rounded to that type; llr must already hold values of that type.
  * bits (nullable): (nblk, ld_bits) uint8 hard decisions, 1 = negative LLR.
  * hard (nullable): (nblk, ld_hard) packed hard decisions, n/8 bytes, MSB
  *   first in each byte (numpy packbits order).
