@@ -22,7 +22,8 @@ Contents (reference file:line each restates):
 * ``flood`` -- ``ldpc_oracle.c`` (lab/ldpc_kernel.c semantics and the
   float64 / torch semantics); ``flood_ref`` -- the reference kernel itself;
   ``flood_weighted`` -- the same kernel semantics with per-iteration,
-  per-check-degree scale/offset minima (the learned decoder), numpy.
+  per-check-degree scale/offset minima (the learned decoder), numpy;
+  ``flood_torch_narrow`` -- lab/m9_gpu.py:138-220 in bfloat16 / float16.
 """
 from __future__ import annotations
 
@@ -188,6 +189,89 @@ def flood_weighted(llr, tables, n, walpha, wbeta, dbucket, iters=50,
             tot = (lam + s).astype(f32)
         bits[b] = (tot < 0)
     return bits, conv, its, bad
+
+
+def _narrow(x, dtype):
+    """Round float32 values to bfloat16 / float16 (round to nearest even) and
+    back: the result of a torch operation in that dtype."""
+    x = np.asarray(x, np.float32)
+    if dtype == "float16":
+        return x.astype(np.float16).astype(np.float32)
+    u = x.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32)
+
+
+def flood_torch_narrow(llr, tables, n, iters=50, alpha=0.75, dtype="bfloat16"):
+    """The reference's torch min-sum decoder run with dtype bfloat16 / float16
+    (lab/m9_gpu.py:138-220): every elementwise operation computed in float32
+    and its result rounded to the narrow type.  Per-edge messages m in the
+    CSR edge order; each iteration v = tot[cidx] - m, first/second minimum of
+    |v| per check (first position wins ties), m = round(round(alpha) * out)
+    with the sign parity ^ (v < 0), then tot = llr + m summed over each bit's
+    edges in edge order (bits of lower degree add 0.0, as the reference's
+    padded table does), hard decisions and the syndrome of tot; a block
+    freezes at its first zero syndrome with its = it + 1 (no iteration-0
+    retire).  llr: (nblk, n) already in the narrow type (float64 input is
+    rounded by the caller, as the reference's ``.to(dtype)``).  Checks of
+    degree 1 are assumed absent (the reference pads with a large finite
+    value, here infinity).  Returns (bits uint8, conv bool, its int32,
+    bad int32)."""
+    cptr, cidx, vptr, vedge = [np.asarray(t) for t in tables]
+    lam = np.asarray(llr, np.float32)
+    nb = lam.shape[0]
+    nc = len(cptr) - 1
+    deg = np.diff(cptr)
+    dmax = int(deg.max())
+    E = len(cidx)
+    echk = np.repeat(np.arange(nc), deg)
+    eslot = np.arange(E) - cptr[echk]
+    vdeg = np.diff(vptr)
+    ar = _narrow(np.float32(alpha), dtype)
+    m = np.zeros((nb, E), np.float32)
+    tot = lam.copy()
+    out_bits = np.zeros((nb, n), np.uint8)
+    out_its = np.full(nb, iters, np.int32)
+    out_bad = np.zeros(nb, np.int32)
+    frozen = np.zeros(nb, bool)
+    bad = np.zeros(nb, np.int32)
+    bits = (tot < 0).astype(np.uint8)
+    rows = np.arange(nb)[:, None]
+    for it in range(iters):
+        v = _narrow(tot[:, cidx] - m, dtype)
+        sg = v < 0
+        par = np.zeros((nb, nc), np.int64)
+        np.add.at(par, (slice(None), echk), sg.astype(np.int64))
+        par &= 1
+        mag = np.full((nb, nc, dmax), np.inf, np.float32)
+        mag[:, echk, eslot] = np.abs(v)
+        m1 = mag.min(2)
+        first = np.argmax(mag == m1[:, :, None], axis=2)
+        mag[rows, np.arange(nc)[None, :], first] = np.inf
+        m2 = mag.min(2)
+        outv = np.where(eslot[None, :] == first[:, echk], m2[:, echk], m1[:, echk])
+        mm = _narrow(ar * outv, dtype)
+        m = np.where((par[:, echk] == 1) ^ sg, -mm, mm).astype(np.float32)
+        tot = lam.copy()
+        for k in range(int(vdeg.max())):
+            add = np.zeros((nb, n), np.float32)
+            sel = vdeg > k
+            add[:, sel] = m[:, vedge[vptr[:-1][sel] + k]]
+            tot = _narrow(tot + add, dtype)
+        bits = (tot < 0).astype(np.uint8)
+        syn = np.zeros((nb, nc), np.int64)
+        np.add.at(syn, (slice(None), echk), bits[:, cidx].astype(np.int64))
+        bad = (syn & 1).sum(1).astype(np.int32)
+        newly = ~frozen & (bad == 0)
+        out_bits[newly] = bits[newly]
+        out_its[newly] = it + 1
+        frozen |= newly
+        if frozen.all():
+            break
+    live = ~frozen
+    out_bits[live] = bits[live]
+    out_bad[live] = bad[live]
+    return out_bits, frozen, out_its, out_bad
 
 
 def flood_ref(llr, tables, n, iters=50, alpha=0.75, threads=1):
