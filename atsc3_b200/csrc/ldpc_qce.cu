@@ -1795,6 +1795,7 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
   meta[79] = p.nhrows;
   meta[80] = p.vbin_lo;
   meta[81] = p.vbin_hi;
+  meta[82] = QBINS;
   if (rdesc) std::memcpy(rdesc, t.rdesc.data(), t.rdesc.size() * 16);
   if (rptr) std::memcpy(rptr, t.rptr.data(), t.rptr.size() * 4);
   if (cdesc) std::memcpy(cdesc, t.cdesc.data(), t.cdesc.size() * 16);
@@ -1804,6 +1805,19 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
   if (itab) std::memcpy(itab, t.itab.data(), t.itab.size() * 16);
   if (hitems)
     for (size_t i = 0; i < t.hitems.size(); ++i) hitems[i] = t.hitems[i];
+  return 0;
+}
+
+int32_t atsc3_ldpc_qce_bins_host(int32_t n, int32_t kldpc, int32_t qa, int32_t qb,
+                                 const int32_t *rowptr, const int32_t *addr,
+                                 int32_t cluster, int32_t *wbin) {
+  using namespace atsc3;
+  ATSC3_ARG(rowptr && addr && wbin, "null argument");
+  QcePlan p;
+  QceTables t;
+  int rc = qce_build(n, kldpc, qa, qb, rowptr, addr, cluster, &p, &t);
+  if (rc) return rc;
+  std::memcpy(wbin, t.wbin.data(), t.wbin.size() * 4);
   return 0;
 }
 

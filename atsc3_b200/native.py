@@ -62,6 +62,8 @@ SIGNATURES = {
     "atsc3_ldpc_qce_decode_f64": (c_i32, [c_vp, c_vp, c_i64, c_i32, c_i32, c_f64,
                                           c_i32, c_vp, c_i64, c_vp, c_i64, c_vp,
                                           c_vp, c_vp, c_i32, c_vp]),
+    "atsc3_ldpc_qce_bins_host": (c_i32, [c_i32, c_i32, c_i32, c_i32, c_vp, c_vp, c_i32,
+                                         c_vp]),
     "atsc3_ldpc_qce_tables_host2": (c_i32, [c_i32, c_i32, c_i32, c_i32, c_vp,
                                             c_vp, c_i32, c_vp, c_vp, c_vp,
                                             c_vp, c_vp, c_vp, c_vp, c_vp,

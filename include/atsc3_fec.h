@@ -286,7 +286,9 @@ int32_t atsc3_ldpc_qce_tables_host(int32_t n, int32_t kldpc, int32_t qldpc,
  * c from meta[42+c] to meta[43+c] (its light items when heavy rows exist),
  * [59] heavy rows present, [60] degree that sets the compile-time slot
  * count, [61] variable-phase items, [62..78] heavy items of CTA c:
- * hitems[meta[62+c] .. meta[63+c]), [79] heavy rows (block rows 0 ..).
+ * hitems[meta[62+c] .. meta[63+c]), [79] heavy rows (block rows 0 ..),
+ * [80] / [81] least / greatest estimated variable-item bin load, [82] bins
+ * per CTA (QBINS).
  * s0b: (n) rotation start in the identity rows; itab: int4 per
  * variable-phase item; hitems: heavy check items, grouped by CTA.  Array
  * outputs may be null. */
@@ -298,6 +300,15 @@ int32_t atsc3_ldpc_qce_tables_host2(int32_t n, int32_t kldpc, int32_t qa,
                                     int32_t *ccols, uint8_t *s0,
                                     uint8_t *s0b, int32_t *itab,
                                     int32_t *hitems);
+
+/* Variable-item bins of the edge-buffer plan (host only, no device work):
+ * wbin = (cluster, QBINS + 1) offsets, relative to each CTA's first item in
+ * the itab of atsc3_ldpc_qce_tables_host2; warp w of a CTA of T threads walks
+ * bins w*QBINS/(T/32) .. (w+1)*QBINS/(T/32) - 1.  QBINS is meta[82] of
+ * atsc3_ldpc_qce_tables_host2 (32). */
+int32_t atsc3_ldpc_qce_bins_host(int32_t n, int32_t kldpc, int32_t qa, int32_t qb,
+                                 const int32_t *rowptr, const int32_t *addr,
+                                 int32_t cluster, int32_t *wbin);
 
 int32_t atsc3_ldpc_qce_config(const atsc3_ldpc_qce_plan *plan, int32_t threads,
                               int32_t semantics, int32_t *out);
