@@ -530,14 +530,15 @@ int qce_build(int n, int K, int QA, int QB, const int32_t *rowptr,
     // Deal the CTA's items to QBINS bins, the most expensive first, each to
     // the least-loaded bin (longest-processing-time rule), so that every
     // warp walking its own bin has about the same work; a bin keeps its
-    // items in column order.  Estimated cost (instructions per item):
-    // pair 44, 1-4 slots in registers 20 + 2 d (d + 3), any slots 50 + 12 d
-    // (two zones: 60 + 12 d).
+    // items in column order.  Estimated cost (cycles per item of a
+    // 1024-thread CTA under full load, fitted to per-warp phase times of
+    // 64800-bit 6/15, 8/15 and 10/15 codewords): pair 840, 1-4 slots in
+    // registers 280 + 240 d, any slots 1330 + 140 d (two zones: + 200).
     std::vector<int> cost(items.size()), order(items.size());
     for (size_t i = 0; i < items.size(); ++i) {
       const int d = items[i].z & 0xFF, mode = (items[i].z >> 25) & 3;
-      cost[i] = mode == VM_PAIR ? 44 : mode == VM_EXACT ? 20 + 2 * d * (d + 3)
-              : mode == VM_GEN ? 50 + 12 * d : 60 + 12 * d;
+      cost[i] = mode == VM_PAIR ? 840 : mode == VM_EXACT ? 280 + 240 * d
+              : mode == VM_GEN ? 1330 + 140 * d : 1530 + 140 * d;
       order[i] = (int)i;
     }
     std::stable_sort(order.begin(), order.end(),

@@ -251,15 +251,15 @@ def test_qce_shared_memory_fits_b200_at_cluster_6():
 def test_variable_items_dealt_evenly_to_warp_bins(rate, n, cluster):
     """The host deals each CTA's variable-phase items to 32 warp bins, the
     most expensive first, each to the least-loaded bin: the bins' estimated
-    costs then differ by at most the largest item's (50 + 12 x the column
-    degree, two zones +10), the item list keeps every item once, and the
+    costs then differ by at most the largest item's (1330 + 140 x the column
+    degree, two zones +200), the item list keeps every item once, and the
     exported bin offsets (atsc3_ldpc_qce_bins_host) cut each CTA's items
     into QBINS consecutive, non-overlapping runs."""
     K, QA, QB, meta, rdesc, rptr, cdesc, ccols, s0, s0b, itab, hitems = \
         qce_tables(rate, n, cluster)
     lo, hi = int(meta[80]), int(meta[81])
     dmax = int(cdesc[:, 0].max())
-    assert 0 < lo <= hi and hi - lo <= 60 + 12 * dmax
+    assert 0 < lo <= hi and hi - lo <= 1530 + 140 * dmax
     starts = sorted((int(y), int(x)) for x, y, z, w in itab)
     assert len(starts) == len(set(starts)) == len(itab)
     qbins = int(meta[82])
