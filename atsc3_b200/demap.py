@@ -182,6 +182,8 @@ def demap_llr_fast(cells, mod, rate, sigma2=None, dtype=np.float64, ex=None,
     compatibility.  ``sigma2`` may also be a per-cell array (divided after
     the minima)."""
     torch = _torch()
+    if np.size(cells) == 0:         # nothing to demap (no sigma2 estimate either)
+        return np.zeros(0, np.float64)
     if np.dtype(dtype) == np.float64:
         z = np.ascontiguousarray(np.asarray(cells), np.complex128).reshape(1, -1)
         s2 = sigma2

@@ -221,7 +221,7 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
     want_t = torch.float64 if plan.dtype == "float64" else torch.float32
     if llr.dtype != want_t or llr.device.type != "cuda":
         raise TypeError(f"llr must be a CUDA {want_t} tensor")
-    if llr.dim() != 2 or llr.shape[1] != plan.n or llr.stride(1) != 1:
+    if llr.dim() != 2 or llr.shape[1] != plan.n or (llr.shape[0] and llr.stride(1) != 1):
         raise ValueError("llr must be (nblk, n) with unit column stride")
     nblk = llr.shape[0]
     dev = llr.device
@@ -237,6 +237,8 @@ def decode_flood(plan, llr, iters=50, alpha=0.75, semantics="kernel",
             o[k] = torch.empty(nblk, dtype=dt, device=dev)
     bits = o.get("bits") if want_bits else None
     hard = o.get("hard") if want_hard else None
+    if nblk == 0:                  # nothing to launch (empty tensors' strides are arbitrary)
+        return o
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
     kind = getattr(plan, "kind", "csr")
     if weights is not None and kind not in ("qc", "qce"):
@@ -430,7 +432,7 @@ def decode_layered(plan, llr, iters=50, alpha=0.75, want_bits=True,
     torch = _torch()
     if llr.dtype != torch.float32 or llr.device.type != "cuda":
         raise TypeError("llr must be a CUDA float32 tensor")
-    if llr.dim() != 2 or llr.shape[1] != plan.n or llr.stride(1) != 1:
+    if llr.dim() != 2 or llr.shape[1] != plan.n or (llr.shape[0] and llr.stride(1) != 1):
         raise ValueError("llr must be (nblk, n) with unit column stride")
     nblk = llr.shape[0]
     dev = llr.device
@@ -446,6 +448,8 @@ def decode_layered(plan, llr, iters=50, alpha=0.75, want_bits=True,
             o[k] = torch.empty(nblk, dtype=dt, device=dev)
     bits = o.get("bits") if want_bits else None
     hard = o.get("hard") if want_hard else None
+    if nblk == 0:                  # nothing to launch (empty tensors' strides are arbitrary)
+        return o
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
     N.call("atsc3_ldpc_layered_decode", plan.handle, llr.data_ptr(),
            llr.stride(0), nblk, int(iters), float(alpha), N.ptr(bits),
@@ -502,7 +506,8 @@ def sp_decode(tab, llr, iters=100, out=None, stream=None):
     unsatisfied count).  Returns device tensors bits, conv, its, bad."""
     torch = _torch()
     if llr.dtype != torch.float64 or llr.device.type != "cuda" or \
-            llr.dim() != 2 or llr.shape[1] != tab["n"] or llr.stride(1) != 1:
+            llr.dim() != 2 or llr.shape[1] != tab["n"] or \
+            (llr.shape[0] and llr.stride(1) != 1):
         raise TypeError("llr must be a (nblk, n) CUDA float64 tensor")
     nblk, n = llr.shape
     dev = llr.device
@@ -511,6 +516,8 @@ def sp_decode(tab, llr, iters=100, out=None, stream=None):
     o.setdefault("conv", torch.empty(nblk, dtype=torch.uint8, device=dev))
     o.setdefault("its", torch.empty(nblk, dtype=torch.int32, device=dev))
     o.setdefault("bad", torch.empty(nblk, dtype=torch.int32, device=dev))
+    if nblk == 0:
+        return o
     nbytes = ctypes.c_int64()
     N.call("atsc3_ldpc_sp_workspace", n, tab["nedges"], nblk, ctypes.byref(nbytes))
     work = torch.empty(max(8, nbytes.value), dtype=torch.uint8, device=dev)
