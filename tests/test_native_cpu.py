@@ -162,3 +162,27 @@ def test_noalloc_refuses_bch_lengths_past_the_codeword(kldpc, kpay, what):
         None, None, None, None, None, None)
     assert rc == -3
     assert what in N.lib().atsc3_last_error().decode()
+
+
+def test_minsum_f32_degree_above_128_returns_minus_one_and_writes_nothing():
+    """lab/ldpc_kernel.c:78-80: a check of more than MAX_ROW_DEG = 128 edges
+    makes ldpc_minsum_f32 return -1 before it writes any output (the check
+    runs before any device work, so this needs no GPU)."""
+    import ctypes
+    n = 129
+    cptr = np.array([0, n], np.int32)
+    cidx = np.arange(n, dtype=np.int32)
+    vptr = np.arange(n + 1, dtype=np.int32)
+    vedge = np.arange(n, dtype=np.int32)
+    llr = np.ones((2, n), np.float32)
+    bits = np.full((2, n), 7, np.uint8)
+    conv = np.full(2, 7, np.uint8)
+    its = np.full(2, -7, np.int32)
+    bad = np.full(2, -7, np.int32)
+    rc = N.lib().ldpc_minsum_f32(llr.ctypes.data, 2, n, 1, n, cptr.ctypes.data,
+                                 cidx.ctypes.data, vptr.ctypes.data, vedge.ctypes.data,
+                                 10, ctypes.c_float(0.75), bits.ctypes.data,
+                                 conv.ctypes.data, its.ctypes.data, bad.ctypes.data, None)
+    assert rc == -1
+    assert (bits == 7).all() and (conv == 7).all() and (its == -7).all() and (bad == -7).all()
+
