@@ -1,8 +1,9 @@
 """GpuMinSum(dtype="bfloat16"/"float16") on the GPU against
 ``oracle.flood_torch_narrow`` (the reference's torch decoder in that dtype,
 lab/m9_gpu.py:138-220, pinned against the reference itself by
-tests/test_oracle_narrow.py): bits, conv, its and bad identical.  Both cases
-mix converging and stuck blocks (16200 6/15 at 1.5 dB; 64800 8/15 at its
+tests/test_oracle_narrow.py): bits, conv, its and bad identical.  All three cases
+mix converging and stuck blocks (16200 6/15 at 1.5 dB; the Type A 16200 3/15 at
+-3.75 dB: two of six converge; 64800 8/15 at its
 measured threshold, 7.75 dB: one block converges at 28 iterations, two stick
 with 6 and 2 unsatisfied checks in bfloat16)."""
 import numpy as np
@@ -17,6 +18,7 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("dtype", ["bfloat16", "float16"])
 @pytest.mark.parametrize("rate,n,mod,esn0,chan,nblk", [
     ("6/15", 16200, "QPSK", 1.5, "awgn", 6),
+    ("3/15", 16200, "QPSK", -3.75, "awgn", 6),
     ("8/15", 64800, "16QAM", 7.75, "awgn", 3)])
 def test_gpuminsum_narrow_vs_oracle(dtype, rate, n, mod, esn0, chan, nblk):
     import torch

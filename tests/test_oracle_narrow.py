@@ -29,15 +29,16 @@ def _case(rate, n, mod, esn0, chan, nblk, seed):
 
 
 @pytest.mark.parametrize("dtype", ["bfloat16", "float16"])
-def test_narrow_oracle_matches_reference_torch_cpu(dtype):
+@pytest.mark.parametrize("rate,esn0", [("6/15", 1.5), ("3/15", -3.75)])
+def test_narrow_oracle_matches_reference_torch_cpu(dtype, rate, esn0):
     import torch
     for p in (os.path.dirname(LAB), LAB):
         if p not in sys.path:
             sys.path.insert(0, p)
     import m3_ldpc
     import m9_gpu
-    rate, n = "6/15", 16200
-    lam = _case(rate, n, "QPSK", 1.5, "awgn", 6, 21)
+    n = 16200                      # 6/15 Type B, 3/15 Type A
+    lam = _case(rate, n, "QPSK", esn0, "awgn", 6, 21)
     want = m9_gpu.GpuMinSum(m3_ldpc.parity_check(rate, n), n, iters=30,
                             device="cpu", dtype=dtype).decode(lam)
     tdt = torch.bfloat16 if dtype == "bfloat16" else torch.float16
