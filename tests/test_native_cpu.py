@@ -186,3 +186,17 @@ def test_minsum_f32_degree_above_128_returns_minus_one_and_writes_nothing():
     assert rc == -1
     assert (bits == 7).all() and (conv == 7).all() and (its == -7).all() and (bad == -7).all()
 
+
+
+def test_gpuminsum_argument_checks_before_any_device_work():
+    """GpuMinSum accepts the reference's four dtypes (lab/m9_gpu.py:100-101)
+    and refuses others, and kernel semantics outside float32, before it
+    builds a plan (so these raise without a GPU)."""
+    import pytest
+    from atsc3_b200 import ldpc
+    with pytest.raises(ValueError):
+        ldpc.GpuMinSum([[0, 1]], 2, dtype="int8")
+    for dt in ("float64", "bfloat16", "float16"):
+        with pytest.raises(ValueError):
+            ldpc.GpuMinSum([[0, 1]], 2, dtype=dt, semantics="kernel")
+    assert set(ldpc.SEMANTICS) == {"kernel", "torch", "torch_bf16", "torch_f16"}
