@@ -196,7 +196,8 @@ def _narrow(x, dtype):
     back: the result of a torch operation in that dtype."""
     x = np.asarray(x, np.float32)
     if dtype == "float16":
-        return x.astype(np.float16).astype(np.float32)
+        with np.errstate(over="ignore"):        # overflow to +-inf is the result
+            return x.astype(np.float16).astype(np.float32)
     u = x.view(np.uint32).astype(np.uint64)
     r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
     return r.view(np.float32)
